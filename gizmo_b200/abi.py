@@ -1,0 +1,131 @@
+"""ctypes mirror of include/gizmo_hydro.h and the loader for the CUDA library.
+
+The C-ABI library ``gizmo_b200/lib/libgizmo_hydro.so`` is the product: the
+neighbour grid and the density / gradient / force kernels for sm_100a behind
+the ``gz_*`` entry points. This module only declares the structures and
+argument types; it never falls back to anything when the library is absent
+(``load_library`` raises).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+KERNEL_CUBIC = 3
+KERNEL_WENDLAND_C2 = 6
+METHOD_MFM = 0
+METHOD_MFV = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_NO_DEVICE = 3
+ERR_ORDER = 4
+ERR_CAPACITY = 5
+ERR_DENSITY_MAXITER = 1155
+ERR_EMPTY_BRACKET = 90001009
+ERR_RIEMANN = 1234
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class GzParams(C.Structure):
+    _fields_ = [
+        ("kernel", C.c_int),
+        ("method", C.c_int),
+        ("precision", C.c_int),
+        ("first_step", C.c_int),
+        ("selfgravity_off", C.c_int),
+        ("reserved", C.c_int),
+        ("box_size", C.c_double),
+        ("gamma", C.c_double),
+        ("des_num_ngb", C.c_double),
+        ("max_num_ngb_dev", C.c_double),
+        ("min_kernel_radius", C.c_double),
+        ("max_kernel_radius", C.c_double),
+    ]
+
+
+class GzParticles(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("pos", _dp),
+        ("vel", _dp),
+        ("mass", _dp),
+        ("u", _dp),
+        ("dt", _dp),
+        ("h", _dp),
+        ("cond", _dp),
+    ]
+
+
+OUTPUT_FIELDS = [
+    ("h", 1), ("num_ngb", 1), ("drkern", 1), ("divvel", 1), ("rho", 1), ("pressure", 1),
+    ("nvt", 6), ("cond", 1), ("fce", 1), ("pvel", 3), ("grad_rho", 3), ("grad_p", 3),
+    ("grad_v", 9), ("accel", 3), ("dudt", 1), ("vsig", 1), ("dtmass", 1), ("dmass", 1),
+    ("gravwork", 3),
+]
+
+
+class GzOutputs(C.Structure):
+    _fields_ = [(name, _dp) for name, _ in OUTPUT_FIELDS] + [("iters", _ip)]
+
+
+class GzStatusInfo(C.Structure):
+    _fields_ = [
+        ("code", C.c_int),
+        ("index", C.c_int),
+        ("density_iterations", C.c_int),
+        ("reserved", C.c_int),
+        ("pairs_density", C.c_int64),
+        ("pairs_symmetric", C.c_int64),
+        ("device_bytes", C.c_int64),
+        ("message", C.c_char * 256),
+    ]
+
+
+EXPORTED_SYMBOLS = [
+    "gz_create", "gz_destroy", "gz_set_params", "gz_upload", "gz_hydro_density",
+    "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream",
+    "gz_neighbors", "gz_density_sums",
+]
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libgizmo_hydro.so")
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load the CUDA C-ABI library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"gizmo_b200: CUDA library {p} is missing; run __graft_entry__.build() "
+            "(nvcc, sm_100a). There is no CPU fallback.")
+    lib = C.CDLL(p)
+    vp = C.c_void_p
+    lib.gz_create.argtypes = [C.POINTER(GzParams), C.c_int, C.POINTER(vp)]
+    lib.gz_destroy.argtypes = [vp]
+    lib.gz_set_params.argtypes = [vp, C.POINTER(GzParams)]
+    lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
+    for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):
+        getattr(lib, name).argtypes = [vp, _ip, C.c_int]
+    lib.gz_download.argtypes = [vp, C.POINTER(GzOutputs)]
+    lib.gz_status.argtypes = [vp, C.POINTER(GzStatusInfo)]
+    lib.gz_stream.argtypes = [vp]
+    lib.gz_stream.restype = vp
+    lib.gz_neighbors.argtypes = [vp, _ip, C.c_int, C.c_int, C.POINTER(C.c_int64), _ip]
+    lib.gz_density_sums.argtypes = [vp, _ip, C.c_int, _dp, _dp]
+    for name in EXPORTED_SYMBOLS:
+        if name != "gz_stream":
+            getattr(lib, name).restype = C.c_int
+    if path is None:
+        _lib = lib
+    return lib

@@ -1,0 +1,174 @@
+/* include/gizmo_hydro.h -- C ABI of the B200 meshless hydro pass.
+ *
+ * Drop-in boundary for GIZMO's hydro neighbour loops. In the reference the
+ * three host entry points
+ *     void density(void)             src/hydro/density_loop.cc:764
+ *     void hydro_gradient_calc(void) src/hydro/gradients_loop.cc:458
+ *     void hydro_force(void)         src/hydro/hydro_force_loop.cc:423
+ * drive the neighbour-loop runner (run_neighbor_loop_iterative<DensitySpec>,
+ * run_neighbor_loop<GradientsSpec>, run_neighbor_loop<HydroForceSpec>;
+ * src/mesh/neighbor_loop_runner.h:1614-1629) over the global P[] / CellP[]
+ * arrays. A shim compiled into the reference host replaces those three
+ * runner calls with the gz_hydro_* calls below; the host keeps gravity,
+ * cooling, domain, timestep and I/O. The shim gathers the P/CellP fields
+ * listed in gz_particles (AoS -> SoA) for gz_upload and scatters the
+ * gz_outputs fields back after gz_download.
+ *
+ * Conventions (mirroring the reference's endrun() semantics without a stop):
+ *   - every call returns GZ_OK (0) or a nonzero code; reference stop codes
+ *     are kept where one exists (1155, 90001009, 1234);
+ *   - no exceptions cross the ABI and device code never traps: device-side
+ *     failures are recorded in a status word and read by gz_status;
+ *   - the library owns all device memory; the caller owns host arrays;
+ *   - one context per thread at a time; each context has its own stream.
+ * Plain pointers and sizes only. Arrays are row-major [n][k] FP64 in the
+ * caller's original particle order.
+ */
+#ifndef GIZMO_HYDRO_H
+#define GIZMO_HYDRO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Kernel functions (KERNEL_FUNCTION, src/mesh/kernel.h:268-438). */
+#define GZ_KERNEL_CUBIC        3   /* Morris cubic spline, norm 8/pi */
+#define GZ_KERNEL_WENDLAND_C2  6   /* Wendland C2, norm 21/(2 pi) */
+
+/* Hydro methods (HYDRO_MESHLESS_FINITE_MASS / _VOLUME). */
+#define GZ_METHOD_MFM 0
+#define GZ_METHOD_MFV 1
+
+/* Arithmetic forms of the pass. */
+#define GZ_PRECISION_FP64  0   /* every pair and per-particle operation in FP64 */
+#define GZ_PRECISION_MIXED 1   /* FP32 pair math; FP64 positions, membership,
+                                  h-iteration, 3x3 inversion and flux sums */
+
+/* Return codes. */
+#define GZ_OK                   0
+#define GZ_ERR_ARG              1       /* bad argument or size */
+#define GZ_ERR_CUDA             2       /* CUDA runtime error (message in gz_status) */
+#define GZ_ERR_NO_DEVICE        3
+#define GZ_ERR_ORDER            4       /* pass called before its inputs exist */
+#define GZ_ERR_CAPACITY         5       /* a device work buffer would exceed its limit */
+#define GZ_ERR_DENSITY_MAXITER  1155    /* neighbor_loop_runner.cc:7485 endrun(1155) */
+#define GZ_ERR_EMPTY_BRACKET    90001009 /* density_loop.h:891-895 */
+#define GZ_ERR_RIEMANN          1234    /* hydro_core_meshless_functions.h:403-425 */
+
+/* Run-time configuration: the All.* fields and compile-time flags the pass
+ * reads. Non-cosmological (cf_atime = 1, ComovingIntegrationOn = 0). */
+typedef struct gz_params {
+    int    kernel;             /* GZ_KERNEL_* */
+    int    method;             /* GZ_METHOD_* */
+    int    precision;          /* GZ_PRECISION_* */
+    int    first_step;         /* 1 when All.Time == All.TimeBegin (density_loop.h:523-525) */
+    int    selfgravity_off;    /* SELFGRAVITY_OFF: limiter h_lim/stol (gradients_loop.cc:1094-1096)
+                                  and MFM entropic thresholds (hydro_functions.h:175-183) */
+    int    reserved;
+    double box_size;           /* All.BoxSize, periodic in x, y, z */
+    double gamma;              /* EOS_GAMMA (ideal gas P = (gamma-1) rho u) */
+    double des_num_ngb;        /* All.DesNumNgb */
+    double max_num_ngb_dev;    /* All.MaxNumNgbDeviation */
+    double min_kernel_radius;  /* All.MinKernelRadius */
+    double max_kernel_radius;  /* All.MaxKernelRadius */
+} gz_params;
+
+/* Inputs per gas particle (the P / CellP fields the pass reads). */
+typedef struct gz_particles {
+    int64_t       n;
+    const double *pos;    /* [n][3] P[i].Pos, inside [0, box_size) */
+    const double *vel;    /* [n][3] CellP[i].VelPred */
+    const double *mass;   /* [n]    P[i].Mass */
+    const double *u;      /* [n]    CellP[i].InternalEnergyPred */
+    const double *dt;     /* [n]    get_particle_timestep_in_physical(i) */
+    const double *h;      /* [n]    P[i].KernelRadius seed for the density iteration */
+    const double *cond;   /* [n]    CellP[i].ConditionNumber from the previous step (0 if none) */
+} gz_particles;
+
+/* Outputs; any pointer may be NULL to skip that field. */
+typedef struct gz_outputs {
+    double *h;         /* [n]    P.KernelRadius */
+    double *num_ngb;   /* [n]    P.NumNgb (after ^(1/3)) */
+    double *drkern;    /* [n]    P.DrkernNgbFactor */
+    double *divvel;    /* [n]    P.Particle_DivVel */
+    double *rho;       /* [n]    CellP.Density */
+    double *pressure;  /* [n]    CellP.Pressure */
+    double *nvt;       /* [n][6] CellP.NV_T (inverse, xx yy zz xy yz xz) */
+    double *cond;      /* [n]    CellP.ConditionNumber */
+    double *fce;       /* [n]    CellP.FaceClosureError */
+    double *pvel;      /* [n][3] CellP.ParticleVel (MFV) */
+    double *grad_rho;  /* [n][3] CellP.Gradients.Density */
+    double *grad_p;    /* [n][3] CellP.Gradients.Pressure */
+    double *grad_v;    /* [n][9] CellP.Gradients.Velocity (row k = grad v_k) */
+    double *accel;     /* [n][3] CellP.HydroAccel (dv/dt) */
+    double *dudt;      /* [n]    CellP.DtInternalEnergy (du/dt) */
+    double *vsig;      /* [n]    CellP.MaxSignalVel */
+    double *dtmass;    /* [n]    CellP.DtMass (MFV) */
+    double *dmass;     /* [n]    CellP.dMass (MFV) */
+    double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
+    int    *iters;     /* [n]    density iterations taken */
+} gz_outputs;
+
+typedef struct gz_status_info {
+    int      code;              /* first recorded error code, 0 if none */
+    int      index;             /* original particle index it refers to, -1 if none */
+    int      density_iterations;/* iterations of the last density pass */
+    int      reserved;
+    int64_t  pairs_density;     /* accepted one-way pairs summed over iterations */
+    int64_t  pairs_symmetric;   /* symmetric pairs (rows of the gradient/force lists) */
+    int64_t  device_bytes;      /* device memory held by the context */
+    char     message[256];
+} gz_status_info;
+
+typedef struct gz_context gz_context;
+
+/* Create a context on CUDA device `device` (its own stream). */
+int gz_create(const gz_params *params, int device, gz_context **out);
+int gz_destroy(gz_context *ctx);
+/* Replace the run-time configuration (keeps particle data). */
+int gz_set_params(gz_context *ctx, const gz_params *params);
+
+/* Copy inputs host -> device and mark the neighbour grid stale.
+ * Replaces the arena acquire of neighbor_loop_runner.cc:2297-2302. */
+int gz_upload(gz_context *ctx, const gz_particles *in);
+
+/* The three passes. `active` lists original indices (NULL = all particles),
+ * like ActiveParticleList filtered by density_isactive / GasGrad_isactive.
+ *   gz_hydro_density   : DensitySpec loop + density_finalize_post_runner
+ *   gz_hydro_gradients : GradientsSpec loop + gradient finalize/limiter
+ *   gz_hydro_force     : preloop + HydroForceSpec loop + hydro_final_operations */
+int gz_hydro_density(gz_context *ctx, const int *active, int n_active);
+int gz_hydro_gradients(gz_context *ctx, const int *active, int n_active);
+int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
+
+/* Copy outputs device -> host (original order). */
+int gz_download(gz_context *ctx, const gz_outputs *out);
+
+/* Error/progress record of the context (device status word included). */
+int gz_status(gz_context *ctx, gz_status_info *info);
+
+/* CUDA stream of the context (cudaStream_t), for callers that time or
+ * order work around the passes. */
+void *gz_stream(gz_context *ctx);
+
+/* Exact neighbour sets of the last pass, for bit-exact checks against a CPU
+ * search. mode 0: one-way r < h_i at the converged h; mode 1: symmetric
+ * 0 < r and (r < h_i or r < h_j). Rows follow `active` (NULL = all),
+ * entries are original indices sorted ascending. Call once with
+ * nbrs == NULL to get offsets (n_active + 1 entries); then with nbrs sized
+ * offsets[n_active]. */
+int gz_neighbors(gz_context *ctx, const int *active, int n_active, int mode,
+                 int64_t *offsets, int *nbrs);
+
+/* Density accumulator at the current kernel lengths, no iteration: for each
+ * active, acc[a][14] = {Ngb, Rho, DrkernNgb, DivVel, NV_T xx,yy,zz,xy,yz,xz,
+ * face x,y,z, 0} and pv[a][3] = ParticleVel sum (MFV), exactly the
+ * DensitySpec::pair_kernel sums (density_loop.h:1140-1385). */
+int gz_density_sums(gz_context *ctx, const int *active, int n_active, double *acc, double *pv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

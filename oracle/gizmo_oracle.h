@@ -1,0 +1,106 @@
+/* oracle/gizmo_oracle.h -- CPU restatement of GIZMO's meshless hydro pass.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker the CUDA path is compared
+ * against; nothing in the product (gizmo_b200/, include/) links it. It is
+ * loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline
+ * leg, and nowhere else.
+ *
+ * It restates, in plain C with no fused multiply-adds, the reference's
+ *   - density / kernel-length solve   (hydro/density_loop.h:515-961, 1140-1385;
+ *                                      hydro/density_loop.cc:303-733)
+ *   - gradient pass + slope limiter   (hydro/gradient_functions.h:304-665;
+ *                                      hydro/gradients_loop.cc:76-136, 848-1130)
+ *   - MFM/MFV force pass              (hydro/hydro_functions.h:56-546;
+ *                                      hydro/hydro_core_meshless_functions.h:48-616;
+ *                                      hydro/compute_finitevol_faces_functions.h:46-168;
+ *                                      hydro/reimann.h:125-1090;
+ *                                      hydro/hydro_toplevel.cc:133-253, 457-565)
+ * for the ideal-gas, non-MHD, non-cosmological, 3-D, periodic-box build, and
+ * an exact neighbour search applying the reference predicates
+ * (density_loop.h:1163-1171 one-way; hydro_functions.h:77-83 symmetric).
+ *
+ * Parity is pinned against the reference's own pair bodies compiled from
+ * its sources by oracle/build_ref.sh (see tests/test_oracle_vs_reference.py).
+ */
+#ifndef GIZMO_ORACLE_H
+#define GIZMO_ORACLE_H
+
+#include "../include/gizmo_hydro.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Particle state in original (unsorted) order, all FP64, row-major [n][k]. */
+typedef struct orc_state {
+    int n;
+    /* inputs */
+    double *pos;       /* [n][3] P.Pos */
+    double *vel;       /* [n][3] CellP.VelPred */
+    double *mass;      /* [n]    P.Mass */
+    double *u;         /* [n]    CellP.InternalEnergyPred */
+    double *dt;        /* [n]    physical timestep (get_particle_timestep_in_physical) */
+    double *h;         /* [n]    P.KernelRadius (in: seed, out: converged) */
+    double *cond;      /* [n]    CellP.ConditionNumber (in: previous value, out: new) */
+    /* density outputs */
+    double *num_ngb;   /* [n]    P.NumNgb (after the ^(1/3) transform) */
+    double *drkern;    /* [n]    P.DrkernNgbFactor */
+    double *divvel;    /* [n]    P.Particle_DivVel */
+    double *rho;       /* [n]    CellP.Density */
+    double *pressure;  /* [n]    CellP.Pressure */
+    double *nvt;       /* [n][6] CellP.NV_T inverse, {xx,yy,zz,xy,yz,xz} */
+    double *fce;       /* [n]    CellP.FaceClosureError */
+    double *pvel;      /* [n][3] CellP.ParticleVel (MFV) */
+    int    *iters;     /* [n]    density iterations taken */
+    /* gradient outputs */
+    double *grad_rho;  /* [n][3] */
+    double *grad_p;    /* [n][3] */
+    double *grad_v;    /* [n][9] row k = d v_k / d x */
+    /* force outputs */
+    double *accel;     /* [n][3] CellP.HydroAccel */
+    double *dudt;      /* [n]    CellP.DtInternalEnergy */
+    double *vsig;      /* [n]    CellP.MaxSignalVel */
+    double *dtmass;    /* [n]    CellP.DtMass (MFV) */
+    double *dmass;     /* [n]    CellP.dMass (MFV) */
+    double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
+} orc_state;
+
+/* Neighbour sets in CSR form, original indices, each row sorted ascending. */
+typedef struct orc_csr {
+    long long *offsets;  /* [n_rows + 1] */
+    int       *nbrs;     /* [offsets[n_rows]] */
+    int        n_rows;
+} orc_csr;
+
+/* Runs the three passes (or one of them) on the active set (NULL = all).
+ * Return 0 on success or a reference stop code (1155 density did not
+ * converge, 90001009 empty bracket, 1234 no positive-pressure Riemann
+ * solution). n_threads <= 0 uses the OpenMP default. */
+int orc_density(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
+int orc_gradients(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
+int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
+
+/* Density sums at a fixed kernel length, no iteration: writes the raw
+ * accumulator of density_loop.h:1140-1385 for each active into acc[a][14]:
+ * {Ngb, Rho, DrkernNgb, DivVel, NV_T xx,yy,zz,xy,yz,xz, face x,y,z, 0}
+ * plus ParticleVel into pv[a][3] (MFV). */
+int orc_density_sums(const gz_params *p, const orc_state *s, const int *active, int n_active,
+                     double *acc, double *pv, int n_threads);
+
+/* Exact neighbour sets. mode 0: one-way r < h_i (density); mode 1:
+ * symmetric 0 < r and (r < h_i or r < h_j) (gradients, force).
+ * Rows follow the active list. Free with orc_csr_free. */
+int orc_neighbors(const gz_params *p, const orc_state *s, const int *active, int n_active,
+                  int mode, orc_csr *out, int n_threads);
+void orc_csr_free(orc_csr *c);
+
+/* One-time timing helper for the CPU baseline: runs density (from the
+ * given h seeds) -> gradients -> force on `n_active` targets and returns
+ * wall seconds. */
+double orc_full_pass_seconds(const gz_params *p, orc_state *s, const int *active, int n_active,
+                             int n_threads, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

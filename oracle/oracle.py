@@ -1,0 +1,196 @@
+"""Python binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle.so`` (the C restatement, gizmo_oracle.c) and the
+reference's own pair bodies compiled by ``oracle/build_ref.sh`` into
+``oracle/_ref/libgizmo_ref_<config>.so``. Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg use this module: it is the checker, never the
+thing measured or shipped.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from gizmo_b200.abi import GzParams, METHOD_MFM, METHOD_MFV
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+STATE_FIELDS = [  # (name, components, dtype)
+    ("pos", 3, np.float64), ("vel", 3, np.float64), ("mass", 1, np.float64), ("u", 1, np.float64),
+    ("dt", 1, np.float64), ("h", 1, np.float64), ("cond", 1, np.float64),
+    ("num_ngb", 1, np.float64), ("drkern", 1, np.float64), ("divvel", 1, np.float64),
+    ("rho", 1, np.float64), ("pressure", 1, np.float64), ("nvt", 6, np.float64), ("fce", 1, np.float64),
+    ("pvel", 3, np.float64), ("iters", 1, np.int32),
+    ("grad_rho", 3, np.float64), ("grad_p", 3, np.float64), ("grad_v", 9, np.float64),
+    ("accel", 3, np.float64), ("dudt", 1, np.float64), ("vsig", 1, np.float64),
+    ("dtmass", 1, np.float64), ("dmass", 1, np.float64), ("gravwork", 3, np.float64),
+]
+
+
+class OrcState(C.Structure):
+    _fields_ = [("n", C.c_int)] + [(name, _ip if dt == np.int32 else _dp) for name, _, dt in STATE_FIELDS]
+
+
+class OrcCsr(C.Structure):
+    _fields_ = [("offsets", C.POINTER(C.c_longlong)), ("nbrs", _ip), ("n_rows", C.c_int)]
+
+
+def new_state(n: int, inputs: dict) -> dict:
+    """All state arrays for n particles; `inputs` fills pos/vel/mass/u/dt/h/cond."""
+    st = {}
+    for name, k, dt in STATE_FIELDS:
+        shape = (n,) if k == 1 else (n, k)
+        st[name] = np.zeros(shape, dtype=dt)
+    for name, arr in inputs.items():
+        st[name][...] = arr
+    return st
+
+
+def _c_state(st: dict) -> OrcState:
+    s = OrcState()
+    s.n = int(st["pos"].shape[0])
+    for name, _, dt in STATE_FIELDS:
+        a = st[name]
+        assert a.flags["C_CONTIGUOUS"] and a.dtype == dt, name
+        setattr(s, name, a.ctypes.data_as(_ip if dt == np.int32 else _dp))
+    return s
+
+
+def build_oracle() -> None:
+    subprocess.run(["make", "-s", "liboracle.so"], cwd=HERE, check=True)
+
+
+def build_reference() -> None:
+    subprocess.run([os.path.join(HERE, "build_ref.sh")], check=True)
+
+
+def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
+    for name in ("density", "gradients", "force"):
+        f = getattr(lib, f"{prefix}_{name}")
+        f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int]
+        f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_density_sums")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, _dp, _dp, C.c_int]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_full_pass_seconds")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
+    f.restype = C.c_double
+    return lib
+
+
+_libs: dict = {}
+
+
+def ref_config_name(params: GzParams) -> str:
+    g = {5.0 / 3.0: "g53", 1.0001: "g1"}.get(float(params.gamma))
+    m = {METHOD_MFM: "mfm", METHOD_MFV: "mfv"}[params.method]
+    if g is None:
+        raise ValueError(f"no reference build for gamma={params.gamma}")
+    return f"{m}_k{params.kernel}_{g}"
+
+
+def ref_available(params: GzParams) -> bool:
+    try:
+        return os.path.exists(os.path.join(REF_DIR, f"libgizmo_ref_{ref_config_name(params)}.so"))
+    except ValueError:
+        return False
+
+
+class Oracle:
+    """The C restatement (kind='port') or the compiled reference (kind='reference')."""
+
+    def __init__(self, params: GzParams, kind: str = "port", n_threads: int = 0):
+        self.params = params
+        self.kind = kind
+        self.n_threads = n_threads
+        if kind == "port":
+            key = LIB_ORACLE
+            if key not in _libs:
+                if not os.path.exists(LIB_ORACLE):
+                    build_oracle()
+                _libs[key] = _setup(C.CDLL(LIB_ORACLE), "orc")
+            self.prefix = "orc"
+        elif kind == "reference":
+            key = os.path.join(REF_DIR, f"libgizmo_ref_{ref_config_name(params)}.so")
+            if key not in _libs:
+                if not os.path.exists(key):
+                    raise FileNotFoundError(key)
+                _libs[key] = _setup(C.CDLL(key), "ref")
+            self.prefix = "ref"
+        else:
+            raise ValueError(kind)
+        self.lib = _libs[key]
+
+    def _act(self, active):
+        if active is None:
+            return None, 0
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        return a, len(a)
+
+    def _run(self, name: str, st: dict, active=None) -> int:
+        a, na = self._act(active)
+        cs = _c_state(st)
+        f = getattr(self.lib, f"{self.prefix}_{name}")
+        return int(f(C.byref(self.params), C.byref(cs), a.ctypes.data_as(_ip) if a is not None else None, na,
+                     self.n_threads))
+
+    def density(self, st, active=None):
+        return self._run("density", st, active)
+
+    def gradients(self, st, active=None):
+        return self._run("gradients", st, active)
+
+    def force(self, st, active=None):
+        return self._run("force", st, active)
+
+    def density_sums(self, st, active=None):
+        a, na = self._act(active)
+        n_rows = na if a is not None else st["pos"].shape[0]
+        acc = np.zeros((n_rows, 14))
+        pv = np.zeros((n_rows, 3))
+        cs = _c_state(st)
+        f = getattr(self.lib, f"{self.prefix}_density_sums")
+        rc = f(C.byref(self.params), C.byref(cs), a.ctypes.data_as(_ip) if a is not None else None, na,
+               acc.ctypes.data_as(_dp), pv.ctypes.data_as(_dp), self.n_threads)
+        if rc:
+            raise RuntimeError(f"density_sums failed: {rc}")
+        return acc, pv
+
+    def full_pass_seconds(self, st, active=None):
+        a, na = self._act(active)
+        cs = _c_state(st)
+        status = C.c_int(0)
+        f = getattr(self.lib, f"{self.prefix}_full_pass_seconds")
+        t = f(C.byref(self.params), C.byref(cs), a.ctypes.data_as(_ip) if a is not None else None, na,
+              self.n_threads, C.byref(status))
+        return float(t), int(status.value)
+
+
+def neighbors(params: GzParams, st: dict, mode: int, active=None, n_threads: int = 0):
+    """Exact neighbour sets (CSR, original indices, sorted rows) from the C oracle."""
+    lib = Oracle(params, "port").lib
+    lib.orc_neighbors.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int,
+                                  C.POINTER(OrcCsr), C.c_int]
+    lib.orc_neighbors.restype = C.c_int
+    lib.orc_csr_free.argtypes = [C.POINTER(OrcCsr)]
+    a = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+    na = 0 if a is None else len(a)
+    cs = _c_state(st)
+    out = OrcCsr()
+    rc = lib.orc_neighbors(C.byref(params), C.byref(cs), a.ctypes.data_as(_ip) if a is not None else None, na, mode,
+                           C.byref(out), n_threads)
+    if rc:
+        raise RuntimeError(f"orc_neighbors failed: {rc}")
+    n_rows = out.n_rows
+    off = np.ctypeslib.as_array(out.offsets, shape=(n_rows + 1,)).astype(np.int64).copy()
+    nb = np.ctypeslib.as_array(out.nbrs, shape=(max(int(off[-1]), 1),))[: int(off[-1])].astype(np.int32).copy()
+    lib.orc_csr_free(C.byref(out))
+    return off, nb
