@@ -1,0 +1,390 @@
+"""Benchmark of the meshless hydro pass: particle-updates/s, mixed vs FP64 form.
+
+Workload (default): 256^3 = 16,777,216 gas particles, 90% in 1000 Plummer
+spheres + 10% uniform background (seeded synthetic stand-in for the named
+configuration), MFV with HLLC, cubic kernel, 32 neighbours, gamma 5/3.
+One step = one particle-update of every particle: neighbour grid rebuilt from
+the resident inputs, density with kernel-length iteration from the
+steady-state seed (converged h x (1 + U(-0.05, 0.05))), gradients, force.
+
+Arms:
+  (default)          the sm_100a library through its C ABI, device-resident
+                     inputs (`value`), plus the end-to-end rate with pinned host
+                     buffers copied in and results copied out every step (`e2e`).
+  --impl reference   the reference's own pair bodies (oracle/_ref, compiled from
+                     its sources) on the host cores; replicas only for N > 1
+                     (rank 0 runs, the others exit).
+
+Multi-GPU: replicas only (one independent particle set per GPU; the pass has
+no exchange on one box), weak scaling, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "hydro particle-updates/s @256^3: mixed-prec vs FP64 GPU at <=1e-5 rel err"
+UNIT = "particle-updates/s"
+
+# per-pair FLOP constants (FMA = 2, sqrt/div/exp/log = 1 each), counted by hand
+# over the taken MFV/MFM ideal-gas branch of the pair bodies (HLLC solved on the
+# first try): density ~40, gradient ~60, force ~430.
+FLOPS_PER_PAIR = {"density": 40.0, "gradients": 60.0, "force": 430.0}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plummer_mix", choices=["plummer_mix", "sedov", "lognormal"])
+    ap.add_argument("--n1", type=int, default=None, help="particles per axis (default: 256 plummer_mix)")
+    ap.add_argument("--cpu-n1", type=int, default=64, help="size of the CPU-baseline instance")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name: str, n1: int, precision: int):
+    from gizmo_b200 import ics
+
+    if name == "plummer_mix":
+        return ics.plummer_mix(n1, seed=4, precision=precision)
+    if name == "sedov":
+        return ics.sedov(n1, seed=1, precision=precision)
+    return ics.lognormal(n1, seed_density=2, seed_velocity=3, precision=precision)
+
+
+def default_n1(name: str) -> int:
+    return {"plummer_mix": 256, "sedov": 32, "lognormal": 128}[name]
+
+
+def workload_desc(name: str, n1: int) -> str:
+    n = n1 ** 3
+    return {
+        "plummer_mix": f"{n1}^3={n:,} particles: 90% in 1000 Plummer spheres + 10% background, MFV+HLLC, cubic, 32 ngb",
+        "sedov": f"{n1}^3={n:,} particles: Sedov lattice+jitter, MFM, cubic, 32 ngb",
+        "lognormal": f"{n1}^3={n:,} particles: log-normal field sigma_lnrho=1.5, MFM, Wendland C2, 64 ngb",
+    }[name]
+
+
+# --------------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if (args.impl == "ours" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int, impl: str) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if (impl == "ours" and torch.cuda.is_available()) else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def dist_done(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, device: int):
+        self.path = tempfile.mktemp(prefix="gz_clocks_", suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_baseline(n1: int, name: str, kind_pref: str = "reference", steps: int = 1):
+    """Full CPU pass (density -> gradients -> force) of a smaller instance of the
+    same generator on all host threads; returns (rate, seconds, kind, cores, n)."""
+    from oracle import oracle as O
+
+    wl = make_workload(name, n1, 0)
+    kind = kind_pref if (kind_pref == "port" or O.ref_available(wl.params)) else "port"
+    cores = os.cpu_count() or 1
+    orc = O.Oracle(wl.params, kind, n_threads=cores)
+    times = []
+    for _ in range(steps):
+        st = O.new_state(wl.n, wl.inputs())
+        t, status = orc.full_pass_seconds(st)
+        if status:
+            raise RuntimeError(f"CPU pass failed: {status}")
+        times.append(t)
+    t = float(np.mean(times))
+    return wl.n / t, t, kind, cores, wl.n
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args, world, rank, local):
+    import torch
+
+    from gizmo_b200 import abi, ics
+    from gizmo_b200.hydro import HydroPass
+
+    torch.cuda.set_device(local)
+    n1 = args.n1 or default_n1(args.workload)
+    t_gen = time.time()
+    wl = make_workload(args.workload, n1, abi.PRECISION_FP64)
+    N = wl.n
+    t_gen = time.time() - t_gen
+    # steady-state seed: converge once in FP64 from the cold seed
+    hp64 = HydroPass(wl.params, device=local)
+    hp64.upload_workload(wl)
+    hp64.density()
+    conv = hp64.download(["h", "cond"])
+    wl.h = ics.steady_state_seed(conv["h"], 4)
+    wl.cond = conv["cond"]
+    hp64.upload_workload(wl)
+    from gizmo_b200.ics import make_params
+
+    p = wl.params
+    pmix = make_params(p.kernel, p.method, p.gamma, p.des_num_ngb, p.max_num_ngb_dev, abi.PRECISION_MIXED,
+                       p.box_size, p.first_step, p.selfgravity_off, p.min_kernel_radius, p.max_kernel_radius)
+    hpm = HydroPass(pmix, device=local)
+    hpm.upload_workload(wl)
+
+    def run_steps(hp, K, W, record_clock=False):
+        stream = torch.cuda.ExternalStream(hp.stream)
+        for _ in range(W):
+            hp.restage()
+            hp.full_pass()
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if record_clock else None
+        l0 = hp.status()["kernel_launches"]
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+        for k in range(K):
+            ev[k][0].record(stream)
+            hp.restage()
+            ev[k][1].record(stream)
+            hp.density()
+            ev[k][2].record(stream)
+            hp.hydro_gradient_calc()
+            ev[k][3].record(stream)
+            hp.hydro_force()
+            ev[k][4].record(stream)
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        launches = hp.status()["kernel_launches"] - l0
+        total = ev[0][0].elapsed_time(ev[K - 1][4]) / 1e3
+        parts = {nm: float(np.mean([ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(K)])) / 1e3
+                 for i, nm in enumerate(["grid", "density", "gradients", "force"])}
+        return total, parts, clocks, launches
+
+    K, W = args.steps, args.warmup
+    t_mix, parts_mix, clocks, launches = run_steps(hpm, K, W, record_clock=True)
+    st_mix = hpm.status()
+    t_64, parts_64, _, _ = run_steps(hp64, max(1, min(K, 3)), max(1, min(W, 2)))
+    K64 = max(1, min(K, 3))
+    t_mix = dist_max(t_mix, world, "ours")
+    t_64 = dist_max(t_64, world, "ours")
+    value = world * N * K / t_mix
+    value64 = world * N * K64 / t_64
+
+    # accuracy of the mixed form against the FP64 form (same inputs)
+    fields = ["h", "rho", "pressure", "grad_rho", "grad_p", "grad_v", "accel", "dudt", "dtmass", "vsig"]
+    om = hpm.download(fields + ["iters"])
+    o64 = hp64.download(fields + ["iters"])
+    acc = {}
+    for f in fields:
+        a, b = om[f], o64[f]
+        rowa = np.linalg.norm(a.reshape(N, -1), axis=1)
+        rowb = np.linalg.norm(b.reshape(N, -1), axis=1)
+        d = np.linalg.norm((a - b).reshape(N, -1), axis=1)
+        floor = 1e-3 * rowb.max() if f not in ("h", "rho", "pressure", "vsig") else 0.0
+        rel = d / np.maximum(rowb, floor + 1e-300)
+        acc[f] = {"max": float(rel.max()), "p99": float(np.percentile(rel, 99)),
+                  "p50": float(np.median(rel)), "norm": float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300))}
+        del rowa
+    acc["iters_equal_frac"] = float(np.mean(om["iters"] == o64["iters"]))
+    # conservation per pass (both forms)
+    cons = {}
+    for tag, o in (("mixed", om), ("fp64", o64)):
+        m, v = wl.mass, wl.vel
+        dtm = o["dtmass"] if p.method == abi.METHOD_MFV else np.zeros(N)
+        mom = m[:, None] * o["accel"] + v * dtm[:, None]
+        cons[tag] = {"momentum": float(np.abs(mom.sum(0)).max() / np.abs(mom).sum()),
+                     "mass": float(abs(dtm.sum()) / (np.abs(dtm).sum() + 1e-300))}
+
+    # roofline of the dominant kernel (force): algorithmic FLOPs / event time
+    pairs_sym = st_mix["pairs_symmetric"]
+    t_force = parts_mix["force"]
+    achieved = FLOPS_PER_PAIR["force"] * pairs_sym / t_force / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * t_mix / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair / f64 accumulate", "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": workload_desc(args.workload, n1), "n_particles": N, "precision": "mixed",
+                   "h_seed": "steady-state: FP64-converged h x (1+U(-0.05,0.05)), seed 104",
+                   "l2": f"inputs larger than L2 (device state {st_mix['device_bytes'] / 1e9:.1f} GB)",
+                   "parallelism": f"replicas x{world}", "generate_s": round(t_gen, 1)},
+        "fp64_value": value64, "mixed_over_fp64": value / value64,
+        "pass_seconds": {"mixed": parts_mix, "fp64": parts_64},
+        "accuracy_mixed_vs_fp64": acc, "conservation": cons,
+        "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
+        "gpu_launches": launches, "clocks": clocks,
+        "roofline": {"kernel": "k_force<float> (MFV pair flux)", "bound": "fp32",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "peak_source": f"nominal FP32 pipe: 148 SM x 128 lanes x 2 x {sm_mhz:.0f} MHz "
+                                    "(no measured FP32 figure in MEASURED_PEAKS.json)",
+                     "flops_per_pair": FLOPS_PER_PAIR["force"], "traffic": None},
+    }
+
+    # end to end: pinned host buffers in, results out, every step
+    if not args.skip_e2e:
+        pin = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory()
+               for k, v in wl.inputs().items()}
+        outs = {"h": (N,), "rho": (N,), "accel": (N, 3), "dudt": (N,), "vsig": (N,), "dtmass": (N,), "dmass": (N,)}
+        pout = {k: torch.empty(s, dtype=torch.float64, pin_memory=True) for k, s in outs.items()}
+        stream = torch.cuda.ExternalStream(hpm.stream)
+        for _ in range(max(1, min(W, 2))):
+            hpm.upload_raw(N, {k: t.data_ptr() for k, t in pin.items()})
+            hpm.full_pass()
+            hpm.download_raw({k: t.data_ptr() for k, t in pout.items()})
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        Ke = max(1, min(K, 3))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(Ke):
+            hpm.upload_raw(N, {k: t.data_ptr() for k, t in pin.items()})
+            hpm.full_pass()
+            hpm.download_raw({k: t.data_ptr() for k, t in pout.items()})
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = dist_max(e0.elapsed_time(e1) / 1e3, world, "ours")
+        h2d = sum(t.numel() * 8 for t in pin.values())
+        d2h = sum(t.numel() * 8 for t in pout.values())
+        result["e2e"] = {"value": world * N * Ke / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                         "d2h_bytes_per_step": d2h, "steps": Ke}
+    hpm.close()
+    hp64.close()
+
+    if rank == 0 and not args.skip_cpu:
+        rate, secs, kind, cores, ncpu = cpu_baseline(args.cpu_n1, args.workload)
+        result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                  "sample": f"one full density->gradients->force pass of a {args.cpu_n1}^3 "
+                                            f"({ncpu:,}-particle) instance of the same generator, {secs:.2f} s"}
+    return result
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    n1 = args.cpu_n1
+    for _ in range(args.warmup):
+        cpu_baseline(n1, args.workload, "reference", 1)
+    t0 = time.time()
+    rate, secs, kind, cores, ncpu = cpu_baseline(n1, args.workload, "reference", args.steps)
+    wall = time.time() - t0
+    sample = f"{args.steps} full passes of a {n1}^3 ({ncpu:,}-particle) instance of the same generator"
+    return {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator, no dataset)", "impl": "reference",
+        "config": {"workload": workload_desc(args.workload, n1), "n_particles": ncpu, "precision": "fp64",
+                   "parallelism": "host threads", "wall_s": round(wall, 1)},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, world, rank)
+        else:
+            res = run_ours(args, world, rank, local)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        dist_done(world)
+
+
+if __name__ == "__main__":
+    main()

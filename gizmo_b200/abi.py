@@ -83,12 +83,13 @@ class GzStatusInfo(C.Structure):
         ("pairs_density", C.c_int64),
         ("pairs_symmetric", C.c_int64),
         ("device_bytes", C.c_int64),
+        ("kernel_launches", C.c_int64),
         ("message", C.c_char * 256),
     ]
 
 
 EXPORTED_SYMBOLS = [
-    "gz_create", "gz_destroy", "gz_set_params", "gz_upload", "gz_hydro_density",
+    "gz_create", "gz_destroy", "gz_set_params", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream",
     "gz_neighbors", "gz_density_sums",
 ]
@@ -115,6 +116,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_destroy.argtypes = [vp]
     lib.gz_set_params.argtypes = [vp, C.POINTER(GzParams)]
     lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
+    lib.gz_restage.argtypes = [vp]
     for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):
         getattr(lib, name).argtypes = [vp, _ip, C.c_int]
     lib.gz_download.argtypes = [vp, C.POINTER(GzOutputs)]

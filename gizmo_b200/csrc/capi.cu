@@ -1,0 +1,842 @@
+// gizmo_b200/csrc/capi.cu -- the C ABI (include/gizmo_hydro.h): context,
+// device-resident particle mirror, and the pass orchestration that replaces
+// run_neighbor_loop_iterative<DensitySpec>, run_neighbor_loop<GradientsSpec>
+// and run_neighbor_loop<HydroForceSpec> (src/mesh/neighbor_loop_runner.h:1614-1629)
+// inside density() / hydro_gradient_calc() / hydro_force().
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gizmo_hydro.h"
+#include "launch.h"
+
+using namespace gz;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+constexpr double kDensityBuffer = 1.3;  // DensitySpec::mode_a_csr_buffer_factor, density_loop.h:316
+
+}  // namespace
+
+struct gz_context {
+    gz_params prm{};
+    PassParams pp{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0;
+    // sorted SoA mirror
+    DevBuf x, y, z, vx, vy, vz, m, u, dt, h, cond, num_ngb, drkern, divvel, rho, pressure, fce, nvt, pv, grad, accel,
+        dudt, vsig, dtmass, dmass, gw, iters, active;
+    // original-order staging and permutation
+    DevBuf stage, stage3, perm, inv, keys, keys_sorted, idx, cub_tmp, targets_orig, targets, targets_tmp;
+    // resident copies of the uploaded inputs, original order (gz_restage source)
+    DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
+    long long launches = 0;          // kernels of this library launched by the context
+    // grid
+    int F = 1;
+    DevBuf cell_start, hmax;
+    long long level_off[12] = {0};
+    bool grid_valid = false;
+    // density work
+    DevBuf acc, h_built, scratch, keep, todo_a, todo_b, row_of, flag, counts, d_off, d_nbr, n_sel;
+    long long d_nbr_cap = 0;
+    // symmetric rows (shared by gradients and force)
+    DevBuf s_off, s_nbr, s_counts;
+    long long s_nbr_cap = 0;
+    int sym_rows = 0;
+    bool sym_valid = false;
+    std::vector<int> sym_active;     // active list the symmetric rows were built for
+    bool sym_all = false;            // ... or all particles
+    DevBuf status;
+    // host record
+    int err = 0, err_index = -1;
+    char msg[256] = {0};
+    int last_iters = 0;
+    long long pairs_density = 0, pairs_symmetric = 0;
+    bool have_density = false, have_gradients = false;
+    int tpt_density = 16, tpt_gradient = 16, tpt_force = 8;
+};
+
+namespace {
+
+int fail(gz_context *c, int code, const char *what)
+{
+    if (c) {
+        if (!c->err) { c->err = code; }
+        snprintf(c->msg, sizeof(c->msg), "%s", what);
+    }
+    return code;
+}
+
+#define GZ_CUDA(ctx, call)                                                                \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            char b_[200];                                                                 \
+            snprintf(b_, sizeof(b_), "%s: %s", #call, cudaGetErrorString(e_));            \
+            return fail(ctx, GZ_ERR_CUDA, b_);                                            \
+        }                                                                                 \
+    } while (0)
+
+template <typename T> T *ptr(DevBuf &b) { return (T *)b.p; }
+
+int ensure(gz_context *c, DevBuf &b, size_t bytes)
+{
+    if (b.bytes >= bytes && b.p) return 0;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes > 0 ? bytes : 16;
+    GZ_CUDA(c, cudaMalloc(&b.p, want));
+    b.bytes = want;
+    return 0;
+}
+
+void release(DevBuf &b)
+{
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+PassParams make_pass_params(const gz_params &p)
+{
+    PassParams q{};
+    q.kernel = p.kernel;
+    q.method = p.method;
+    q.first_step = p.first_step;
+    q.selfgravity_off = p.selfgravity_off;
+    q.box = p.box_size;
+    q.half = 0.5 * p.box_size;
+    q.gamma = p.gamma;
+    q.des_num_ngb = p.des_num_ngb;
+    q.max_num_ngb_dev = p.max_num_ngb_dev;
+    q.min_kernel_radius = p.min_kernel_radius;
+    q.max_kernel_radius = p.max_kernel_radius;
+    return q;
+}
+
+int check_params(const gz_params *p)
+{
+    if (!p) return GZ_ERR_ARG;
+    if (p->kernel != GZ_KERNEL_CUBIC && p->kernel != GZ_KERNEL_WENDLAND_C2) return GZ_ERR_ARG;
+    if (p->method != GZ_METHOD_MFM && p->method != GZ_METHOD_MFV) return GZ_ERR_ARG;
+    if (p->precision != GZ_PRECISION_FP64 && p->precision != GZ_PRECISION_MIXED) return GZ_ERR_ARG;
+    if (!(p->box_size > 0) || !(p->gamma > 1.0) || !(p->des_num_ngb > 0)) return GZ_ERR_ARG;
+    return GZ_OK;
+}
+
+Particles view(gz_context *c)
+{
+    Particles ps{};
+    ps.n = c->n;
+    ps.x = ptr<double>(c->x); ps.y = ptr<double>(c->y); ps.z = ptr<double>(c->z);
+    ps.vx = ptr<double>(c->vx); ps.vy = ptr<double>(c->vy); ps.vz = ptr<double>(c->vz);
+    ps.m = ptr<double>(c->m); ps.u = ptr<double>(c->u); ps.dt = ptr<double>(c->dt);
+    ps.h = ptr<double>(c->h); ps.cond = ptr<double>(c->cond);
+    ps.num_ngb = ptr<double>(c->num_ngb); ps.drkern = ptr<double>(c->drkern); ps.divvel = ptr<double>(c->divvel);
+    ps.rho = ptr<double>(c->rho); ps.pressure = ptr<double>(c->pressure); ps.fce = ptr<double>(c->fce);
+    ps.nvt = ptr<double>(c->nvt); ps.pv = ptr<double>(c->pv); ps.grad = ptr<double>(c->grad);
+    ps.accel = ptr<double>(c->accel); ps.dudt = ptr<double>(c->dudt); ps.vsig = ptr<double>(c->vsig);
+    ps.dtmass = ptr<double>(c->dtmass); ps.dmass = ptr<double>(c->dmass); ps.gw = ptr<double>(c->gw);
+    ps.iters = ptr<int>(c->iters);
+    ps.active = ptr<unsigned char>(c->active);
+    return ps;
+}
+
+Grid grid_view(gz_context *c)
+{
+    Grid g{};
+    g.F = c->F;
+    g.box = c->prm.box_size;
+    g.cell_start = ptr<int>(c->cell_start);
+    g.hmax = ptr<double>(c->hmax);
+    for (int k = 0; k < 12; k++) g.level_off[k] = c->level_off[k];
+    return g;
+}
+
+// ---------------------------------------------------------------- kernels
+__global__ void k_gather_inputs(int n, const int *__restrict__ perm, const double *__restrict__ pos,
+                                const double *__restrict__ vel, double *x, double *y, double *z, double *vx,
+                                double *vy, double *vz)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const size_t o = (size_t)perm[s];
+    x[s] = pos[3 * o]; y[s] = pos[3 * o + 1]; z[s] = pos[3 * o + 2];
+    vx[s] = vel[3 * o]; vy[s] = vel[3 * o + 1]; vz[s] = vel[3 * o + 2];
+}
+
+__global__ void k_gather1(int n, const int *__restrict__ perm, const double *__restrict__ src, double *dst)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[s] = src[perm[s]];
+}
+
+__global__ void k_inverse(int n, const int *__restrict__ perm, int *inv)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) inv[perm[s]] = s;
+}
+
+// sorted field (component-major [k][n]) -> original order row-major [n][k]
+__global__ void k_scatter_out(int n, int k, const int *__restrict__ perm, const double *__restrict__ src, double *dst)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)n * k) return;
+    const int s = (int)(e / k), c = (int)(e % k);
+    dst[(size_t)perm[s] * k + c] = src[(size_t)c * n + s];
+}
+
+__global__ void k_scatter_int(int n, const int *__restrict__ perm, const int *__restrict__ src, int *dst)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[perm[s]] = src[s];
+}
+
+__global__ void k_map_targets(int na, const int *__restrict__ orig, const int *__restrict__ inv, int *out, int n,
+                              DevStatus *st)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= na) return;
+    const int o = orig[a];
+    if (o < 0 || o >= n) { record_status(st, GZ_ERR_ARG, o); out[a] = 0; return; }
+    out[a] = inv[o];
+}
+
+__global__ void k_iota(int n, int *out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[s] = s;
+}
+
+__global__ void k_set_active(int na, const int *__restrict__ t, unsigned char *flag)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < na) flag[t[a]] = 1;
+}
+
+__global__ void k_density_prep(int na, const int *__restrict__ t, double *h, double maxsoft, DensityScratch *sc,
+                               int *row_of)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= na) return;
+    const int i = t[a];
+    double hv = h[i];
+    if ((hv < 0) || !isfinite(hv) || (hv > 0.99 * maxsoft)) hv = 0.99 * maxsoft;  // density_loop.cc:837-840
+    h[i] = hv;
+    DensityScratch z{};
+    sc[i] = z;
+    row_of[i] = a;
+}
+
+__global__ void k_rows_of(int na, const int *__restrict__ t, int *row_of, const double *__restrict__ h, double f,
+                          double *h_built)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= na) return;
+    const int i = t[a];
+    row_of[i] = a;
+    h_built[i] = h[i] * f;
+}
+
+// ------------------------------------------------------------ host helpers
+int sort_targets(gz_context *c, const int *active, int n_active, int *n_out)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    if (!active) {
+        if (ensure(c, c->targets, sizeof(int) * (size_t)std::max(n, 1))) return c->err;
+        if (n > 0) { k_iota<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->targets)); c->launches++; }
+        *n_out = n;
+    } else {
+        if (n_active < 0 || n_active > n) return fail(c, GZ_ERR_ARG, "n_active out of range");
+        const size_t na = (size_t)std::max(n_active, 1);
+        if (ensure(c, c->targets_orig, sizeof(int) * na) || ensure(c, c->targets_tmp, sizeof(int) * na) ||
+            ensure(c, c->targets, sizeof(int) * na))
+            return c->err;
+        GZ_CUDA(c, cudaMemcpyAsync(c->targets_orig.p, active, sizeof(int) * (size_t)n_active, cudaMemcpyHostToDevice, s));
+        if (n_active > 0) {
+            k_map_targets<<<(n_active + 255) / 256, 256, 0, s>>>(n_active, ptr<int>(c->targets_orig), ptr<int>(c->inv),
+                                                                 ptr<int>(c->targets_tmp), n, ptr<DevStatus>(c->status));
+            c->launches++;
+        }
+        size_t tmp = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tmp, ptr<int>(c->targets_tmp), ptr<int>(c->targets), n_active, 0, 32, s);
+        if (ensure(c, c->cub_tmp, tmp)) return c->err;
+        cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, tmp, ptr<int>(c->targets_tmp), ptr<int>(c->targets), n_active, 0,
+                                       32, s);
+        *n_out = n_active;
+    }
+    GZ_CUDA(c, cudaMemsetAsync(c->active.p, 0, (size_t)std::max(n, 1), s));
+    if (*n_out > 0) {
+        k_set_active<<<(*n_out + 255) / 256, 256, 0, s>>>(*n_out, ptr<int>(c->targets), ptr<unsigned char>(c->active));
+        c->launches++;
+    }
+    return 0;
+}
+
+int exclusive_scan_counts(gz_context *c, int rows, DevBuf &counts, DevBuf &off, long long *total)
+{
+    cudaStream_t s = c->stream;
+    if (ensure(c, off, sizeof(long long) * (size_t)(rows + 1))) return c->err;
+    GZ_CUDA(c, cudaMemsetAsync(off.p, 0, sizeof(long long), s));
+    if (rows > 0) {
+        size_t tmp = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, tmp, ptr<int>(counts), ptr<long long>(off) + 1, rows, s);
+        if (ensure(c, c->cub_tmp, tmp)) return c->err;
+        cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, ptr<int>(counts), ptr<long long>(off) + 1, rows, s);
+    }
+    GZ_CUDA(c, cudaMemcpyAsync(total, ptr<long long>(off) + rows, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    return 0;
+}
+
+int build_rows(gz_context *c, const double *reach, int symmetric, const int *targets, int rows, DevBuf &counts,
+               DevBuf &off, DevBuf &nbr, long long &cap, long long *total)
+{
+    cudaStream_t s = c->stream;
+    Grid g = grid_view(c);
+    if (ensure(c, counts, sizeof(int) * (size_t)std::max(rows, 1))) return c->err;
+    walk_rows(g, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+              rows, ptr<int>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), s);
+    if (rows > 0) c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
+    if (*total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
+    if (*total > cap || !nbr.p) {
+        if (ensure(c, nbr, sizeof(int) * (size_t)std::max(*total, 1ll))) return c->err;
+        cap = (long long)(nbr.bytes / sizeof(int));
+    }
+    walk_rows(g, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+              rows, ptr<int>(counts), ptr<long long>(off), ptr<int>(nbr), ptr<DevStatus>(c->status), s);
+    if (rows > 0) c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+int read_status(gz_context *c)
+{
+    DevStatus h{};
+    GZ_CUDA(c, cudaMemcpyAsync(&h, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    GZ_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (h.code && !c->err) {
+        c->err = h.code;
+        c->err_index = h.index;
+        snprintf(c->msg, sizeof(c->msg), "device status %d at sorted index %d", h.code, h.index);
+    }
+    return h.code;
+}
+
+int build_grid(gz_context *c)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    int F = 1;
+    while (F < 10 && (1ll << (3 * F)) * 2 < (long long)n) F++;
+    c->F = F;
+    const long long ncell = 1ll << (3 * F);
+    long long total = 0;
+    for (int L = 0; L <= F; L++) { c->level_off[L] = total; total += 1ll << (3 * L); }
+    if (ensure(c, c->keys, sizeof(uint32_t) * (size_t)std::max(n, 1)) ||
+        ensure(c, c->keys_sorted, sizeof(uint32_t) * (size_t)std::max(n, 1)) ||
+        ensure(c, c->idx, sizeof(int) * (size_t)std::max(n, 1)) ||
+        ensure(c, c->cell_start, sizeof(int) * (size_t)(ncell + 1)) || ensure(c, c->hmax, sizeof(double) * (size_t)total))
+        return c->err;
+    grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, F, ptr<uint32_t>(c->keys), ptr<int>(c->idx), s);
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, ptr<uint32_t>(c->keys), ptr<uint32_t>(c->keys_sorted), ptr<int>(c->idx),
+                                    ptr<int>(c->perm), n, 0, 3 * F, s);
+    if (ensure(c, c->cub_tmp, tmp)) return c->err;
+    cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, ptr<uint32_t>(c->keys), ptr<uint32_t>(c->keys_sorted),
+                                    ptr<int>(c->idx), ptr<int>(c->perm), n, 0, 3 * F, s);
+    grid_cell_start(n, ptr<uint32_t>(c->keys_sorted), F, ptr<int>(c->cell_start), s);
+    if (n > 0) k_inverse<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->inv));
+    GZ_CUDA(c, cudaGetLastError());
+    c->grid_valid = true;
+    return 0;
+}
+
+int refresh_hmax(gz_context *c)
+{
+    grid_hmax(c->n, ptr<uint32_t>(c->keys_sorted), ptr<double>(c->h), c->F, ptr<double>(c->hmax), c->level_off,
+              c->stream);
+    c->launches += (c->n > 0 ? 1 : 0) + c->F;
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+int build_sym_rows(gz_context *c, int rows)
+{
+    if (refresh_hmax(c)) return c->err;
+    long long total = 0;
+    if (build_rows(c, ptr<double>(c->h), 1, ptr<int>(c->targets), rows, c->s_counts, c->s_off, c->s_nbr, c->s_nbr_cap,
+                   &total))
+        return c->err;
+    c->pairs_symmetric = total;
+    c->sym_rows = rows;
+    c->sym_valid = true;
+    return 0;
+}
+
+}  // namespace
+
+// ===================================================================== ABI
+extern "C" {
+
+int gz_create(const gz_params *params, int device, gz_context **out)
+{
+    if (!out) return GZ_ERR_ARG;
+    *out = nullptr;
+    if (check_params(params)) return GZ_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return GZ_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return GZ_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return GZ_ERR_CUDA;
+    gz_context *c = new (std::nothrow) gz_context();
+    if (!c) return GZ_ERR_CAPACITY;
+    c->prm = *params;
+    c->pp = make_pass_params(*params);
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return GZ_ERR_CUDA; }
+    if (ensure(c, c->status, sizeof(DevStatus))) { cudaStreamDestroy(c->stream); delete c; return GZ_ERR_CUDA; }
+    cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
+    *out = c;
+    return GZ_OK;
+}
+
+int gz_destroy(gz_context *c)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf *all[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
+                     &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
+                     &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
+                     &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
+                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->acc, &c->h_built, &c->scratch,
+                     &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
+                     &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
+                     &c->o_dt, &c->o_h, &c->o_cond};
+    for (DevBuf *b : all) release(*b);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return GZ_OK;
+}
+
+int gz_set_params(gz_context *c, const gz_params *params)
+{
+    if (!c || check_params(params)) return GZ_ERR_ARG;
+    const bool box_changed = params->box_size != c->prm.box_size;
+    c->prm = *params;
+    c->pp = make_pass_params(*params);
+    if (box_changed) c->grid_valid = false;
+    return GZ_OK;
+}
+
+void *gz_stream(gz_context *c) { return c ? (void *)c->stream : nullptr; }
+
+// Rebuild the neighbour grid and the sorted mirror from the resident inputs
+// (the state a pass starts from): Morton keys, radix sort, gathers, zeroed
+// outputs.
+static int stage_inputs(gz_context *c)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    GZ_CUDA(c, cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
+    c->err = 0;
+    c->err_index = -1;
+    c->msg[0] = 0;
+    if (n > 0) {
+        if (build_grid(c)) return c->err;
+        c->launches += 3;  // keys, cell starts, inverse permutation
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        k_gather_inputs<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->stage3), ptr<double>(c->o_vel),
+                                               ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z),
+                                               ptr<double>(c->vx), ptr<double>(c->vy), ptr<double>(c->vz));
+        c->launches += 1;
+        struct { DevBuf *src; DevBuf *dst; } one_in[] = {
+            {&c->o_mass, &c->m}, {&c->o_u, &c->u}, {&c->o_dt, &c->dt}, {&c->o_h, &c->h}, {&c->o_cond, &c->cond}};
+        for (auto &f : one_in) {
+            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(*f.src), ptr<double>(*f.dst));
+            c->launches += 1;
+        }
+        DevBuf *zero[] = {&c->num_ngb, &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig,
+                          &c->dtmass, &c->dmass};
+        for (DevBuf *b : zero) GZ_CUDA(c, cudaMemsetAsync(b->p, 0, sizeof(double) * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->nvt.p, 0, sizeof(double) * 6 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->pv.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->grad.p, 0, sizeof(double) * 15 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->accel.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->gw.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->iters.p, 0, sizeof(int) * (size_t)n, s));
+        GZ_CUDA(c, cudaGetLastError());
+    }
+    c->have_density = c->have_gradients = false;
+    c->sym_valid = false;
+    return 0;
+}
+
+int gz_upload(gz_context *c, const gz_particles *in)
+{
+    if (!c || !in || in->n < 0 || in->n > INT32_MAX / 16) return GZ_ERR_ARG;
+    if (in->n > 0 && (!in->pos || !in->vel || !in->mass || !in->u || !in->dt || !in->h)) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    const int n = (int)in->n;
+    c->n = n;
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)std::max(n, 1);
+    DevBuf *one[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
+                     &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig, &c->dtmass,
+                     &c->dmass, &c->h_built, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond};
+    for (DevBuf *b : one)
+        if (ensure(c, *b, sizeof(double) * N)) return c->err;
+    if (ensure(c, c->nvt, sizeof(double) * 6 * N) || ensure(c, c->pv, sizeof(double) * 3 * N) ||
+        ensure(c, c->grad, sizeof(double) * 15 * N) || ensure(c, c->accel, sizeof(double) * 3 * N) ||
+        ensure(c, c->gw, sizeof(double) * 3 * N) || ensure(c, c->iters, sizeof(int) * N) ||
+        ensure(c, c->active, N) || ensure(c, c->stage, sizeof(double) * 3 * N) ||
+        ensure(c, c->stage3, sizeof(double) * 3 * N) || ensure(c, c->o_vel, sizeof(double) * 3 * N) ||
+        ensure(c, c->perm, sizeof(int) * N) || ensure(c, c->inv, sizeof(int) * N) ||
+        ensure(c, c->acc, sizeof(double) * 17 * N) || ensure(c, c->scratch, sizeof(DensityScratch) * N) ||
+        ensure(c, c->row_of, sizeof(int) * N))
+        return c->err;
+    if (n > 0) {
+        GZ_CUDA(c, cudaMemcpyAsync(c->stage3.p, in->pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
+        GZ_CUDA(c, cudaMemcpyAsync(c->o_vel.p, in->vel, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
+        struct { const double *src; DevBuf *dst; } f1[] = {
+            {in->mass, &c->o_mass}, {in->u, &c->o_u}, {in->dt, &c->o_dt}, {in->h, &c->o_h}, {in->cond, &c->o_cond}};
+        for (auto &f : f1) {
+            if (f.src) GZ_CUDA(c, cudaMemcpyAsync(f.dst->p, f.src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+            else GZ_CUDA(c, cudaMemsetAsync(f.dst->p, 0, sizeof(double) * (size_t)n, s));
+        }
+    }
+    if (stage_inputs(c)) return c->err;
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    return c->err;
+}
+
+int gz_restage(gz_context *c)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid && c->n > 0) return fail(c, GZ_ERR_ORDER, "restage before upload");
+    if (stage_inputs(c)) return c->err;
+    return GZ_OK;
+}
+
+int gz_hydro_density(gz_context *c, const int *active, int n_active)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "density before upload");
+    cudaStream_t s = c->stream;
+    int na = 0;
+    if (sort_targets(c, active, n_active, &na)) return c->err;
+    Particles ps = view(c);
+    const int n = c->n;
+    if (ensure(c, c->todo_a, sizeof(int) * (size_t)std::max(na, 1)) ||
+        ensure(c, c->todo_b, sizeof(int) * (size_t)std::max(na, 1)) ||
+        ensure(c, c->keep, (size_t)std::max(na, 1)) || ensure(c, c->flag, sizeof(int)) ||
+        ensure(c, c->n_sel, sizeof(int)))
+        return c->err;
+    if (na > 0) {
+        k_density_prep<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<double>(c->h),
+                                                         c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch),
+                                                         ptr<int>(c->row_of));
+        c->launches++;
+    }
+    GZ_CUDA(c, cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToDevice, s));
+    int n_todo = na;
+    int *todo = ptr<int>(c->todo_a), *todo_next = ptr<int>(c->todo_b);
+    bool need_rows = true;
+    int iter = 0;
+    for (iter = 0; iter < kMaxIter && n_todo > 0; iter++) {
+        if (need_rows) {
+            // rows for every still-iterating particle at the buffered radius
+            k_rows_of<<<(n_todo + 255) / 256, 256, 0, s>>>(n_todo, todo, ptr<int>(c->row_of), ptr<double>(c->h),
+                                                            kDensityBuffer, ptr<double>(c->h_built));
+            c->launches++;
+            long long total = 0;
+            if (build_rows(c, ptr<double>(c->h_built), 0, todo, n_todo, c->counts, c->d_off, c->d_nbr, c->d_nbr_cap,
+                           &total))
+                return c->err;
+            need_rows = false;
+        }
+        DensityWork w{};
+        w.todo = todo;
+        w.n_todo = n_todo;
+        w.row_of = ptr<int>(c->row_of);
+        w.rows.off = ptr<long long>(c->d_off);
+        w.rows.nbr = ptr<int>(c->d_nbr);
+        w.acc = ptr<double>(c->acc);
+        w.h_built = ptr<double>(c->h_built);
+        w.scratch = ptr<DensityScratch>(c->scratch);
+        w.keep = ptr<unsigned char>(c->keep);
+        w.rebuild = ptr<int>(c->flag);
+        w.iter = iter;
+        GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
+        if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
+        else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);
+        density_after_iter(c->pp, ps, w, ptr<DevStatus>(c->status), s);
+        c->launches += 2;
+        GZ_CUDA(c, cudaGetLastError());
+        size_t tmp = 0;
+        cub::DeviceSelect::Flagged(nullptr, tmp, todo, ptr<unsigned char>(c->keep), todo_next, ptr<int>(c->n_sel), n_todo, s);
+        if (ensure(c, c->cub_tmp, tmp)) return c->err;
+        cub::DeviceSelect::Flagged(c->cub_tmp.p, tmp, todo, ptr<unsigned char>(c->keep), todo_next, ptr<int>(c->n_sel),
+                                   n_todo, s);
+        int hv[2] = {0, 0};
+        GZ_CUDA(c, cudaMemcpyAsync(&hv[0], c->n_sel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaMemcpyAsync(&hv[1], c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+        n_todo = hv[0];
+        need_rows = hv[1] != 0;
+        std::swap(todo, todo_next);
+    }
+    c->last_iters = iter;
+    density_finalize(c->pp, ps, ptr<double>(c->acc), ptr<int>(c->targets), na, s);
+    if (na > 0) c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    (void)n;
+    if (read_status(c)) return c->err;
+    if (n_todo > 0) return fail(c, GZ_ERR_DENSITY_MAXITER, "density did not converge in MAXITER iterations");
+    c->have_density = true;
+    c->sym_valid = false;
+    return GZ_OK;
+}
+
+int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->have_density) return fail(c, GZ_ERR_ORDER, "gradients before density");
+    int na = 0;
+    if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (build_sym_rows(c, na)) return c->err;
+    c->sym_all = (active == nullptr);
+    c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
+    Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
+    Particles ps = view(c);
+    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->stream);
+    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->stream);
+    if (na > 0) c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    if (read_status(c)) return c->err;
+    c->have_gradients = true;
+    return GZ_OK;
+}
+
+int gz_hydro_force(gz_context *c, const int *active, int n_active)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->have_gradients) return fail(c, GZ_ERR_ORDER, "force before gradients");
+    int na = 0;
+    if (sort_targets(c, active, n_active, &na)) return c->err;
+    // the gradient pass's symmetric rows are reused when the active set is
+    // the same (the corridor list shared by both loops, hydro_corridor.cc:195-255)
+    const bool same = c->sym_valid && c->sym_rows == na &&
+                      ((active == nullptr && c->sym_all) ||
+                       (active != nullptr && !c->sym_all && c->sym_active.size() == (size_t)n_active &&
+                        std::equal(c->sym_active.begin(), c->sym_active.end(), active)));
+    if (!same) {
+        if (build_sym_rows(c, na)) return c->err;
+        c->sym_all = (active == nullptr);
+        c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
+    }
+    Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
+    Particles ps = view(c);
+    force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
+    if (c->prm.precision == GZ_PRECISION_MIXED)
+        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->stream);
+    else force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->stream);
+    if (na > 0) c->launches += 2;
+    GZ_CUDA(c, cudaGetLastError());
+    if (read_status(c)) return c->err;
+    return GZ_OK;
+}
+
+int gz_download(gz_context *c, const gz_outputs *o)
+{
+    if (!c || !o) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    const int n = c->n;
+    if (n == 0) return GZ_OK;
+    cudaStream_t s = c->stream;
+    struct { double *dst; DevBuf *src; int k; } f[] = {
+        {o->h, &c->h, 1}, {o->num_ngb, &c->num_ngb, 1}, {o->drkern, &c->drkern, 1}, {o->divvel, &c->divvel, 1},
+        {o->rho, &c->rho, 1}, {o->pressure, &c->pressure, 1}, {o->nvt, &c->nvt, 6}, {o->cond, &c->cond, 1},
+        {o->fce, &c->fce, 1}, {o->pvel, &c->pv, 3}, {o->accel, &c->accel, 3}, {o->dudt, &c->dudt, 1},
+        {o->vsig, &c->vsig, 1}, {o->dtmass, &c->dtmass, 1}, {o->dmass, &c->dmass, 1}, {o->gravwork, &c->gw, 3}};
+    for (auto &e : f) {
+        if (!e.dst) continue;
+        const long long cnt = (long long)n * e.k;
+        k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, e.k, ptr<int>(c->perm), ptr<double>(*e.src),
+                                                                      ptr<double>(c->stage));
+        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->stage.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+    }
+    struct { double *dst; int off; } g[] = {{o->grad_rho, 0}, {o->grad_p, 3}, {o->grad_v, 6}};
+    for (auto &e : g) {
+        if (!e.dst) continue;
+        const int k = (e.off == 6) ? 9 : 3;
+        const long long cnt = (long long)n * k;
+        k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, k, ptr<int>(c->perm),
+                                                                      ptr<double>(c->grad) + (size_t)e.off * n,
+                                                                      ptr<double>(c->stage));
+        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->stage.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+    }
+    if (o->iters) {
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters), ptr<int>(c->stage));
+        GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->stage.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    }
+    GZ_CUDA(c, cudaGetLastError());
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    return GZ_OK;
+}
+
+
+// Host-side reorder of rows built for the sorted targets into the caller's
+// active order with original indices, each row ascending.
+static int rows_to_host(gz_context *c, const int *active, int n_active, int na, DevBuf &off, DevBuf &nbr,
+                        std::vector<long long> &h_off, std::vector<int> &h_nbr, std::vector<int> &order)
+{
+    const int n = c->n;
+    std::vector<long long> o((size_t)na + 1);
+    std::vector<int> tg((size_t)std::max(na, 1)), perm((size_t)std::max(n, 1));
+    GZ_CUDA(c, cudaMemcpy(o.data(), off.p, sizeof(long long) * ((size_t)na + 1), cudaMemcpyDeviceToHost));
+    std::vector<int> e((size_t)std::max(o[(size_t)na], 1ll));
+    if (o[(size_t)na] > 0) GZ_CUDA(c, cudaMemcpy(e.data(), nbr.p, sizeof(int) * (size_t)o[(size_t)na], cudaMemcpyDeviceToHost));
+    if (na > 0) GZ_CUDA(c, cudaMemcpy(tg.data(), c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToHost));
+    if (n > 0) GZ_CUDA(c, cudaMemcpy(perm.data(), c->perm.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+    std::vector<int> slot_of_orig((size_t)std::max(n, 1), -1);
+    for (int a = 0; a < na; a++) slot_of_orig[(size_t)perm[(size_t)tg[(size_t)a]]] = a;
+    const int rows = active ? n_active : n;
+    order.assign((size_t)rows, -1);
+    for (int r = 0; r < rows; r++) order[(size_t)r] = slot_of_orig[(size_t)(active ? active[r] : r)];
+    h_off.assign((size_t)rows + 1, 0);
+    for (int r = 0; r < rows; r++) {
+        const int a = order[(size_t)r];
+        h_off[(size_t)r + 1] = h_off[(size_t)r] + (a >= 0 ? (o[(size_t)a + 1] - o[(size_t)a]) : 0);
+    }
+    h_nbr.assign((size_t)std::max(h_off[(size_t)rows], 1ll), 0);
+    for (int r = 0; r < rows; r++) {
+        const int a = order[(size_t)r];
+        if (a < 0) continue;
+        long long w = h_off[(size_t)r];
+        for (long long k = o[(size_t)a]; k < o[(size_t)a + 1]; k++) h_nbr[(size_t)w++] = perm[(size_t)e[(size_t)k]];
+        std::sort(h_nbr.begin() + h_off[(size_t)r], h_nbr.begin() + h_off[(size_t)r + 1]);
+    }
+    return 0;
+}
+
+int gz_neighbors(gz_context *c, const int *active, int n_active, int mode, int64_t *offsets, int *nbrs)
+{
+    if (!c || !offsets || (mode != 0 && mode != 1)) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "neighbours before upload");
+    int na = 0;
+    if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (mode == 1 && refresh_hmax(c)) return c->err;
+    long long total = 0, cap = 0;
+    DevBuf cnt, off, nbr;
+    int rc = build_rows(c, ptr<double>(c->h), mode, ptr<int>(c->targets), na, cnt, off, nbr, cap, &total);
+    std::vector<long long> h_off;
+    std::vector<int> h_nbr, order;
+    if (!rc) rc = rows_to_host(c, active, n_active, na, off, nbr, h_off, h_nbr, order);
+    release(cnt); release(off); release(nbr);
+    if (rc) return rc;
+    if (read_status(c)) return c->err;
+    const size_t rows = order.size();
+    for (size_t r = 0; r <= rows; r++) offsets[r] = (int64_t)h_off[r];
+    if (nbrs && h_off[rows] > 0) memcpy(nbrs, h_nbr.data(), sizeof(int) * (size_t)h_off[rows]);
+    return GZ_OK;
+}
+
+int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc, double *pv)
+{
+    if (!c || !acc) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "density sums before upload");
+    cudaStream_t s = c->stream;
+    int na = 0;
+    if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (na > 0)
+        k_rows_of<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<int>(c->row_of), ptr<double>(c->h), 1.0,
+                                                    ptr<double>(c->h_built));
+    long long total = 0;
+    if (build_rows(c, ptr<double>(c->h_built), 0, ptr<int>(c->targets), na, c->counts, c->d_off, c->d_nbr,
+                   c->d_nbr_cap, &total))
+        return c->err;
+    Particles ps = view(c);
+    DensityWork w{};
+    w.todo = ptr<int>(c->targets);
+    w.n_todo = na;
+    w.row_of = ptr<int>(c->row_of);
+    w.rows.off = ptr<long long>(c->d_off);
+    w.rows.nbr = ptr<int>(c->d_nbr);
+    w.acc = ptr<double>(c->acc);
+    if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
+    else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);
+    GZ_CUDA(c, cudaGetLastError());
+    const int n = c->n;
+    std::vector<double> a17((size_t)17 * (size_t)std::max(n, 1));
+    std::vector<int> perm((size_t)std::max(n, 1)), tg((size_t)std::max(na, 1));
+    GZ_CUDA(c, cudaMemcpyAsync(a17.data(), c->acc.p, sizeof(double) * 17 * (size_t)n, cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaMemcpyAsync(tg.data(), c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    std::vector<int> sorted_of_orig((size_t)std::max(n, 1), -1);
+    for (int a = 0; a < na; a++) sorted_of_orig[(size_t)perm[(size_t)tg[(size_t)a]]] = tg[(size_t)a];
+    const int rows = active ? n_active : n;
+    for (int r = 0; r < rows; r++) {
+        const int t = sorted_of_orig[(size_t)(active ? active[r] : r)];
+        for (int k = 0; k < 14; k++) acc[(size_t)r * 14 + k] = (t >= 0 && k < 13) ? a17[(size_t)k * n + t] : 0.0;
+        if (pv)
+            for (int k = 0; k < 3; k++) pv[(size_t)r * 3 + k] = t >= 0 ? a17[(size_t)(14 + k) * n + t] : 0.0;
+    }
+    return read_status(c) ? c->err : GZ_OK;
+}
+
+int gz_status(gz_context *c, gz_status_info *info)
+{
+    if (!c || !info) return GZ_ERR_ARG;
+    memset(info, 0, sizeof(*info));
+    cudaSetDevice(c->device);
+    read_status(c);
+    info->code = c->err;
+    info->index = -1;
+    if (c->err_index >= 0 && c->err_index < c->n && c->perm.p) {
+        int orig = -1;
+        if (cudaMemcpy(&orig, ptr<int>(c->perm) + c->err_index, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+            info->index = orig;
+    }
+    info->density_iterations = c->last_iters;
+    info->kernel_launches = c->launches;
+    info->pairs_density = c->pairs_density;
+    info->pairs_symmetric = c->pairs_symmetric;
+    size_t bytes = 0;
+    DevBuf *all[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
+                     &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
+                     &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
+                     &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
+                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->acc, &c->h_built, &c->scratch,
+                     &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
+                     &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
+                     &c->o_dt, &c->o_h, &c->o_cond};
+    for (DevBuf *b : all) bytes += b->bytes;
+    info->device_bytes = (int64_t)bytes;
+    snprintf(info->message, sizeof(info->message), "%s", c->msg);
+    return GZ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+// gizmo_b200/csrc/launch.h -- host launchers shared by the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "state.cuh"
+
+namespace gz {
+
+// grid.cu
+void grid_keys(int n, const double *pos, double box, int F, uint32_t *keys, int *idx, cudaStream_t s);
+void grid_cell_start(int n, const uint32_t *skeys, int F, int *start, cudaStream_t s);
+void grid_hmax(int n, const uint32_t *skeys, const double *h, int F, double *hmax, const long long *level_off,
+               cudaStream_t s);
+void walk_rows(const Grid &g, const double *x, const double *y, const double *z, const double *reach,
+               const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
+               const long long *off, int *nbr, DevStatus *st, cudaStream_t s);
+
+// Work description of the density iteration.
+struct DensityWork {
+    const int *todo;        // sorted indices still iterating
+    int n_todo;
+    const int *row_of;      // sorted index -> row of the density neighbour rows
+    Csr rows;
+    double *acc;            // [17][n] per-particle accumulator (sorted index)
+    double *h_built;        // search radius each row was built with
+    DensityScratch *scratch;
+    unsigned char *keep;    // per todo slot
+    int *rebuild;           // set when a radius outgrows its row
+    int iter;
+};
+
+// passes_fp64.cu / passes_mixed.cu (same kernels, pair arithmetic double / float)
+struct PassLaunch {
+    int tpt_density, tpt_gradient, tpt_force;
+};
+
+void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
+void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
+void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s);
+void density_finalize(const PassParams &p, const Particles &ps, const double *acc, const int *targets, int n_targets,
+                      cudaStream_t s);
+void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                    cudaStream_t s);
+void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                     cudaStream_t s);
+void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                DevStatus *st, cudaStream_t s);
+void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                 DevStatus *st, cudaStream_t s);
+void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
+
+}  // namespace gz

@@ -1,0 +1,385 @@
+// gizmo_b200/csrc/passes.cuh -- the three pair kernels, templated on pair arithmetic T.
+//
+// Included by passes_fp64.cu (T = double, built without FMA contraction) and
+// passes_mixed.cu (T = float). Layout: a group of TPT consecutive lanes owns
+// one target row; lanes stride over the row's neighbours, gather neighbour
+// fields from the sorted SoA mirror (Morton order keeps them in L1/L2),
+// evaluate the pair in T, accumulate in FP64 registers and combine with
+// __shfl_xor within the group. Lane 0 of the group runs the per-particle
+// epilogue (finalize) in FP64.
+#pragma once
+
+#include "launch.h"
+
+namespace gz {
+
+// ---------------------------------------------------------------- density
+// DensitySpec::pair_kernel (density_loop.h:1140-1385), gas i, gas j; the
+// row is a superset (buffered radius) and r2 < h^2 is re-tested exactly.
+template <typename T, int TPT>
+__global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps, DensityWork w)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = gtid / TPT, lane = gtid % TPT;
+    if (slot >= w.n_todo) return;
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
+    const int t = w.todo[slot];
+    const int row = w.row_of[t];
+    const double xi = ps.x[t], yi = ps.y[t], zi = ps.z[t];
+    const double hd = ps.h[t];
+    const double h2 = hd * hd;
+    const T h = T(hd);
+    T hinv, hinv3, hinv4;
+    k_hinv(h, hinv, hinv3, hinv4);
+    const T vix = T(ps.vx[t]), viy = T(ps.vy[t]), viz = T(ps.vz[t]);
+    const int mfv = p.method == 1;
+    double a[17];
+#pragma unroll
+    for (int k = 0; k < 17; k++) a[k] = 0;
+    const long long b0 = w.rows.off[row], b1 = w.rows.off[row + 1];
+    for (long long e = b0 + lane; e < b1; e += TPT) {
+        const int j = w.rows.nbr[e];
+        const double mjd = ps.m[j];
+        if (mjd <= 0) continue;
+        double dx, dy, dz;
+        const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
+        if (r2 >= h2) continue;
+        const T r = Real<T>::sqrt_(T(r2));
+        const T u = r * hinv;
+        T wk, dwk;
+        k_main(p.kernel, u, hinv3, hinv4, wk, dwk);
+        const T mj = T(mjd);
+        const T mj_wk = mj * wk;
+        a[0] += (double)wk;
+        a[1] += (double)mj_wk;
+        const T vjx = T(ps.vx[j]), vjy = T(ps.vy[j]), vjz = T(ps.vz[j]);
+        if (mfv && r == T(0)) {
+            a[14] += (double)(mj_wk * vjx);
+            a[15] += (double)(mj_wk * vjy);
+            a[16] += (double)(mj_wk * vjz);
+        }
+        a[2] += (double)(-(T(3) * hinv * wk + u * dwk));
+        if (r > T(0)) {
+            const T px = T(dx), py = T(dy), pz = T(dz);
+            a[4] += (double)(px * px * wk);
+            a[5] += (double)(py * py * wk);
+            a[6] += (double)(pz * pz * wk);
+            a[7] += (double)(px * py * wk);
+            a[8] += (double)(py * pz * wk);
+            a[9] += (double)(px * pz * wk);
+            a[10] += (double)(wk * px);
+            a[11] += (double)(wk * py);
+            a[12] += (double)(wk * pz);
+            const T dvx = vix - vjx, dvy = viy - vjy, dvz = viz - vjz;
+            if (mfv) {
+                a[14] += (double)(mj_wk * (vix - dvx));
+                a[15] += (double)(mj_wk * (viy - dvy));
+                a[16] += (double)(mj_wk * (viz - dvz));
+            }
+            a[3] -= (double)(dwk * (px * dvx + py * dvy + pz * dvz) / r);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 17; k++) a[k] = warp_sum(a[k], mask, TPT);
+    if (lane == 0) {
+        const size_t n = (size_t)ps.n;
+#pragma unroll
+        for (int k = 0; k < 17; k++) w.acc[k * n + t] = a[k];
+    }
+}
+
+template <typename T>
+void launch_density_sums(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s)
+{
+    if (w.n_todo <= 0) return;
+    const long long threads = (long long)w.n_todo * tpt;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    switch (tpt) {
+        case 4: k_density_sums<T, 4><<<blocks, 256, 0, s>>>(p, ps, w); break;
+        case 8: k_density_sums<T, 8><<<blocks, 256, 0, s>>>(p, ps, w); break;
+        case 32: k_density_sums<T, 32><<<blocks, 256, 0, s>>>(p, ps, w); break;
+        default: k_density_sums<T, 16><<<blocks, 256, 0, s>>>(p, ps, w); break;
+    }
+}
+
+// -------------------------------------------------------------- gradients
+// gradient_accumulate_neighbor (gradient_functions.h:304-665) + the
+// finalize: construct_gradient (gradients_loop.cc:129-136) and
+// local_slopelimiter (gradients_loop.cc:1077-1130).
+template <typename T, int TPT>
+__global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
+                                                   int n_targets, Csr rows)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = gtid / TPT, lane = gtid % TPT;
+    if (slot >= n_targets) return;
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
+    const int i = targets[slot];
+    const size_t n = (size_t)ps.n;
+    const double mi = ps.m[i], rhoi = ps.rho[i], Pi = ps.pressure[i], hid = ps.h[i];
+    const bool enabled = (mi > 0 && rhoi > 0);
+    const double xi = ps.x[i], yi = ps.y[i], zi = ps.z[i];
+    const double hi2 = hid * hid;
+    const T hi = T(hid);
+    T hinv, hinv3, hinv4;
+    k_hinv(hi, hinv, hinv3, hinv4);
+    const T rho_i = T(rhoi), P_i = T(Pi);
+    const T vi[3] = {T(ps.vx[i]), T(ps.vy[i]), T(ps.vz[i])};
+    double gr[15];  // [k][q]: q = rho, P, v0, v1, v2
+    double mx[5], mn[5], maxdist = 0;
+#pragma unroll
+    for (int k = 0; k < 15; k++) gr[k] = 0;
+#pragma unroll
+    for (int k = 0; k < 5; k++) { mx[k] = 0; mn[k] = 0; }
+    if (enabled) {
+        const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
+        for (long long e = b0 + lane; e < b1; e += TPT) {
+            const int j = rows.nbr[e];
+            const double mj = ps.m[j], rhoj = ps.rho[j], hjd = ps.h[j];
+            if (mj <= 0) continue;
+            if (rhoj <= 0 || hjd <= 0) continue;
+            double dx, dy, dz;
+            const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
+            if (r2 <= 0) continue;
+            if ((r2 >= hi2) && (r2 >= hjd * hjd)) continue;
+            const T r = Real<T>::sqrt_(T(r2));
+            T wk_i = T(0), dwk_i = T(0);
+            if (r < hi) k_main(p.kernel, r * hinv, hinv3, hinv4, wk_i, dwk_i);
+            if ((double)r > maxdist) maxdist = (double)r;
+            T d[5];
+            d[0] = T(rhoj) - rho_i;
+            d[1] = T(ps.pressure[j]) - P_i;
+            d[2] = T(ps.vx[j]) - vi[0];
+            d[3] = T(ps.vy[j]) - vi[1];
+            d[4] = T(ps.vz[j]) - vi[2];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                const double dq = (double)d[q];
+                if (dq < mn[q]) mn[q] = dq; else if (dq > mx[q]) mx[q] = dq;
+            }
+            if (r < hi) {
+                const T dp[3] = {T(dx), T(dy), T(dz)};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const T wxyz = -wk_i * dp[k];
+                    gr[5 * k + 0] += (double)(wxyz * d[0]);
+                    gr[5 * k + 1] += (double)(wxyz * d[1]);
+                    gr[5 * k + 2] += (double)(d[2] * wxyz);
+                    gr[5 * k + 3] += (double)(d[3] * wxyz);
+                    gr[5 * k + 4] += (double)(d[4] * wxyz);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 15; k++) gr[k] = warp_sum(gr[k], mask, TPT);
+#pragma unroll
+    for (int q = 0; q < 5; q++) { mx[q] = warp_max(mx[q], mask, TPT); mn[q] = warp_min(mn[q], mask, TPT); }
+    maxdist = warp_max(maxdist, mask, TPT);
+    if (lane != 0) return;
+    double g_rho[3] = {0, 0, 0}, g_p[3] = {0, 0, 0}, g_v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (enabled) {
+        double nv[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) nv[k] = ps.nvt[k * n + i];
+        double s_rho[3] = {gr[0], gr[5], gr[10]}, s_p[3] = {gr[1], gr[6], gr[11]};
+        sym_matvec(nv, s_rho, g_rho);
+        sym_matvec(nv, s_p, g_p);
+        for (int c = 0; c < 3; c++) {
+            double s_v[3] = {gr[2 + c], gr[7 + c], gr[12 + c]};
+            sym_matvec(nv, s_v, g_v[c]);
+        }
+        double stol = 0.0, h_lim = hid;
+        const double d_max = dmax(hid, maxdist);
+        h_lim = d_max;
+        double a_limiter = 0.25;
+        const double CN = ps.cond[i];
+        if (CN > 100) a_limiter = dmin(0.5, 0.25 + 0.25 * (CN - 100) / 100);
+        if (p.selfgravity_off) { h_lim = hid; stol = 0.1; }
+        slopelimiter(g_rho, mx[0], mn[0], a_limiter, h_lim, 0, 1, d_max, rhoi);
+        slopelimiter(g_p, mx[1], mn[1], a_limiter, h_lim, stol, 1, d_max, Pi);
+        for (int c = 0; c < 3; c++) slopelimiter(g_v[c], mx[2 + c], mn[2 + c], a_limiter, h_lim, stol, 0, 0, 0);
+    }
+    for (int k = 0; k < 3; k++) {
+        ps.grad[(0 + k) * n + i] = g_rho[k];
+        ps.grad[(3 + k) * n + i] = g_p[k];
+        for (int c = 0; c < 3; c++) ps.grad[(6 + 3 * c + k) * n + i] = g_v[c][k];
+    }
+}
+
+template <typename T>
+void launch_gradients(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                      cudaStream_t s)
+{
+    if (n_targets <= 0) return;
+    const long long threads = (long long)n_targets * tpt;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    switch (tpt) {
+        case 4: k_gradients<T, 4><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
+        case 8: k_gradients<T, 8><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
+        case 32: k_gradients<T, 32><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
+        default: k_gradients<T, 16><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
+    }
+}
+
+// ------------------------------------------------------------------ force
+template <typename T> GZ_DEV void load_side(const Particles &ps, int i, double gamma, Side<T> &S)
+{
+    const size_t n = (size_t)ps.n;
+    S.v[0] = T(ps.vx[i]); S.v[1] = T(ps.vy[i]); S.v[2] = T(ps.vz[i]);
+    S.pv[0] = T(ps.pv[i]); S.pv[1] = T(ps.pv[n + i]); S.pv[2] = T(ps.pv[2 * n + i]);
+#pragma unroll
+    for (int k = 0; k < 6; k++) S.nvt[k] = T(ps.nvt[k * n + i]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { S.grho[k] = T(ps.grad[k * n + i]); S.gp[k] = T(ps.grad[(3 + k) * n + i]); }
+#pragma unroll
+    for (int k = 0; k < 9; k++) S.gv[k] = T(ps.grad[(6 + k) * n + i]);
+    const double rho = ps.rho[i], P = ps.pressure[i];
+    S.m = T(ps.m[i]);
+    S.rho = T(rho);
+    S.P = T(P);
+    S.h = T(ps.h[i]);
+    S.cs = T((rho > 0) ? sqrt(gamma * P / rho) : 0.0);  // effective_soundspeed, cell_data.h:703-713
+    S.cond = T(ps.cond[i]);
+    S.fce = T(ps.fce[i]);
+    S.drk = T(ps.drkern[i]);
+    S.dt = ps.dt[i];
+}
+
+// Row i of the symmetric list: every pair is evaluated in one canonical
+// orientation (lower sorted index as the R side) so the flux seen from i and
+// from j are exact negatives -- mass and momentum are conserved to roundoff
+// of the FP64 accumulation. i-side accumulation follows
+// hydro_functions.h:419-509, j-side dMass writes hydro_functions.h:511-532,
+// writeback hydro_force_loop.cc:227-391, final operations
+// hydro_toplevel.cc:133-253.
+template <typename T, int TPT>
+__global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const int *__restrict__ targets,
+                                               int n_targets, Csr rows, DevStatus *st)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = gtid / TPT, lane = gtid % TPT;
+    if (slot >= n_targets) return;
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
+    const int i = targets[slot];
+    const size_t n = (size_t)ps.n;
+    const int mfv = p.method == 1;
+    GConst<T> gc;
+    {
+        const double G0 = p.gamma;
+        gc.G0 = T(G0); gc.G1 = T((G0 - 1.0) / (2.0 * G0)); gc.G2 = T((G0 + 1.0) / (2.0 * G0));
+        gc.G3 = T((2.0 * G0 / (G0 - 1.0))); gc.G4 = T(2.0 / (G0 - 1.0)); gc.G5 = T(2.0 / (G0 + 1.0));
+        gc.G6 = T((G0 - 1.0) / (G0 + 1.0)); gc.G7 = T(0.5 * (G0 - 1.0)); gc.G8 = T(1.0 / G0); gc.G9 = T(G0 - 1.0);
+        gc.mfv = mfv;
+    }
+    const double mi = ps.m[i], rhoi = ps.rho[i];
+    const bool enabled = (mi > 0 && rhoi > 0);
+    const double xi = ps.x[i], yi = ps.y[i], zi = ps.z[i], hid = ps.h[i], dti = ps.dt[i];
+    Side<T> SI;
+    load_side(ps, i, p.gamma, SI);
+    double acc[3] = {0, 0, 0}, dtE = 0, dtm = 0, dm = 0, gw[3] = {0, 0, 0}, vs = 0;
+    int stop = 0;
+    if (enabled) {
+        vs = (double)SI.cs;
+        const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
+        for (long long e = b0 + lane; e < b1; e += TPT) {
+            const int j = rows.nbr[e];
+            const double mj = ps.m[j], rhoj = ps.rho[j];
+            if (!(mj > 0 && rhoj > 0)) continue;
+            double dx, dy, dz;
+            const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
+            const double hjd = ps.h[j];
+            Side<T> SJ;
+            load_side(ps, j, p.gamma, SJ);
+            PairFlux<T> F;
+            double sign;
+            if (i < j) {
+                const T dp[3] = {T(dx), T(dy), T(dz)};
+                force_pair(p.kernel, mfv, p.selfgravity_off, gc, SI, SJ, dp, r2, hid, hjd, F, stop);
+                sign = 1.0;
+            } else {
+                const T dp[3] = {T(-dx), T(-dy), T(-dz)};
+                force_pair(p.kernel, mfv, p.selfgravity_off, gc, SJ, SI, dp, r2, hjd, hid, F, stop);
+                sign = -1.0;
+            }
+            if (!F.valid) continue;
+            const double frho = sign * (double)F.rho;
+            acc[0] += sign * (double)F.v[0];
+            acc[1] += sign * (double)F.v[1];
+            acc[2] += sign * (double)F.v[2];
+            dtE += sign * (double)F.p;
+            if ((double)F.vsig_ts > vs) vs = (double)F.vsig_ts;
+            if (mfv) {
+                double self_dm, accepted, other_dm;
+                mfv_mass_side(frho, dti, SJ.dt, mi, mj, self_dm, accepted, other_dm);
+                dtm += frho;
+                dm += self_dm;
+                gw[0] += dx * accepted;
+                gw[1] += dy * accepted;
+                gw[2] += dz * accepted;
+                if (ps.active[j]) {
+                    double sj, aj, oj;  // j's own evaluation writes onto i
+                    mfv_mass_side(-frho, SJ.dt, dti, mj, mi, sj, aj, oj);
+                    dm += oj;
+                } else if (other_dm != 0) {
+                    atomicAdd(ps.dmass + j, other_dm);
+                }
+            }
+        }
+    }
+    if (stop) record_status(st, stop, i);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { acc[k] = warp_sum(acc[k], mask, TPT); gw[k] = warp_sum(gw[k], mask, TPT); }
+    dtE = warp_sum(dtE, mask, TPT);
+    dtm = warp_sum(dtm, mask, TPT);
+    dm = warp_sum(dm, mask, TPT);
+    vs = warp_max(vs, mask, TPT);
+    if (lane != 0) return;
+    // writeback: preloop zeros + this row's sums; MaxSignalVel floor
+    const double cs_i = (rhoi > 0) ? sqrt(p.gamma * ps.pressure[i] / rhoi) : sqrt(p.gamma * (p.gamma - 1.) * ps.u[i]);
+    double vsig = kMinReal;
+    const double max_sig = fmax(vs, cs_i);
+    if (vsig < max_sig) vsig = max_sig;
+    double a3[3] = {acc[0], acc[1], acc[2]}, du = dtE, g3[3] = {gw[0], gw[1], gw[2]};
+    if (mi > 0) {
+        const double v[3] = {ps.vx[i], ps.vy[i], ps.vz[i]};
+        if (mfv) {
+            const double d[3] = {v[0] - ps.pv[i], v[1] - ps.pv[n + i], v[2] - ps.pv[2 * n + i]};
+            const double v2_p = vsig * vsig + (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            vsig = sqrt(v2_p);
+        }
+        du -= (v[0] * a3[0] + v[1] * a3[1] + v[2] * a3[2]);
+        if (mfv) {
+            du += 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * dtm;
+            for (int k = 0; k < 3; k++) a3[k] -= v[k] * dtm;
+        }
+        const double inv = 1.0 / mi;
+        for (int k = 0; k < 3; k++) a3[k] *= inv;
+        if (mfv) du -= ps.u[i] * dtm;
+        du /= mi;
+        if (mfv) for (int k = 0; k < 3; k++) g3[k] *= inv;
+        if (hid >= 0.99 * p.max_kernel_radius) du = 0;
+    }
+    for (int k = 0; k < 3; k++) { ps.accel[k * n + i] = a3[k]; ps.gw[k * n + i] = g3[k]; }
+    ps.dudt[i] = du;
+    ps.vsig[i] = vsig;
+    ps.dtmass[i] = dtm;
+    ps.dmass[i] += dm;
+}
+
+template <typename T>
+void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                  DevStatus *st, cudaStream_t s)
+{
+    if (n_targets <= 0) return;
+    const long long threads = (long long)n_targets * tpt;
+    const unsigned blocks = (unsigned)((threads + 127) / 128);
+    switch (tpt) {
+        case 4: k_force<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
+        case 8: k_force<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
+        case 32: k_force<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
+        default: k_force<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
+    }
+}
+
+}  // namespace gz

@@ -1,0 +1,128 @@
+// gizmo_b200/csrc/passes_fp64.cu -- FP64 form of the pair kernels plus the
+// per-particle FP64 epilogues shared by both forms. Built with -fmad=false so
+// every product and sum rounds as in the reference's CPU build.
+#include "passes.cuh"
+
+namespace gz {
+
+void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s)
+{
+    launch_density_sums<double>(p, ps, w, tpt, s);
+}
+
+void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                    cudaStream_t s)
+{
+    launch_gradients<double>(p, ps, targets, n_targets, rows, tpt, s);
+}
+
+void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                DevStatus *st, cudaStream_t s)
+{
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, s);
+}
+
+// DensitySpec::after_iter_body per iterating particle, plus the runner's
+// radius update and compaction flag (neighbor_loop_runner.cc:7340-7372).
+__global__ void k_after_iter(PassParams p, Particles ps, DensityWork w, DevStatus *st)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= w.n_todo) return;
+    const int t = w.todo[s];
+    const size_t n = (size_t)ps.n;
+    double acc[14];
+    for (int k = 0; k < 14; k++) acc[k] = w.acc[k * n + t];
+    const double h = ps.h[t];
+    DensityScratch sc = w.scratch[t];
+    double nh = h;
+    int stop = 0;
+    const int conv = after_iter(p, w.iter, h, acc, ps.cond[t], sc, nh, stop);
+    w.scratch[t] = sc;
+    ps.iters[t] = w.iter + 1;
+    if (stop) record_status(st, stop, t);
+    if (conv) {
+        w.keep[s] = 0;
+    } else {
+        ps.h[t] = nh;
+        w.keep[s] = 1;
+        if (nh > w.h_built[t]) atomicExch(w.rebuild, 1);
+    }
+}
+
+void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s)
+{
+    if (w.n_todo <= 0) return;
+    k_after_iter<<<(w.n_todo + 127) / 128, 128, 0, s>>>(p, ps, w, st);
+}
+
+// density_finalize_post_runner (density_loop.cc:303-733), gas, non-SPH.
+__global__ void k_density_finalize(PassParams p, Particles ps, const double *__restrict__ accb,
+                                   const int *__restrict__ targets, int n_targets)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_targets) return;
+    const int i = targets[s];
+    const size_t n = (size_t)ps.n;
+    double acc[17];
+    for (int k = 0; k < 17; k++) acc[k] = accb[k * n + i];
+    const double h = ps.h[i];
+    double NumNgb = acc[0], Drk = acc[2], DivV = acc[3];
+    if (NumNgb > 0) {
+        Drk *= h / (3 * NumNgb);
+        DivV /= NumNgb;
+        NumNgb *= kVolNorm * pow(h, 3.0);
+    } else { NumNgb = Drk = DivV = 0; }
+    if (Drk > -0.9) Drk = 1.0 / (1.0 + Drk); else Drk = 1.0;
+    DivV *= Drk;
+    ps.drkern[i] = Drk;
+    ps.divvel[i] = DivV;
+    double rho = acc[1];
+    double pvl[3] = {acc[14], acc[15], acc[16]};
+    double CN, fce, Tn[3][3];
+    nvt_invert(h, NumNgb, acc + 4, acc + 10, CN, Tn, fce);
+    ps.nvt[0 * n + i] = Tn[0][0]; ps.nvt[1 * n + i] = Tn[1][1]; ps.nvt[2 * n + i] = Tn[2][2];
+    ps.nvt[3 * n + i] = Tn[0][1]; ps.nvt[4 * n + i] = Tn[1][2]; ps.nvt[5 * n + i] = Tn[0][2];
+    ps.cond[i] = CN;
+    ps.fce[i] = fce;
+    const double m = ps.m[i];
+    if (m > 0) {
+        if (rho > 0 && p.method == 1) {
+            const double eps = 0.3;
+            const double v[3] = {ps.vx[i], ps.vy[i], ps.vz[i]};
+            for (int k = 0; k < 3; k++) pvl[k] = v[k] * (1.0 - eps) + pvl[k] * (eps / rho);
+        }
+        if ((h > 0) && (NumNgb > 0)) rho = m * NumNgb / (kVolNorm * pow(h, 3.0));
+        else if (h <= 0) rho = 0;
+        else rho = m / (kVolNorm * pow(h, 3.0));
+        ps.pressure[i] = (p.gamma - 1) * ps.u[i] * rho;
+    }
+    ps.rho[i] = rho;
+    for (int k = 0; k < 3; k++) ps.pv[k * n + i] = pvl[k];
+    ps.num_ngb[i] = (NumNgb > 0) ? pow(NumNgb, 1.0 / 3) : 0;
+}
+
+void density_finalize(const PassParams &p, const Particles &ps, const double *acc, const int *targets, int n_targets,
+                      cudaStream_t s)
+{
+    if (n_targets <= 0) return;
+    k_density_finalize<<<(n_targets + 127) / 128, 128, 0, s>>>(p, ps, acc, targets, n_targets);
+}
+
+// hydro_force_initial_operations_preloop (hydro_toplevel.cc:457-565): the
+// running dMass of every active cell restarts at zero (the other preloop
+// fields are assigned outright by the force kernel).
+__global__ void k_force_preloop(Particles ps, const int *__restrict__ targets, int n_targets)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_targets) return;
+    ps.dmass[targets[s]] = 0;
+}
+
+void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s)
+{
+    (void)p;
+    if (n_targets <= 0) return;
+    k_force_preloop<<<(n_targets + 255) / 256, 256, 0, s>>>(ps, targets, n_targets);
+}
+
+}  // namespace gz

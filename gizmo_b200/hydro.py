@@ -1,0 +1,199 @@
+"""Host-side mirror of GIZMO's hydro entry points over the B200 C ABI.
+
+``HydroPass`` holds one device context (its own CUDA stream) and exposes the
+reference's three entry points under their own names:
+
+    density()              src/hydro/density_loop.cc:764
+    hydro_gradient_calc()  src/hydro/gradients_loop.cc:458
+    hydro_force()          src/hydro/hydro_force_loop.cc:423
+
+The reference reads the global P[] / CellP[] arrays; here the caller uploads
+the same fields (``upload``) and reads the results back (``download``). A
+reference stop (endrun) becomes a ``GizmoHydroError`` carrying the same code
+(1155 density did not converge, 90001009 empty bracket, 1234 no positive
+Riemann pressure). All work runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class GizmoHydroError(RuntimeError):
+    def __init__(self, code: int, message: str = ""):
+        super().__init__(f"gizmo_b200 error {code}: {message}")
+        self.code = code
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _f64(a, shape):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != shape:
+        a = a.reshape(shape)
+    return a
+
+
+class HydroPass:
+    """One device-resident particle set and the density -> gradient -> force pass."""
+
+    def __init__(self, params: abi.GzParams, device: int = 0):
+        self.lib = abi.load_library()
+        self.params = params
+        self._ctx = C.c_void_p()
+        rc = self.lib.gz_create(C.byref(params), int(device), C.byref(self._ctx))
+        if rc:
+            raise GizmoHydroError(rc, "gz_create failed")
+        self.n = 0
+        self._keep = []
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self.lib.gz_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_params(self, params: abi.GzParams):
+        self._check(self.lib.gz_set_params(self._ctx, C.byref(params)))
+        self.params = params
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.gz_stream(self._ctx) or 0)
+
+    # -- data ---------------------------------------------------------------
+    def upload(self, pos, vel, mass, u, dt, h, cond=None):
+        n = int(np.asarray(mass).shape[0])
+        arrs = dict(pos=_f64(pos, (n, 3)), vel=_f64(vel, (n, 3)), mass=_f64(mass, (n,)), u=_f64(u, (n,)),
+                    dt=_f64(dt, (n,)), h=_f64(h, (n,)),
+                    cond=_f64(np.zeros(n) if cond is None else cond, (n,)))
+        p = abi.GzParticles()
+        p.n = n
+        for k, a in arrs.items():
+            setattr(p, k, _dp(a))
+        self._check(self.lib.gz_upload(self._ctx, C.byref(p)))
+        self.n = n
+
+    def upload_raw(self, n: int, ptrs: dict):
+        """Upload from caller-owned host buffers (e.g. pinned memory): ptrs maps
+        pos/vel/mass/u/dt/h/cond to addresses of row-major FP64 arrays."""
+        p = abi.GzParticles()
+        p.n = int(n)
+        for k in ("pos", "vel", "mass", "u", "dt", "h", "cond"):
+            if ptrs.get(k):
+                setattr(p, k, C.cast(C.c_void_p(int(ptrs[k])), C.POINTER(C.c_double)))
+        self._check(self.lib.gz_upload(self._ctx, C.byref(p)))
+        self.n = int(n)
+
+    def download_raw(self, ptrs: dict):
+        """Download into caller-owned host buffers (addresses per output field)."""
+        o = abi.GzOutputs()
+        for k, v in ptrs.items():
+            if k == "iters":
+                o.iters = C.cast(C.c_void_p(int(v)), C.POINTER(C.c_int))
+            else:
+                setattr(o, k, C.cast(C.c_void_p(int(v)), C.POINTER(C.c_double)))
+        self._check(self.lib.gz_download(self._ctx, C.byref(o)))
+
+    def restage(self):
+        """Rebuild grid + sorted mirror from the resident inputs (no host traffic)."""
+        self._check(self.lib.gz_restage(self._ctx))
+
+    def upload_workload(self, wl):
+        self.upload(wl.pos, wl.vel, wl.mass, wl.u, wl.dt, wl.h, wl.cond)
+
+    def download(self, fields=None) -> dict:
+        n = self.n
+        names = [f for f, _ in abi.OUTPUT_FIELDS] + ["iters"]
+        want = names if fields is None else list(fields)
+        out = {}
+        o = abi.GzOutputs()
+        for name, k in abi.OUTPUT_FIELDS:
+            if name in want:
+                a = np.zeros((n,) if k == 1 else (n, k))
+                out[name] = a
+                setattr(o, name, _dp(a))
+        if "iters" in want:
+            a = np.zeros(n, dtype=np.int32)
+            out["iters"] = a
+            o.iters = _ip(a)
+        self._check(self.lib.gz_download(self._ctx, C.byref(o)))
+        return out
+
+    # -- the three entry points ---------------------------------------------
+    def _active(self, active):
+        if active is None:
+            return None, 0
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self._keep = [a]
+        return _ip(a), int(a.shape[0])
+
+    def density(self, active=None):
+        ap, na = self._active(active)
+        self._check(self.lib.gz_hydro_density(self._ctx, ap, na))
+
+    def hydro_gradient_calc(self, active=None):
+        ap, na = self._active(active)
+        self._check(self.lib.gz_hydro_gradients(self._ctx, ap, na))
+
+    def hydro_force(self, active=None):
+        ap, na = self._active(active)
+        self._check(self.lib.gz_hydro_force(self._ctx, ap, na))
+
+    def full_pass(self, active=None):
+        self.density(active)
+        self.hydro_gradient_calc(active)
+        self.hydro_force(active)
+
+    # -- diagnostics ----------------------------------------------------------
+    def neighbors(self, mode: int, active=None):
+        ap, na = self._active(active)
+        rows = na if active is not None else self.n
+        off = np.zeros(rows + 1, dtype=np.int64)
+        self._check(self.lib.gz_neighbors(self._ctx, ap, na, int(mode),
+                                          off.ctypes.data_as(C.POINTER(C.c_int64)), None))
+        nb = np.zeros(max(int(off[-1]), 1), dtype=np.int32)
+        self._check(self.lib.gz_neighbors(self._ctx, ap, na, int(mode),
+                                          off.ctypes.data_as(C.POINTER(C.c_int64)), _ip(nb)))
+        return off, nb[: int(off[-1])]
+
+    def density_sums(self, active=None):
+        ap, na = self._active(active)
+        rows = na if active is not None else self.n
+        acc = np.zeros((rows, 14))
+        pv = np.zeros((rows, 3))
+        self._check(self.lib.gz_density_sums(self._ctx, ap, na, _dp(acc), _dp(pv)))
+        return acc, pv
+
+    def status(self) -> dict:
+        s = abi.GzStatusInfo()
+        self.lib.gz_status(self._ctx, C.byref(s))
+        return dict(code=s.code, index=s.index, density_iterations=s.density_iterations,
+                    pairs_density=s.pairs_density, pairs_symmetric=s.pairs_symmetric,
+                    device_bytes=s.device_bytes, kernel_launches=s.kernel_launches, message=s.message.decode(errors="replace"))
+
+    def _check(self, rc: int):
+        if rc:
+            st = self.status()
+            raise GizmoHydroError(int(rc), st.get("message", ""))

@@ -127,7 +127,7 @@ def _grf(ng: int, slope: float, rng: np.random.Generator) -> np.ndarray:
     amp = k2 ** (slope / 4.0)  # sqrt(P(k)), P ~ k^slope
     amp[0, 0, 0] = 0.0
     f = (rng.standard_normal(k2.shape) + 1j * rng.standard_normal(k2.shape)) * amp
-    field = np.fft.irfftn(f, s=(ng, ng, ng))
+    field = np.fft.irfftn(f, s=(ng, ng, ng), axes=(0, 1, 2))
     return field / field.std()
 
 
@@ -142,7 +142,7 @@ def _solenoidal_velocity(ng: int, slope: float, rng: np.random.Generator) -> np.
     v = (rng.standard_normal((3,) + k2.shape) + 1j * rng.standard_normal((3,) + k2.shape)) * amp
     kv = (K * v).sum(0) / k2
     v -= K * kv
-    out = np.stack([np.fft.irfftn(v[c], s=(ng, ng, ng)) for c in range(3)], axis=-1)
+    out = np.stack([np.fft.irfftn(v[c], s=(ng, ng, ng), axes=(0, 1, 2)) for c in range(3)], axis=-1)
     return out
 
 

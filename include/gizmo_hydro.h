@@ -119,6 +119,7 @@ typedef struct gz_status_info {
     int64_t  pairs_density;     /* accepted one-way pairs summed over iterations */
     int64_t  pairs_symmetric;   /* symmetric pairs (rows of the gradient/force lists) */
     int64_t  device_bytes;      /* device memory held by the context */
+    int64_t  kernel_launches;   /* kernels of this library launched by the context so far */
     char     message[256];
 } gz_status_info;
 
@@ -130,9 +131,16 @@ int gz_destroy(gz_context *ctx);
 /* Replace the run-time configuration (keeps particle data). */
 int gz_set_params(gz_context *ctx, const gz_params *params);
 
-/* Copy inputs host -> device and mark the neighbour grid stale.
- * Replaces the arena acquire of neighbor_loop_runner.cc:2297-2302. */
+/* Copy inputs host -> device, build the neighbour grid (Morton sort) and the
+ * sorted particle mirror. Replaces the arena acquire of
+ * neighbor_loop_runner.cc:2297-2302 and the spatial-index build of
+ * gpu_neighbor_list.cc:1134-1169. */
 int gz_upload(gz_context *ctx, const gz_particles *in);
+
+/* Rebuild the grid and the sorted mirror from the inputs already resident
+ * on the device (the last gz_upload), resetting kernel lengths and condition
+ * numbers to the uploaded values: the start of a pass without host traffic. */
+int gz_restage(gz_context *ctx);
 
 /* The three passes. `active` lists original indices (NULL = all particles),
  * like ActiveParticleList filtered by density_isactive / GasGrad_isactive.

@@ -1,0 +1,56 @@
+"""Shared helpers for the tests (comparison metrics, fixture loading)."""
+from __future__ import annotations
+
+import glob
+import os
+
+import numpy as np
+
+from gizmo_b200.abi import GzParams
+from gizmo_b200.ics import Workload
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+DENSITY_FIELDS = ["h", "num_ngb", "drkern", "divvel", "rho", "pressure", "nvt", "cond", "fce", "pvel"]
+GRADIENT_FIELDS = ["grad_rho", "grad_p", "grad_v"]
+FORCE_FIELDS = ["accel", "dudt", "vsig", "dtmass", "dmass", "gravwork"]
+
+
+def rel_err(a, b, floor_frac: float = 1e-6) -> float:
+    """max |a-b| / max(|b|, floor_frac * max|b|), element-wise over the field."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if b.size == 0:
+        return 0.0
+    top = float(np.max(np.abs(b)))
+    if top == 0.0:
+        return float(np.max(np.abs(a)))
+    scale = np.maximum(np.abs(b), floor_frac * top)
+    return float(np.max(np.abs(a - b) / scale))
+
+
+def norm_err(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+def golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(path: str):
+    z = np.load(path)
+    p = GzParams()
+    p.kernel, p.method, p.precision, p.first_step, p.selfgravity_off = [int(v) for v in z["params"]]
+    (p.box_size, p.gamma, p.des_num_ngb, p.max_num_ngb_dev, p.min_kernel_radius,
+     p.max_kernel_radius) = [float(v) for v in z["fparams"]]
+    inputs = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
+    outputs = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
+    return p, inputs, outputs
+
+
+def workload_from(params, inputs, name="fixture") -> Workload:
+    return Workload(name, params, inputs["pos"], inputs["vel"], inputs["mass"], inputs["u"], inputs["dt"],
+                    inputs["h"], inputs["cond"])

@@ -1,0 +1,81 @@
+"""The C-ABI library: it loads, exports every entry point declared in
+include/gizmo_hydro.h, its ctypes mirror has the C layout, and it fails
+cleanly (no trap, an error code) when no GPU is present."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from gizmo_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gizmo_hydro.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void\s*\*)\s*(gz_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_the_exports():
+    assert set(declared_functions()) == set(abi.EXPORTED_SYMBOLS)
+
+
+def test_library_loads_and_exports_all_symbols():
+    lib = abi.load_library()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_struct_layouts_match_c(tmp_path):
+    prog = tmp_path / "layout.c"
+    prog.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "gizmo_hydro.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(gz_params), sizeof(gz_particles), sizeof(gz_outputs), sizeof(gz_status_info));
+  printf("%zu %zu %zu\n", offsetof(gz_params, box_size), offsetof(gz_particles, cond), offsetof(gz_outputs, iters));
+  printf("%zu %zu\n", offsetof(gz_status_info, pairs_density), offsetof(gz_status_info, message));
+  return 0; }
+''')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(prog), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    got = [int(v) for v in out]
+    want = [C.sizeof(abi.GzParams), C.sizeof(abi.GzParticles), C.sizeof(abi.GzOutputs), C.sizeof(abi.GzStatusInfo),
+            abi.GzParams.box_size.offset, abi.GzParticles.cond.offset, abi.GzOutputs.iters.offset,
+            abi.GzStatusInfo.pairs_density.offset, abi.GzStatusInfo.message.offset]
+    assert got == want
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device path")
+def test_create_without_device_returns_code():
+    lib = abi.load_library()
+    from gizmo_b200 import ics
+    p = ics.sedov(4).params
+    ctx = C.c_void_p()
+    assert lib.gz_create(C.byref(p), 0, C.byref(ctx)) == abi.ERR_NO_DEVICE
+    assert not ctx
+
+
+def test_bad_arguments_rejected_before_device_use():
+    lib = abi.load_library()
+    from gizmo_b200 import ics
+    p = ics.sedov(4).params
+    p.kernel = 5
+    ctx = C.c_void_p()
+    assert lib.gz_create(C.byref(p), 0, C.byref(ctx)) == abi.ERR_ARG
+    assert lib.gz_create(None, 0, C.byref(ctx)) == abi.ERR_ARG
+    assert lib.gz_upload(None, None) == abi.ERR_ARG
+    assert lib.gz_hydro_density(None, None, 0) == abi.ERR_ARG

@@ -1,0 +1,184 @@
+"""Parity of the sm_100a pass (through the C ABI) with the CPU oracle.
+
+Tolerances (written here, checked per field):
+  * neighbour sets (one-way at the converged h, symmetric): bit-exact;
+  * density sums at a fixed h, FP64 form: relative 1e-12 (summation order only);
+  * full FP64 pass vs the oracle: relative 1e-10 (element-wise; force fields use
+    a floor of 1e-3 x the field maximum, since their sums cancel);
+  * mixed form vs the FP64 form: h and density per particle 1e-5;
+  * conservation per pass, both forms: |sum of pair fluxes| <= 1e-12 x sum |fluxes|
+    for mass (MFV), momentum and energy.
+"""
+import numpy as np
+import pytest
+
+from gizmo_b200 import abi, ics
+from gizmo_b200.hydro import GizmoHydroError, HydroPass
+from oracle import oracle as O
+from tests._util import DENSITY_FIELDS, FORCE_FIELDS, GRADIENT_FIELDS, norm_err, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "sedov16": lambda p=0: ics.sedov(16, seed=1, precision=p),
+    "plummer16": lambda p=0: ics.plummer_mix(16, seed=4, n_spheres=12, precision=p),
+    "lognormal16": lambda p=0: ics.lognormal(16, seed_density=2, seed_velocity=3, grid=32, precision=p),
+}
+
+
+def gpu_pass(wl, active=None, prior_full=False):
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        if prior_full:
+            hp.full_pass()
+        hp.full_pass(active)
+        return hp.download()
+
+
+def oracle_pass(wl, active=None, prior_full=False):
+    st = O.new_state(wl.n, wl.inputs())
+    orc = O.Oracle(wl.params, "port")
+    if prior_full:
+        assert orc.density(st) == 0 and orc.gradients(st) == 0 and orc.force(st) == 0
+    assert orc.density(st, active) == 0
+    assert orc.gradients(st, active) == 0
+    assert orc.force(st, active) == 0
+    return st
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_density_sums_fixed_h_fp64(name):
+    wl = CASES[name]()
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        acc_g, pv_g = hp.density_sums()
+    st = O.new_state(wl.n, wl.inputs())
+    acc_o, pv_o = O.Oracle(wl.params, "port").density_sums(st)
+    for c in range(13):
+        assert rel_err(acc_g[:, c], acc_o[:, c], 1e-9) < 1e-12, c
+    assert rel_err(pv_g, pv_o, 1e-9) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_full_pass_fp64_matches_oracle(name):
+    wl = CASES[name]()
+    g = gpu_pass(wl)
+    o = oracle_pass(wl)
+    assert np.array_equal(g["iters"], o["iters"])
+    for f in DENSITY_FIELDS + GRADIENT_FIELDS:
+        assert rel_err(g[f], o[f], 1e-6) < 1e-10, f
+    for f in FORCE_FIELDS:
+        assert rel_err(g[f], o[f], 1e-3) < 1e-10, f
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_neighbour_sets_bit_exact(name):
+    wl = CASES[name]()
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.density()
+        h = hp.download(["h"])["h"]
+        g0 = hp.neighbors(0)
+        g1 = hp.neighbors(1)
+        rng = np.random.default_rng(5)
+        sub = rng.choice(wl.n, size=wl.n // 5, replace=False).astype(np.int32)
+        g1s = hp.neighbors(1, sub)
+    st = O.new_state(wl.n, wl.inputs())
+    st["h"][:] = h
+    o0 = O.neighbors(wl.params, st, 0)
+    o1 = O.neighbors(wl.params, st, 1)
+    o1s = O.neighbors(wl.params, st, 1, sub)
+    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g1s, o1s)]:
+        assert np.array_equal(go, oo)
+        assert np.array_equal(gn, on)
+    assert g0[0][-1] > 30 * wl.n  # rows are populated
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_active_subset_matches_oracle(name):
+    wl = CASES[name]()
+    rng = np.random.default_rng(17)
+    active = np.sort(rng.choice(wl.n, size=wl.n // 4, replace=False)).astype(np.int32)
+    g = gpu_pass(wl, active, prior_full=True)
+    o = oracle_pass(wl, active, prior_full=True)
+    for f in DENSITY_FIELDS + GRADIENT_FIELDS:
+        assert rel_err(g[f], o[f], 1e-6) < 1e-10, f
+    for f in FORCE_FIELDS:
+        assert rel_err(g[f], o[f], 1e-3) < 1e-10, f
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_form_against_fp64(name):
+    g64 = gpu_pass(CASES[name](abi.PRECISION_FP64))
+    g32 = gpu_pass(CASES[name](abi.PRECISION_MIXED))
+    assert rel_err(g32["h"], g64["h"]) < 1e-5
+    assert rel_err(g32["rho"], g64["rho"]) < 1e-5
+    for f in GRADIENT_FIELDS + ["accel", "dudt"]:
+        assert norm_err(g32[f], g64[f]) < 1e-3, f
+
+
+def _conservation(wl, out):
+    m = wl.mass
+    v = wl.vel
+    mfv = wl.params.method == abi.METHOD_MFV
+    dtm = out["dtmass"] if mfv else np.zeros(wl.n)
+    mom = m[:, None] * out["accel"] + v * dtm[:, None]  # pair momentum flux sum per particle
+    res = {"momentum": np.abs(mom.sum(0)).max() / np.abs(mom).sum()}
+    ke = 0.5 * (v * v).sum(1)
+    egy = m * out["dudt"] + (v * (m[:, None] * out["accel"])).sum(1) + ke * dtm + wl.u * dtm
+    res["energy"] = abs(egy.sum()) / np.abs(egy).sum()
+    if mfv:
+        res["mass_rate"] = abs(dtm.sum()) / np.abs(dtm).sum()
+        res["mass_step"] = abs(out["dmass"].sum()) / np.abs(out["dmass"]).sum()
+    return res
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+@pytest.mark.parametrize("name", CASES)
+def test_conservation_per_pass(name, precision):
+    wl = CASES[name](precision)
+    out = gpu_pass(wl)
+    for k, v in _conservation(wl, out).items():
+        assert v <= 1e-12, (k, v)
+
+
+def test_tiny_and_duplicate_particles():
+    wl = ics.sedov(3, seed=2)
+    wl.pos[5] = wl.pos[4]  # two particles at the same place: r = 0 pairs
+    wl.params.des_num_ngb = 8.0
+    g = gpu_pass(wl)
+    o = oracle_pass(wl)
+    for f in DENSITY_FIELDS + GRADIENT_FIELDS:
+        assert rel_err(g[f], o[f], 1e-6) < 1e-10, f
+    for f in FORCE_FIELDS:
+        assert rel_err(g[f], o[f], 1e-3) < 1e-10, f
+
+
+def test_empty_bracket_stop_code_and_index():
+    wl = ics.sedov(8, seed=1)
+    wl.h[37] = 0.0  # no neighbour inside r < 0: the reference stops with 90001009
+    st = O.new_state(wl.n, wl.inputs())
+    assert O.Oracle(wl.params, "port").density(st) == abi.ERR_EMPTY_BRACKET
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        with pytest.raises(GizmoHydroError) as e:
+            hp.density()
+        assert e.value.code == abi.ERR_EMPTY_BRACKET
+        assert hp.status()["index"] == 37
+
+
+def test_bad_active_index_and_order():
+    wl = ics.sedov(6, seed=1)
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        with pytest.raises(GizmoHydroError) as e:
+            hp.hydro_gradient_calc()
+        assert e.value.code == abi.ERR_ORDER
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        with pytest.raises(GizmoHydroError) as e:
+            hp.density(np.array([0, wl.n + 3], dtype=np.int32))
+        assert e.value.code == abi.ERR_ARG
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.full_pass(np.zeros(0, dtype=np.int32))  # empty active set is a no-op
