@@ -39,10 +39,11 @@ struct gz_context {
     DevBuf stage, stage3, perm, inv, keys, keys_sorted, idx, cub_tmp, targets_orig, targets, targets_tmp;
     // resident copies of the uploaded inputs, original order (gz_restage source)
     DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
+    DevBuf dl;                       // download staging, [9][n] doubles (widest output field)
     long long launches = 0;          // kernels of this library launched by the context
     // grid
-    int F = 1;
-    DevBuf cell_start, hmax;
+    int D = 1;
+    DevBuf cell_start, hmax, bmax;
     long long level_off[12] = {0};
     bool grid_valid = false;
     // density work
@@ -155,23 +156,31 @@ Particles view(gz_context *c)
 Grid grid_view(gz_context *c)
 {
     Grid g{};
-    g.F = c->F;
+    g.D = c->D;
+    g.n = c->n;
     g.box = c->prm.box_size;
+    g.keys = ptr<unsigned long long>(c->keys_sorted);
     g.cell_start = ptr<int>(c->cell_start);
     g.hmax = ptr<double>(c->hmax);
+    g.bmax = ptr<double>(c->bmax);
     for (int k = 0; k < 12; k++) g.level_off[k] = c->level_off[k];
     return g;
 }
 
 // ---------------------------------------------------------------- kernels
+// Gathers positions/velocities into sorted order. Positions must lie in
+// [0, box) (the periodic domain the octree covers; the search prunes nodes
+// by their geometric boxes): others are reported as GZ_ERR_ARG.
 __global__ void k_gather_inputs(int n, const int *__restrict__ perm, const double *__restrict__ pos,
                                 const double *__restrict__ vel, double *x, double *y, double *z, double *vx,
-                                double *vy, double *vz)
+                                double *vy, double *vz, double box, DevStatus *st)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const size_t o = (size_t)perm[s];
-    x[s] = pos[3 * o]; y[s] = pos[3 * o + 1]; z[s] = pos[3 * o + 2];
+    const double px = pos[3 * o], py = pos[3 * o + 1], pz = pos[3 * o + 2];
+    if (!(px >= 0 && px < box && py >= 0 && py < box && pz >= 0 && pz < box)) record_status(st, GZ_ERR_ARG, s);
+    x[s] = px; y[s] = py; z[s] = pz;
     vx[s] = vel[3 * o]; vy[s] = vel[3 * o + 1]; vz[s] = vel[3 * o + 2];
 }
 
@@ -340,25 +349,27 @@ int build_grid(gz_context *c)
 {
     const int n = c->n;
     cudaStream_t s = c->stream;
-    int F = 1;
-    while (F < 10 && (1ll << (3 * F)) * 2 < (long long)n) F++;
-    c->F = F;
-    const long long ncell = 1ll << (3 * F);
+    int D = 1;  // dense top levels: about 8 particles per level-D node on average
+    while (D < 8 && (1ll << (3 * D)) * 8 < (long long)n) D++;
+    c->D = D;
+    const long long ncell = 1ll << (3 * D);
     long long total = 0;
-    for (int L = 0; L <= F; L++) { c->level_off[L] = total; total += 1ll << (3 * L); }
-    if (ensure(c, c->keys, sizeof(uint32_t) * (size_t)std::max(n, 1)) ||
-        ensure(c, c->keys_sorted, sizeof(uint32_t) * (size_t)std::max(n, 1)) ||
-        ensure(c, c->idx, sizeof(int) * (size_t)std::max(n, 1)) ||
-        ensure(c, c->cell_start, sizeof(int) * (size_t)(ncell + 1)) || ensure(c, c->hmax, sizeof(double) * (size_t)total))
+    for (int L = 0; L <= D; L++) { c->level_off[L] = total; total += 1ll << (3 * L); }
+    const size_t N = (size_t)std::max(n, 1);
+    if (ensure(c, c->keys, sizeof(unsigned long long) * N) || ensure(c, c->keys_sorted, sizeof(unsigned long long) * N) ||
+        ensure(c, c->idx, sizeof(int) * N) || ensure(c, c->cell_start, sizeof(int) * (size_t)(ncell + 1)) ||
+        ensure(c, c->hmax, sizeof(double) * (size_t)total) || ensure(c, c->bmax, sizeof(double) * (N / 32 + 1)))
         return c->err;
-    grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, F, ptr<uint32_t>(c->keys), ptr<int>(c->idx), s);
+    grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, ptr<unsigned long long>(c->keys), ptr<int>(c->idx), s);
     size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, ptr<uint32_t>(c->keys), ptr<uint32_t>(c->keys_sorted), ptr<int>(c->idx),
-                                    ptr<int>(c->perm), n, 0, 3 * F, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, ptr<unsigned long long>(c->keys),
+                                    ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n, 0,
+                                    63, s);
     if (ensure(c, c->cub_tmp, tmp)) return c->err;
-    cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, ptr<uint32_t>(c->keys), ptr<uint32_t>(c->keys_sorted),
-                                    ptr<int>(c->idx), ptr<int>(c->perm), n, 0, 3 * F, s);
-    grid_cell_start(n, ptr<uint32_t>(c->keys_sorted), F, ptr<int>(c->cell_start), s);
+    cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, ptr<unsigned long long>(c->keys),
+                                    ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n, 0,
+                                    63, s);
+    grid_cell_start(n, ptr<unsigned long long>(c->keys_sorted), D, ptr<int>(c->cell_start), s);
     if (n > 0) k_inverse<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->inv));
     GZ_CUDA(c, cudaGetLastError());
     c->grid_valid = true;
@@ -367,9 +378,8 @@ int build_grid(gz_context *c)
 
 int refresh_hmax(gz_context *c)
 {
-    grid_hmax(c->n, ptr<uint32_t>(c->keys_sorted), ptr<double>(c->h), c->F, ptr<double>(c->hmax), c->level_off,
-              c->stream);
-    c->launches += (c->n > 0 ? 1 : 0) + c->F;
+    c->launches += grid_hmax(c->n, ptr<unsigned long long>(c->keys_sorted), ptr<double>(c->h), c->D,
+                             ptr<double>(c->hmax), c->level_off, ptr<double>(c->bmax), c->stream);
     GZ_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -422,10 +432,10 @@ int gz_destroy(gz_context *c)
                      &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
                      &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
                      &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
-                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->acc, &c->h_built, &c->scratch,
+                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->bmax, &c->acc, &c->h_built, &c->scratch,
                      &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
                      &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
-                     &c->o_dt, &c->o_h, &c->o_cond};
+                     &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
     for (DevBuf *b : all) release(*b);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -461,7 +471,8 @@ static int stage_inputs(gz_context *c)
         const unsigned blocks = (unsigned)((n + 255) / 256);
         k_gather_inputs<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->stage3), ptr<double>(c->o_vel),
                                                ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z),
-                                               ptr<double>(c->vx), ptr<double>(c->vy), ptr<double>(c->vz));
+                                               ptr<double>(c->vx), ptr<double>(c->vy), ptr<double>(c->vz),
+                                               c->prm.box_size, ptr<DevStatus>(c->status));
         c->launches += 1;
         struct { DevBuf *src; DevBuf *dst; } one_in[] = {
             {&c->o_mass, &c->m}, {&c->o_u, &c->u}, {&c->o_dt, &c->dt}, {&c->o_h, &c->h}, {&c->o_cond, &c->cond}};
@@ -496,7 +507,7 @@ int gz_upload(gz_context *c, const gz_particles *in)
     const size_t N = (size_t)std::max(n, 1);
     DevBuf *one[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
                      &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig, &c->dtmass,
-                     &c->dmass, &c->h_built, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond};
+                     &c->dmass, &c->h_built, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
     for (DevBuf *b : one)
         if (ensure(c, *b, sizeof(double) * N)) return c->err;
     if (ensure(c, c->nvt, sizeof(double) * 6 * N) || ensure(c, c->pv, sizeof(double) * 3 * N) ||
@@ -671,6 +682,7 @@ int gz_download(gz_context *c, const gz_outputs *o)
     const int n = c->n;
     if (n == 0) return GZ_OK;
     cudaStream_t s = c->stream;
+    if (ensure(c, c->dl, sizeof(double) * 9 * (size_t)n)) return c->err;
     struct { double *dst; DevBuf *src; int k; } f[] = {
         {o->h, &c->h, 1}, {o->num_ngb, &c->num_ngb, 1}, {o->drkern, &c->drkern, 1}, {o->divvel, &c->divvel, 1},
         {o->rho, &c->rho, 1}, {o->pressure, &c->pressure, 1}, {o->nvt, &c->nvt, 6}, {o->cond, &c->cond, 1},
@@ -679,9 +691,12 @@ int gz_download(gz_context *c, const gz_outputs *o)
     for (auto &e : f) {
         if (!e.dst) continue;
         const long long cnt = (long long)n * e.k;
+        if ((size_t)cnt * sizeof(double) > c->dl.bytes || (size_t)cnt * sizeof(double) > e.src->bytes)
+            return fail(c, GZ_ERR_CAPACITY, "download staging smaller than the field");
         k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, e.k, ptr<int>(c->perm), ptr<double>(*e.src),
-                                                                      ptr<double>(c->stage));
-        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->stage.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+                                                                      ptr<double>(c->dl));
+        c->launches++;
+        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaStreamSynchronize(s));
     }
     struct { double *dst; int off; } g[] = {{o->grad_rho, 0}, {o->grad_p, 3}, {o->grad_v, 6}};
@@ -689,15 +704,18 @@ int gz_download(gz_context *c, const gz_outputs *o)
         if (!e.dst) continue;
         const int k = (e.off == 6) ? 9 : 3;
         const long long cnt = (long long)n * k;
+        if ((size_t)cnt * sizeof(double) > c->dl.bytes) return fail(c, GZ_ERR_CAPACITY, "download staging too small");
         k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, k, ptr<int>(c->perm),
                                                                       ptr<double>(c->grad) + (size_t)e.off * n,
-                                                                      ptr<double>(c->stage));
-        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->stage.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+                                                                      ptr<double>(c->dl));
+        c->launches++;
+        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaStreamSynchronize(s));
     }
     if (o->iters) {
-        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters), ptr<int>(c->stage));
-        GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->stage.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters), ptr<int>(c->dl));
+        c->launches++;
+        GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
     }
     GZ_CUDA(c, cudaGetLastError());
     GZ_CUDA(c, cudaStreamSynchronize(s));
@@ -711,13 +729,18 @@ static int rows_to_host(gz_context *c, const int *active, int n_active, int na, 
                         std::vector<long long> &h_off, std::vector<int> &h_nbr, std::vector<int> &order)
 {
     const int n = c->n;
+    cudaStream_t s = c->stream;
     std::vector<long long> o((size_t)na + 1);
     std::vector<int> tg((size_t)std::max(na, 1)), perm((size_t)std::max(n, 1));
-    GZ_CUDA(c, cudaMemcpy(o.data(), off.p, sizeof(long long) * ((size_t)na + 1), cudaMemcpyDeviceToHost));
+    // the rows were written on the context's (non-blocking) stream: copy back on it
+    GZ_CUDA(c, cudaMemcpyAsync(o.data(), off.p, sizeof(long long) * ((size_t)na + 1), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
     std::vector<int> e((size_t)std::max(o[(size_t)na], 1ll));
-    if (o[(size_t)na] > 0) GZ_CUDA(c, cudaMemcpy(e.data(), nbr.p, sizeof(int) * (size_t)o[(size_t)na], cudaMemcpyDeviceToHost));
-    if (na > 0) GZ_CUDA(c, cudaMemcpy(tg.data(), c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToHost));
-    if (n > 0) GZ_CUDA(c, cudaMemcpy(perm.data(), c->perm.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+    if (o[(size_t)na] > 0)
+        GZ_CUDA(c, cudaMemcpyAsync(e.data(), nbr.p, sizeof(int) * (size_t)o[(size_t)na], cudaMemcpyDeviceToHost, s));
+    if (na > 0) GZ_CUDA(c, cudaMemcpyAsync(tg.data(), c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToHost, s));
+    if (n > 0) GZ_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
     std::vector<int> slot_of_orig((size_t)std::max(n, 1), -1);
     for (int a = 0; a < na; a++) slot_of_orig[(size_t)perm[(size_t)tg[(size_t)a]]] = a;
     const int rows = active ? n_active : n;
@@ -817,7 +840,9 @@ int gz_status(gz_context *c, gz_status_info *info)
     info->index = -1;
     if (c->err_index >= 0 && c->err_index < c->n && c->perm.p) {
         int orig = -1;
-        if (cudaMemcpy(&orig, ptr<int>(c->perm) + c->err_index, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+        if (cudaMemcpyAsync(&orig, ptr<int>(c->perm) + c->err_index, sizeof(int), cudaMemcpyDeviceToHost, c->stream) ==
+                cudaSuccess &&
+            cudaStreamSynchronize(c->stream) == cudaSuccess)
             info->index = orig;
     }
     info->density_iterations = c->last_iters;
@@ -829,10 +854,10 @@ int gz_status(gz_context *c, gz_status_info *info)
                      &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
                      &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
                      &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
-                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->acc, &c->h_built, &c->scratch,
+                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->bmax, &c->acc, &c->h_built, &c->scratch,
                      &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
                      &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
-                     &c->o_dt, &c->o_h, &c->o_cond};
+                     &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
     for (DevBuf *b : all) bytes += b->bytes;
     info->device_bytes = (int64_t)bytes;
     snprintf(info->message, sizeof(info->message), "%s", c->msg);

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #define GZ_DEV __device__ __forceinline__
+// pair and per-particle math: callable from host code too (CPU emulation in tests)
+#define GZ_HD __host__ __device__ __forceinline__
 
 namespace gz {
 

@@ -9,10 +9,10 @@
 namespace gz {
 
 // grid.cu
-void grid_keys(int n, const double *pos, double box, int F, uint32_t *keys, int *idx, cudaStream_t s);
-void grid_cell_start(int n, const uint32_t *skeys, int F, int *start, cudaStream_t s);
-void grid_hmax(int n, const uint32_t *skeys, const double *h, int F, double *hmax, const long long *level_off,
-               cudaStream_t s);
+void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s);
+void grid_cell_start(int n, const unsigned long long *skeys, int D, int *start, cudaStream_t s);
+int grid_hmax(int n, const unsigned long long *skeys, const double *h, int D, double *hmax, const long long *level_off,
+              double *bmax, cudaStream_t s);
 void walk_rows(const Grid &g, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
                const long long *off, int *nbr, DevStatus *st, cudaStream_t s);

@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
             if ((r2 >= hi2) && (r2 >= hjd * hjd)) continue;
             const T r = Real<T>::sqrt_(T(r2));
             T wk_i = T(0), dwk_i = T(0);
-            if (r < hi) k_main(p.kernel, r * hinv, hinv3, hinv4, wk_i, dwk_i);
+            const bool in_i = Real<T>::inside(r, r2, hi, hid);
+            if (in_i) k_main(p.kernel, Real<T>::below_one(r * hinv), hinv3, hinv4, wk_i, dwk_i);
             if ((double)r > maxdist) maxdist = (double)r;
             T d[5];
             d[0] = T(rhoj) - rho_i;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
                 const double dq = (double)d[q];
                 if (dq < mn[q]) mn[q] = dq; else if (dq > mx[q]) mx[q] = dq;
             }
-            if (r < hi) {
+            if (in_i) {
                 const T dp[3] = {T(dx), T(dy), T(dz)};
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
@@ -292,16 +293,14 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
             Side<T> SJ;
             load_side(ps, j, p.gamma, SJ);
             PairFlux<T> F;
-            double sign;
-            if (i < j) {
-                const T dp[3] = {T(dx), T(dy), T(dz)};
-                force_pair(p.kernel, mfv, p.selfgravity_off, gc, SI, SJ, dp, r2, hid, hjd, F, stop);
-                sign = 1.0;
-            } else {
-                const T dp[3] = {T(-dx), T(-dy), T(-dz)};
-                force_pair(p.kernel, mfv, p.selfgravity_off, gc, SJ, SI, dp, r2, hjd, hid, F, stop);
-                sign = -1.0;
-            }
+            // one call site for both orientations: the lower sorted index is the
+            // R side, so rows i and j run the identical instruction sequence on
+            // identical operands and get bit-identical fluxes
+            const bool fwd = i < j;
+            const double sign = fwd ? 1.0 : -1.0;
+            const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
+            force_pair(p.kernel, mfv, p.selfgravity_off, gc, fwd ? SI : SJ, fwd ? SJ : SI, dp, r2, fwd ? hid : hjd,
+                       fwd ? hjd : hid, F, stop);
             if (!F.valid) continue;
             const double frho = sign * (double)F.rho;
             acc[0] += sign * (double)F.v[0];

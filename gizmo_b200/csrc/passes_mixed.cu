@@ -4,9 +4,16 @@
 
 namespace gz {
 
+// The density sums feed the bracketed kernel-length iteration, whose
+// accept/bracket decisions are discontinuous in NumNgb, DrkernNgb, NV_T and
+// the face weights: computing them in FP32 moves the converged h of any
+// particle whose count sits within ~1e-7 of a band edge by up to the band
+// width (~1e-3). The mixed form therefore takes them in FP64 -- the same
+// kernel as the FP64 form, so both forms converge to identical h -- and uses
+// FP32 for the gradient and force pair arithmetic.
 void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s)
 {
-    launch_density_sums<float>(p, ps, w, tpt, s);
+    density_sums_fp64(p, ps, w, tpt, s);
 }
 
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,

@@ -16,32 +16,45 @@ namespace gz {
 
 template <typename T> struct Real;
 template <> struct Real<double> {
-    static GZ_DEV double min_real() { return 1e-56; }  // MIN_REAL_NUMBER
-    static GZ_DEV double sqrt_(double x) { return sqrt(x); }
-    static GZ_DEV double pow_(double x, double y) { return pow(x, y); }
-    static GZ_DEV bool isnan_(double x) { return isnan(x); }
+    static GZ_HD double min_real() { return 1e-56; }  // MIN_REAL_NUMBER
+    static GZ_HD double sqrt_(double x) { return sqrt(x); }
+    static GZ_HD double pow_(double x, double y) { return pow(x, y); }
+    static GZ_HD bool isnan_(double x) { return isnan(x); }
+    // HLLC degenerate-wave tolerance 1e-12 (|S_L| + |S_R| + MIN_REAL), reimann.h:570
+    static GZ_HD double hllc_tol(double s) { return 1.e-12 * (s + 1e-56); }
+    // kernel support as the reference decides it: on r = sqrt(r2) < h
+    static GZ_HD bool inside(double r, double /*r2d*/, double h, double /*hd*/) { return r < h; }
+    static GZ_HD double below_one(double u) { return u; }
 };
 template <> struct Real<float> {
     // smallest value of the same role that FP32 represents (normal float)
-    static GZ_DEV float min_real() { return 1e-37f; }
-    static GZ_DEV float sqrt_(float x) { return sqrtf(x); }
-    static GZ_DEV float pow_(float x, float y) { return powf(x, y); }
-    static GZ_DEV bool isnan_(float x) { return isnan(x); }
+    static GZ_HD float min_real() { return 1e-37f; }
+    static GZ_HD float sqrt_(float x) { return sqrtf(x); }
+    static GZ_HD float pow_(float x, float y) { return powf(x, y); }
+    static GZ_HD bool isnan_(float x) { return isnan(x); }
+    // same tolerance, floored at the smallest normal so the all-zero vacuum
+    // state (S_L = S_M = S_R = 0) is still trapped instead of dividing 0 by 0
+    static GZ_HD float hllc_tol(float s) { return fmaxf(1.e-12f * s, 1e-37f); }
+    // kernel support decided on the exact FP64 r2 < h^2 (the same pairs as the
+    // FP64 form); FP32 rounding of r may reach h there, so u is kept below 1
+    // and a pair inside the support never has both kernel weights zero
+    static GZ_HD bool inside(float, double r2d, float, double hd) { return r2d < hd * hd; }
+    static GZ_HD float below_one(float u) { return u < 1.0f ? u : 0.99999994f; }
 };
 
-template <typename T> GZ_DEV T dmax(T a, T b) { return (a > b) ? a : b; }  // DMAX, macros.h:219
-template <typename T> GZ_DEV T dmin(T a, T b) { return (a < b) ? a : b; }  // DMIN, macros.h:220
+template <typename T> GZ_HD T dmax(T a, T b) { return (a > b) ? a : b; }  // DMAX, macros.h:219
+template <typename T> GZ_HD T dmin(T a, T b) { return (a < b) ? a : b; }  // DMIN, macros.h:220
 
 // ---------------------------------------------------------------- kernel
 // kernel_hinv + kernel_main (mesh/kernel.h:245-438): K=3 cubic, K=6 Wendland C2.
-template <typename T> GZ_DEV void k_hinv(T h, T &hinv, T &hinv3, T &hinv4)
+template <typename T> GZ_HD void k_hinv(T h, T &hinv, T &hinv3, T &hinv4)
 {
     hinv = T(1.0) / h;
     hinv3 = hinv * hinv * hinv;
     hinv4 = hinv3 * hinv;
 }
 
-template <typename T> GZ_DEV void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T &dwk)
+template <typename T> GZ_HD void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T &dwk)
 {
     if (u >= T(1)) { wk = T(0); dwk = T(0); return; }
     T w, dw;
@@ -69,7 +82,7 @@ template <typename T> GZ_DEV void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T
 
 // ------------------------------------------------------------ 3x3 inverse
 // Mat3::invert (math_types/mat3.h:50-63) + matrix_invert_ndims (core/proto.h:75-95).
-GZ_DEV double invert3(const double T[3][3], double Ti[3][3])
+GZ_HD double invert3(const double T[3][3], double Ti[3][3])
 {
     double fro = (T[0][0] * T[0][0] + T[0][1] * T[0][1] + T[0][2] * T[0][2]) +
                  (T[1][0] * T[1][0] + T[1][1] * T[1][1] + T[1][2] * T[1][2]) +
@@ -98,7 +111,7 @@ GZ_DEV double invert3(const double T[3][3], double Ti[3][3])
 
 // NV_T inversion with conditioning + face-closure error
 // (density_loop.h:572-637; density_loop.cc:444-504). acc: raw sums.
-GZ_DEV void nvt_invert(double h, double NumNgb, const double *acc_nvt, const double *acc_face, double &CN,
+GZ_HD void nvt_invert(double h, double NumNgb, const double *acc_nvt, const double *acc_face, double &CN,
                        double Tn[3][3], double &fce)
 {
     const double V_i = kVolNorm * pow(h, 3.0) / (NumNgb > 0 ? NumNgb : 1.0);
@@ -145,7 +158,7 @@ struct PassParams {
 
 // DensitySpec::after_iter_body for gas (density_loop.h:515-961). acc[14]:
 // Ngb Rho DrkernNgb DivVel NVT(6) face(3) -. Returns 1 when converged.
-GZ_DEV int after_iter(const PassParams &p, int iter, double h, const double *acc, double cond_prev, DensityScratch &sc,
+GZ_HD int after_iter(const PassParams &p, int iter, double h, const double *acc, double cond_prev, DensityScratch &sc,
                       double &new_h_out, int &stop)
 {
     double desnumngb = p.des_num_ngb;
@@ -275,7 +288,7 @@ GZ_DEV int after_iter(const PassParams &p, int iter, double h, const double *acc
 
 // ---------------------------------------------------------- gradients
 // local_slopelimiter, Newtonian branch (gradients_loop.cc:76-104).
-GZ_DEV void slopelimiter(double *g, double valmax, double valmin, double alim, double h, double shoot_tol,
+GZ_HD void slopelimiter(double *g, double valmax, double valmin, double alim, double h, double shoot_tol,
                          int pos_preserve, double d_max, double val_cen)
 {
     double d_abs = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
@@ -294,7 +307,7 @@ GZ_DEV void slopelimiter(double *g, double valmax, double valmin, double alim, d
     }
 }
 
-template <typename T> GZ_DEV void sym_matvec(const T *s, const T *v, T *o)
+template <typename T> GZ_HD void sym_matvec(const T *s, const T *v, T *o)
 {  // SymmetricTensor2::matvec (symmetric_tensor2.h:80-84)
     const T a = s[0] * v[0] + s[3] * v[1] + s[5] * v[2];
     const T b = s[3] * v[0] + s[1] * v[1] + s[4] * v[2];
@@ -308,12 +321,12 @@ template <typename T> struct RVec { Crv<T> L, R; };
 template <typename T> struct ROut { T P_M, S_M; Crv<T> F; };
 template <typename T> struct GConst { T G0, G1, G2, G3, G4, G5, G6, G7, G8, G9; int mfv; };
 
-template <typename T> GZ_DEV T dot3(const T *a, const T *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-template <typename T> GZ_DEV T nsq3(const T *a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }
+template <typename T> GZ_HD T dot3(const T *a, const T *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+template <typename T> GZ_HD T nsq3(const T *a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }
 
 // get_wavespeeds_and_pressure_star (reimann.h:485-549)
 template <typename T>
-GZ_DEV void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, T hL, T hR, T &SLo, T &SRo,
+GZ_HD void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, T hL, T hR, T &SLo, T &SRo,
                        T ptl, const GConst<T> &gc)
 {
     const T MR = Real<T>::min_real();
@@ -361,13 +374,13 @@ GZ_DEV void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T 
 
 // HLLC_fluxes, MFV, face frame (reimann.h:559-615)
 template <typename T>
-GZ_DEV void hllc_fluxes(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T hL, T hR, T S_L, T S_R)
+GZ_HD void hllc_fluxes(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T hL, T hR, T S_L, T S_R)
 {
     const T P_M = o.P_M, S_M = o.S_M;
     if ((P_M <= T(0)) || Real<T>::isnan_(P_M)) return;
     T nfac, eK, dv2, vf = T(0);
     {
-        const T tol_s = T(1.e-12) * (fabs(S_L) + fabs(S_R) + Real<T>::min_real());
+        const T tol_s = Real<T>::hllc_tol(fabs(S_L) + fabs(S_R));
         if ((fabs(S_M - S_L) < tol_s) || (fabs(S_M - S_R) < tol_s) || (fabs(S_M - vf) < tol_s)) {
             o.F.rho = T(0);
             o.F.p = o.P_M * o.S_M;
@@ -406,7 +419,7 @@ GZ_DEV void hllc_fluxes(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T
 
 // Riemann_solver_KurganovTadmor_PWK (reimann.h:445-477), SLOPE_LIMITER_TOLERANCE 1
 template <typename T>
-GZ_DEV void riemann_kt(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, T hL, T hR,
+GZ_HD void riemann_kt(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, T hL, T hR,
                        const GConst<T> &gc)
 {
     T S_L, S_R, S_M, alpha;
@@ -438,7 +451,7 @@ GZ_DEV void riemann_kt(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T 
 
 // guess_for_pressure (reimann.h:1025-1062)
 template <typename T>
-GZ_DEV T guess_pressure(const RVec<T> &rv, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD T guess_pressure(const RVec<T> &rv, T vL, T vR, T cL, T cR, const GConst<T> &gc)
 {
     const T pv = T(0.5) * (rv.L.p + rv.R.p) - T(0.125) * (vR - vL) * (rv.L.p + rv.R.p) * (cL + cR);
     const T pmin = dmin(rv.L.p, rv.R.p), pmax = dmax(rv.L.p, rv.R.p);
@@ -459,7 +472,7 @@ GZ_DEV T guess_pressure(const RVec<T> &rv, T vL, T vR, T cL, T cR, const GConst<
 
 // iterative_Riemann_solver (reimann.h:965-1020), NMAX_ITER 1000, TOL_ITER 1e-6
 template <typename T>
-GZ_DEV int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T cR, const GConst<T> &gc)
 {
     T Pg, Pg_prev, W_L = T(0), W_R = T(0), Z_L, Z_R, tol, pratio;
     int niter = 0;
@@ -504,7 +517,7 @@ GZ_DEV int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T 
 
 // vacuum / fan sampling at S = 0 (reimann.h:672-840)
 template <typename T>
-GZ_DEV void sample_vac_left(const RVec<T> &rv, ROut<T> &o, const T *n, T vR, T cR, const GConst<T> &gc)
+GZ_HD void sample_vac_left(const RVec<T> &rv, ROut<T> &o, const T *n, T vR, T cR, const GConst<T> &gc)
 {
     const T S = T(0), S_R = vR - gc.G4 * cR;
     if (!gc.mfv) { o.P_M = T(0); o.S_M = S_R; return; }
@@ -522,7 +535,7 @@ GZ_DEV void sample_vac_left(const RVec<T> &rv, ROut<T> &o, const T *n, T vR, T c
 }
 
 template <typename T>
-GZ_DEV void sample_vac_right(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T cL, const GConst<T> &gc)
+GZ_HD void sample_vac_right(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T cL, const GConst<T> &gc)
 {
     const T S = T(0), S_L = vL + gc.G4 * cL;
     if (!gc.mfv) { o.P_M = T(0); o.S_M = S_L; return; }
@@ -540,7 +553,7 @@ GZ_DEV void sample_vac_right(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T 
 }
 
 template <typename T>
-GZ_DEV void sample_vac_internal(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD void sample_vac_internal(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc)
 {
     const T S = T(0), S_L = vL + gc.G4 * cL, S_R = vR - gc.G4 * cR;
     if (S <= S_L) sample_vac_right(rv, o, n, vL, cL, gc);
@@ -558,7 +571,7 @@ GZ_DEV void sample_vac_internal(const RVec<T> &rv, ROut<T> &o, const T *n, T vL,
 }
 
 template <typename T>
-GZ_DEV void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc)
 {
     if (!gc.mfv) return;
     const T S = T(0);
@@ -625,7 +638,7 @@ GZ_DEV void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T v
 }
 
 // convert_face_to_flux (reimann.h:1070-1083)
-template <typename T> GZ_DEV void face_to_flux(ROut<T> &o, const T *n, const GConst<T> &gc)
+template <typename T> GZ_HD void face_to_flux(ROut<T> &o, const T *n, const GConst<T> &gc)
 {
     const T rho = o.F.rho, P = o.F.p;
     T v[3] = {o.F.v[0], o.F.v[1], o.F.v[2]};
@@ -639,7 +652,7 @@ template <typename T> GZ_DEV void face_to_flux(ROut<T> &o, const T *n, const GCo
 
 // Riemann_solver_exact (reimann.h:625-664)
 template <typename T>
-GZ_DEV void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
+GZ_HD void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
                           int &stop)
 {
     if ((rv.L.p == T(0) && rv.R.p == T(0)) || (rv.L.rho == T(0) && rv.R.rho == T(0))) {
@@ -660,7 +673,7 @@ GZ_DEV void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR,
 
 // Riemann_solver, hydro branch (reimann.h:282-370); rv taken by value as in the reference
 template <typename T>
-GZ_DEV void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GConst<T> &gc, int &stop)
+GZ_HD void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GConst<T> &gc, int &stop)
 {
     if ((rv.L.p < T(0) && rv.R.p < T(0)) || (rv.L.rho < T(0)) || (rv.R.rho < T(0))) { o.P_M = T(0); return; }
     rv.L.cs = Real<T>::sqrt_(gc.G0 * rv.L.p / rv.L.rho);
@@ -686,7 +699,7 @@ GZ_DEV void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GCon
 
 // reconstruct_face_states, non-MHD (reimann.h:125-244)
 template <typename T>
-GZ_DEV void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, const T *d_j, T &Q_L, T &Q_R, int mode)
+GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, const T *d_j, T &Q_L, T &Q_R, int mode)
 {
     if (mode == 0) { Q_R = Q_i; Q_L = Q_j; return; }
     if (Q_i == Q_j) { Q_L = Q_R = Q_i; return; }
@@ -741,7 +754,7 @@ template <typename T> struct PairFlux {
 // r2 its exact FP64 square. The support test uses r2 in FP64 so both forms
 // pick the same pairs.
 template <typename T>
-GZ_DEV void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc, const Side<T> &I, const Side<T> &J,
+GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc, const Side<T> &I, const Side<T> &J,
                        const T dp[3], double r2d, double hi_d, double hj_d, PairFlux<T> &out, int &stop)
 {
     out.valid = 0;
@@ -761,9 +774,9 @@ GZ_DEV void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc
     T hinv_i, hinv3_i, hinv4_i, hinv_j, hinv3_j, hinv4_j;
     T wk_i = T(0), dwk_i = T(0), wk_j = T(0), dwk_j = T(0);
     k_hinv(I.h, hinv_i, hinv3_i, hinv4_i);
-    if (r < I.h) k_main(kf, r * hinv_i, hinv3_i, hinv4_i, wk_i, dwk_i);
+    if (Real<T>::inside(r, r2d, I.h, hi_d)) k_main(kf, Real<T>::below_one(r * hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
     k_hinv(J.h, hinv_j, hinv3_j, hinv4_j);
-    if (r < J.h) k_main(kf, r * hinv_j, hinv3_j, hinv4_j, wk_j, dwk_j);
+    if (Real<T>::inside(r, r2d, J.h, hj_d)) k_main(kf, Real<T>::below_one(r * hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
     const T cnumcrit2 = T(kCnDanger) * T(kCnDanger) - I.cond * I.cond;
     T eps_big = T(0.5), eps_small = T(1.e-3);
     if (!mfv && !selfgravity_off) { eps_small = T(1.e-2); eps_big = T(0.6); }
@@ -904,7 +917,7 @@ GZ_DEV void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc
 // with this side's flux f_rho, its own dt and the other's, returns this side's
 // dMass increment, the accepted flux for its GravWorkTerm, and the write it
 // makes on the other side's dMass.
-GZ_DEV void mfv_mass_side(double f_rho, double dt_self, double dt_other, double m_self, double m_other,
+GZ_HD void mfv_mass_side(double f_rho, double dt_self, double dt_other, double m_self, double m_other,
                           double &dmass_self, double &accepted, double &dmass_other)
 {
     double dmass_holder = f_rho * dt_self, lim;

@@ -31,14 +31,19 @@ struct Particles {
     const unsigned char *active;    // 1 for particles of the current active set
 };
 
-// Octree pyramid over the sorted particles: fine level F has 8^F cells;
-// an octree node (level L, Morton index m) owns the sorted range
-// [cell_start[m << 3(F-L)], cell_start[(m+1) << 3(F-L)]).
+// Implicit octree over the Morton-sorted particles (63-bit keys, 21 levels):
+// node (level L, Morton index m) owns the sorted run of keys with prefix m.
+// The top D levels have a dense table of node starts (cell_start, level D)
+// and node maxima of h (hmax, levels 0..D); below D, children are found by
+// binary search in `keys` and h maxima come from 32-particle block maxima.
 struct Grid {
-    int F;
+    int D;
+    int n;
     double box;
-    const int *cell_start;          // [8^F + 1]
-    const double *hmax;             // node maxima of h, all levels
+    const unsigned long long *keys; // sorted keys [n]
+    const int *cell_start;          // [8^D + 1]
+    const double *hmax;             // node maxima of h, levels 0..D
+    const double *bmax;             // [ceil(n/32)] block maxima of h
     long long level_off[12];
 };
 

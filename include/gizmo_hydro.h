@@ -78,7 +78,8 @@ typedef struct gz_params {
 /* Inputs per gas particle (the P / CellP fields the pass reads). */
 typedef struct gz_particles {
     int64_t       n;
-    const double *pos;    /* [n][3] P[i].Pos, inside [0, box_size) */
+    const double *pos;    /* [n][3] P[i].Pos, inside [0, box_size); a position outside is
+                             reported as GZ_ERR_ARG (with its index) by the next pass */
     const double *vel;    /* [n][3] CellP[i].VelPred */
     const double *mass;   /* [n]    P[i].Mass */
     const double *u;      /* [n]    CellP[i].InternalEnergyPred */
