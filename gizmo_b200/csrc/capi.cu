@@ -41,14 +41,13 @@ struct gz_context {
     DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
     DevBuf dl;                       // download staging, [9][n] doubles (widest output field)
     long long launches = 0;          // kernels of this library launched by the context
-    // grid
-    int D = 1;
-    DevBuf cell_start, hmax, bmax;
-    long long level_off[12] = {0};
+    // octree over the sorted particles
+    DevBuf t_node, t_lo, t_hi, t_parent, t_done, t_nch, t_cpos;
+    int t_nodes = 0, t_levels = 0;
     bool grid_valid = false;
-    // density work
-    DevBuf acc, h_built, scratch, keep, todo_a, todo_b, row_of, flag, counts, d_off, d_nbr, n_sel;
-    long long d_nbr_cap = 0;
+    // density work: rows are [d_beg[t], d_end[t]) in d_nbr; d_used entries are taken
+    DevBuf acc, h_built, scratch, keep, regrow, todo_a, todo_b, grow, d_beg, d_end, flag, counts, d_off, d_nbr, n_sel;
+    long long d_nbr_cap = 0, d_used = 0;
     // symmetric rows (shared by gradients and force)
     DevBuf s_off, s_nbr, s_counts;
     long long s_nbr_cap = 0;
@@ -153,19 +152,29 @@ Particles view(gz_context *c)
     return ps;
 }
 
-Grid grid_view(gz_context *c)
+std::vector<DevBuf *> all_buffers(gz_context *c)
 {
-    Grid g{};
-    g.D = c->D;
-    g.n = c->n;
-    g.box = c->prm.box_size;
-    g.keys = ptr<unsigned long long>(c->keys_sorted);
-    g.cell_start = ptr<int>(c->cell_start);
-    g.hmax = ptr<double>(c->hmax);
-    g.bmax = ptr<double>(c->bmax);
-    for (int k = 0; k < 12; k++) g.level_off[k] = c->level_off[k];
-    return g;
+    return {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
+            &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
+            &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
+            &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
+            &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
+            &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
+            &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
+            &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
+
+Tree tree_view(gz_context *c)
+{
+    Tree t{};
+    t.box = c->prm.box_size;
+    t.n_nodes = c->t_nodes;
+    t.node = ptr<int4>(c->t_node);
+    t.lo = ptr<double4>(c->t_lo);
+    t.hi = ptr<double4>(c->t_hi);
+    return t;
+}
+
 
 // ---------------------------------------------------------------- kernels
 // Gathers positions/velocities into sorted order. Positions must lie in
@@ -233,8 +242,7 @@ __global__ void k_set_active(int na, const int *__restrict__ t, unsigned char *f
     if (a < na) flag[t[a]] = 1;
 }
 
-__global__ void k_density_prep(int na, const int *__restrict__ t, double *h, double maxsoft, DensityScratch *sc,
-                               int *row_of)
+__global__ void k_density_prep(int na, const int *__restrict__ t, double *h, double maxsoft, DensityScratch *sc)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= na) return;
@@ -244,17 +252,23 @@ __global__ void k_density_prep(int na, const int *__restrict__ t, double *h, dou
     h[i] = hv;
     DensityScratch z{};
     sc[i] = z;
-    row_of[i] = a;
 }
 
-__global__ void k_rows_of(int na, const int *__restrict__ t, int *row_of, const double *__restrict__ h, double f,
-                          double *h_built)
+// search radius of the density rows about to be built for t[0..na)
+__global__ void k_row_radius(int na, const int *__restrict__ t, const double *__restrict__ h, double f, double *h_built)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < na) h_built[t[a]] = h[t[a]] * f;
+}
+
+// rows just built for t[0..na) at nbr + base: record them per particle
+__global__ void k_set_rows(int na, const int *__restrict__ t, const long long *__restrict__ off, long long base,
+                           long long *beg, long long *end)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= na) return;
-    const int i = t[a];
-    row_of[i] = a;
-    h_built[i] = h[i] * f;
+    beg[t[a]] = base + off[a];
+    end[t[a]] = base + off[a + 1];
 }
 
 // ------------------------------------------------------------ host helpers
@@ -309,24 +323,32 @@ int exclusive_scan_counts(gz_context *c, int rows, DevBuf &counts, DevBuf &off, 
     return 0;
 }
 
+// Exact neighbour rows of `targets` (count walk, scan, fill walk), written
+// at nbr + base; the first `base` entries of nbr are kept if it must grow.
 int build_rows(gz_context *c, const double *reach, int symmetric, const int *targets, int rows, DevBuf &counts,
-               DevBuf &off, DevBuf &nbr, long long &cap, long long *total)
+               DevBuf &off, DevBuf &nbr, long long &cap, long long *total, long long base = 0)
 {
     cudaStream_t s = c->stream;
-    Grid g = grid_view(c);
+    Tree t = tree_view(c);
     if (ensure(c, counts, sizeof(int) * (size_t)std::max(rows, 1))) return c->err;
-    walk_rows(g, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
               rows, ptr<int>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
-    if (*total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
-    if (*total > cap || !nbr.p) {
-        if (ensure(c, nbr, sizeof(int) * (size_t)std::max(*total, 1ll))) return c->err;
+    if (base + *total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
+    if (base + *total > cap || !nbr.p) {
+        const long long want = std::max(base + *total, base > 0 ? cap + cap / 2 : 0ll);
+        DevBuf grown;
+        if (ensure(c, grown, sizeof(int) * (size_t)std::max(want, 1ll))) return c->err;
+        if (base > 0) GZ_CUDA(c, cudaMemcpyAsync(grown.p, nbr.p, sizeof(int) * (size_t)base, cudaMemcpyDeviceToDevice, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+        release(nbr);
+        nbr = grown;
         cap = (long long)(nbr.bytes / sizeof(int));
     }
-    walk_rows(g, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<int>(counts), ptr<long long>(off), ptr<int>(nbr), ptr<DevStatus>(c->status), s);
+    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+              rows, ptr<int>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     return 0;
@@ -349,16 +371,9 @@ int build_grid(gz_context *c)
 {
     const int n = c->n;
     cudaStream_t s = c->stream;
-    int D = 1;  // dense top levels: about 8 particles per level-D node on average
-    while (D < 8 && (1ll << (3 * D)) * 8 < (long long)n) D++;
-    c->D = D;
-    const long long ncell = 1ll << (3 * D);
-    long long total = 0;
-    for (int L = 0; L <= D; L++) { c->level_off[L] = total; total += 1ll << (3 * L); }
     const size_t N = (size_t)std::max(n, 1);
     if (ensure(c, c->keys, sizeof(unsigned long long) * N) || ensure(c, c->keys_sorted, sizeof(unsigned long long) * N) ||
-        ensure(c, c->idx, sizeof(int) * N) || ensure(c, c->cell_start, sizeof(int) * (size_t)(ncell + 1)) ||
-        ensure(c, c->hmax, sizeof(double) * (size_t)total) || ensure(c, c->bmax, sizeof(double) * (N / 32 + 1)))
+        ensure(c, c->idx, sizeof(int) * N))
         return c->err;
     grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, ptr<unsigned long long>(c->keys), ptr<int>(c->idx), s);
     size_t tmp = 0;
@@ -369,17 +384,78 @@ int build_grid(gz_context *c)
     cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, ptr<unsigned long long>(c->keys),
                                     ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n, 0,
                                     63, s);
-    grid_cell_start(n, ptr<unsigned long long>(c->keys_sorted), D, ptr<int>(c->cell_start), s);
     if (n > 0) k_inverse<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->inv));
     GZ_CUDA(c, cudaGetLastError());
-    c->grid_valid = true;
     return 0;
 }
 
+// Octree over the sorted keys, split top-down one level per step (the size of
+// the next level is read back each step), then boxes and h maxima bottom-up.
+int build_tree(gz_context *c)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    c->t_nodes = 0;
+    c->t_levels = 0;
+    if (n == 0) return 0;
+    long long cap = std::max<long long>(1024, n / 4);
+    if (c->t_node.bytes >= sizeof(int4) * 1024) cap = std::max<long long>(cap, (long long)(c->t_node.bytes / sizeof(int4)));
+    if (ensure(c, c->t_node, sizeof(int4) * (size_t)cap) || ensure(c, c->t_parent, sizeof(int) * (size_t)cap))
+        return c->err;
+    const int4 root = make_int4(0, n, -1, 0);
+    const int no_parent = -1;
+    GZ_CUDA(c, cudaMemcpyAsync(c->t_node.p, &root, sizeof(int4), cudaMemcpyHostToDevice, s));
+    GZ_CUDA(c, cudaMemcpyAsync(c->t_parent.p, &no_parent, sizeof(int), cudaMemcpyHostToDevice, s));
+    int beg = 0, cnt = 1, L = 0;
+    const unsigned long long *keys = ptr<unsigned long long>(c->keys_sorted);
+    while (cnt > 0) {
+        if (ensure(c, c->t_nch, sizeof(int) * (size_t)cnt)) return c->err;
+        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<int>(c->t_nch), s);
+        c->launches++;
+        long long next = 0;
+        if (exclusive_scan_counts(c, cnt, c->t_nch, c->t_cpos, &next)) return c->err;
+        const long long end = (long long)beg + cnt;
+        if (end + next > INT32_MAX) return fail(c, GZ_ERR_CAPACITY, "octree exceeds capacity");
+        if (end + next > cap) {
+            // grow, keeping the nodes built so far
+            const long long want = std::max(end + next, cap * 2);
+            DevBuf gn, gp;
+            if (ensure(c, gn, sizeof(int4) * (size_t)want) || ensure(c, gp, sizeof(int) * (size_t)want)) return c->err;
+            GZ_CUDA(c, cudaMemcpyAsync(gn.p, c->t_node.p, sizeof(int4) * (size_t)end, cudaMemcpyDeviceToDevice, s));
+            GZ_CUDA(c, cudaMemcpyAsync(gp.p, c->t_parent.p, sizeof(int) * (size_t)end, cudaMemcpyDeviceToDevice, s));
+            GZ_CUDA(c, cudaStreamSynchronize(s));
+            release(c->t_node);
+            release(c->t_parent);
+            c->t_node = gn;
+            c->t_parent = gp;
+            cap = want;
+        }
+        tree_write(keys, L, ptr<int4>(c->t_node), ptr<int>(c->t_parent), beg, cnt, ptr<long long>(c->t_cpos), (int)end, s);
+        c->launches++;
+        GZ_CUDA(c, cudaGetLastError());
+        beg = (int)end;
+        cnt = (int)next;
+        L++;
+    }
+    c->t_nodes = beg;
+    c->t_levels = L;
+    if (ensure(c, c->t_lo, sizeof(double4) * (size_t)c->t_nodes) || ensure(c, c->t_hi, sizeof(double4) * (size_t)c->t_nodes) ||
+        ensure(c, c->t_done, sizeof(int) * (size_t)c->t_nodes))
+        return c->err;
+    tree_up(c->t_nodes, ptr<int4>(c->t_node), ptr<int>(c->t_parent), ptr<double>(c->x), ptr<double>(c->y),
+            ptr<double>(c->z), ptr<double>(c->h), ptr<double4>(c->t_lo), ptr<double4>(c->t_hi), ptr<int>(c->t_done), 1, s);
+    c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// node maxima of h after the radii changed
 int refresh_hmax(gz_context *c)
 {
-    c->launches += grid_hmax(c->n, ptr<unsigned long long>(c->keys_sorted), ptr<double>(c->h), c->D,
-                             ptr<double>(c->hmax), c->level_off, ptr<double>(c->bmax), c->stream);
+    tree_up(c->t_nodes, ptr<int4>(c->t_node), ptr<int>(c->t_parent), ptr<double>(c->x), ptr<double>(c->y),
+            ptr<double>(c->z), ptr<double>(c->h), ptr<double4>(c->t_lo), ptr<double4>(c->t_hi), ptr<int>(c->t_done), 0,
+            c->stream);
+    if (c->t_nodes > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -428,15 +504,7 @@ int gz_destroy(gz_context *c)
     if (!c) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf *all[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
-                     &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
-                     &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
-                     &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
-                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->bmax, &c->acc, &c->h_built, &c->scratch,
-                     &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
-                     &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
-                     &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
-    for (DevBuf *b : all) release(*b);
+    for (DevBuf *b : all_buffers(c)) release(*b);
     cudaStreamDestroy(c->stream);
     delete c;
     return GZ_OK;
@@ -454,9 +522,9 @@ int gz_set_params(gz_context *c, const gz_params *params)
 
 void *gz_stream(gz_context *c) { return c ? (void *)c->stream : nullptr; }
 
-// Rebuild the neighbour grid and the sorted mirror from the resident inputs
-// (the state a pass starts from): Morton keys, radix sort, gathers, zeroed
-// outputs.
+// Rebuild the sorted mirror and the octree from the resident inputs (the
+// state a pass starts from): Morton keys, radix sort, gathers, zeroed
+// outputs, tree.
 static int stage_inputs(gz_context *c)
 {
     const int n = c->n;
@@ -467,7 +535,7 @@ static int stage_inputs(gz_context *c)
     c->msg[0] = 0;
     if (n > 0) {
         if (build_grid(c)) return c->err;
-        c->launches += 3;  // keys, cell starts, inverse permutation
+        c->launches += 2;  // keys, inverse permutation
         const unsigned blocks = (unsigned)((n + 255) / 256);
         k_gather_inputs<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->stage3), ptr<double>(c->o_vel),
                                                ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z),
@@ -490,7 +558,9 @@ static int stage_inputs(gz_context *c)
         GZ_CUDA(c, cudaMemsetAsync(c->gw.p, 0, sizeof(double) * 3 * (size_t)n, s));
         GZ_CUDA(c, cudaMemsetAsync(c->iters.p, 0, sizeof(int) * (size_t)n, s));
         GZ_CUDA(c, cudaGetLastError());
+        if (build_tree(c)) return c->err;
     }
+    c->grid_valid = true;
     c->have_density = c->have_gradients = false;
     c->sym_valid = false;
     return 0;
@@ -517,7 +587,7 @@ int gz_upload(gz_context *c, const gz_particles *in)
         ensure(c, c->stage3, sizeof(double) * 3 * N) || ensure(c, c->o_vel, sizeof(double) * 3 * N) ||
         ensure(c, c->perm, sizeof(int) * N) || ensure(c, c->inv, sizeof(int) * N) ||
         ensure(c, c->acc, sizeof(double) * 17 * N) || ensure(c, c->scratch, sizeof(DensityScratch) * N) ||
-        ensure(c, c->row_of, sizeof(int) * N))
+        ensure(c, c->d_beg, sizeof(long long) * N) || ensure(c, c->d_end, sizeof(long long) * N))
         return c->err;
     if (n > 0) {
         GZ_CUDA(c, cudaMemcpyAsync(c->stage3.p, in->pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
@@ -555,42 +625,52 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
     const int n = c->n;
     if (ensure(c, c->todo_a, sizeof(int) * (size_t)std::max(na, 1)) ||
         ensure(c, c->todo_b, sizeof(int) * (size_t)std::max(na, 1)) ||
-        ensure(c, c->keep, (size_t)std::max(na, 1)) || ensure(c, c->flag, sizeof(int)) ||
-        ensure(c, c->n_sel, sizeof(int)))
+        ensure(c, c->grow, sizeof(int) * (size_t)std::max(na, 1)) || ensure(c, c->keep, (size_t)std::max(na, 1)) ||
+        ensure(c, c->regrow, (size_t)std::max(na, 1)) || ensure(c, c->flag, sizeof(int)) ||
+        ensure(c, c->n_sel, sizeof(int) * 2))
         return c->err;
     if (na > 0) {
         k_density_prep<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<double>(c->h),
-                                                         c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch),
-                                                         ptr<int>(c->row_of));
+                                                         c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch));
         c->launches++;
     }
     GZ_CUDA(c, cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToDevice, s));
     int n_todo = na;
     int *todo = ptr<int>(c->todo_a), *todo_next = ptr<int>(c->todo_b);
-    bool need_rows = true;
+    // Rows at the buffered radius (DensitySpec's CSR buffer factor) are built
+    // for every target first; afterwards only the particles whose radius
+    // outgrew their row get a new row, appended behind the others.
+    const int *grow = todo;
+    int n_grow = n_todo;
+    long long base = 0;
+    c->pairs_density = 0;
     int iter = 0;
     for (iter = 0; iter < kMaxIter && n_todo > 0; iter++) {
-        if (need_rows) {
-            // rows for every still-iterating particle at the buffered radius
-            k_rows_of<<<(n_todo + 255) / 256, 256, 0, s>>>(n_todo, todo, ptr<int>(c->row_of), ptr<double>(c->h),
-                                                            kDensityBuffer, ptr<double>(c->h_built));
+        if (n_grow > 0) {
+            k_row_radius<<<(n_grow + 255) / 256, 256, 0, s>>>(n_grow, grow, ptr<double>(c->h), kDensityBuffer,
+                                                               ptr<double>(c->h_built));
             c->launches++;
             long long total = 0;
-            if (build_rows(c, ptr<double>(c->h_built), 0, todo, n_todo, c->counts, c->d_off, c->d_nbr, c->d_nbr_cap,
-                           &total))
+            if (build_rows(c, ptr<double>(c->h_built), 0, grow, n_grow, c->counts, c->d_off, c->d_nbr, c->d_nbr_cap,
+                           &total, base))
                 return c->err;
-            need_rows = false;
+            k_set_rows<<<(n_grow + 255) / 256, 256, 0, s>>>(n_grow, grow, ptr<long long>(c->d_off), base,
+                                                             ptr<long long>(c->d_beg), ptr<long long>(c->d_end));
+            c->launches++;
+            base += total;
+            c->pairs_density += total;
         }
         DensityWork w{};
         w.todo = todo;
         w.n_todo = n_todo;
-        w.row_of = ptr<int>(c->row_of);
-        w.rows.off = ptr<long long>(c->d_off);
-        w.rows.nbr = ptr<int>(c->d_nbr);
+        w.beg = ptr<long long>(c->d_beg);
+        w.end = ptr<long long>(c->d_end);
+        w.nbr = ptr<int>(c->d_nbr);
         w.acc = ptr<double>(c->acc);
         w.h_built = ptr<double>(c->h_built);
         w.scratch = ptr<DensityScratch>(c->scratch);
         w.keep = ptr<unsigned char>(c->keep);
+        w.regrow = ptr<unsigned char>(c->regrow);
         w.rebuild = ptr<int>(c->flag);
         w.iter = iter;
         GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
@@ -601,18 +681,30 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         GZ_CUDA(c, cudaGetLastError());
         size_t tmp = 0;
         cub::DeviceSelect::Flagged(nullptr, tmp, todo, ptr<unsigned char>(c->keep), todo_next, ptr<int>(c->n_sel), n_todo, s);
-        if (ensure(c, c->cub_tmp, tmp)) return c->err;
+        size_t tmp2 = 0;
+        cub::DeviceSelect::Flagged(nullptr, tmp2, todo, ptr<unsigned char>(c->regrow), ptr<int>(c->grow),
+                                   ptr<int>(c->n_sel) + 1, n_todo, s);
+        if (ensure(c, c->cub_tmp, std::max(tmp, tmp2))) return c->err;
         cub::DeviceSelect::Flagged(c->cub_tmp.p, tmp, todo, ptr<unsigned char>(c->keep), todo_next, ptr<int>(c->n_sel),
                                    n_todo, s);
-        int hv[2] = {0, 0};
+        int hv[3] = {0, 0, 0};
+        GZ_CUDA(c, cudaMemcpyAsync(&hv[2], c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaMemcpyAsync(&hv[0], c->n_sel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GZ_CUDA(c, cudaMemcpyAsync(&hv[1], c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaStreamSynchronize(s));
+        n_grow = 0;
+        if (hv[2]) {
+            cub::DeviceSelect::Flagged(c->cub_tmp.p, tmp2, todo, ptr<unsigned char>(c->regrow), ptr<int>(c->grow),
+                                       ptr<int>(c->n_sel) + 1, n_todo, s);
+            GZ_CUDA(c, cudaMemcpyAsync(&hv[1], ptr<int>(c->n_sel) + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            GZ_CUDA(c, cudaStreamSynchronize(s));
+            n_grow = hv[1];
+            grow = ptr<int>(c->grow);
+        }
         n_todo = hv[0];
-        need_rows = hv[1] != 0;
         std::swap(todo, todo_next);
     }
     c->last_iters = iter;
+    c->d_used = base;
     density_finalize(c->pp, ps, ptr<double>(c->acc), ptr<int>(c->targets), na, s);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
@@ -794,19 +886,22 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
     if (na > 0)
-        k_rows_of<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<int>(c->row_of), ptr<double>(c->h), 1.0,
-                                                    ptr<double>(c->h_built));
+        k_row_radius<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<double>(c->h), 1.0,
+                                                       ptr<double>(c->h_built));
     long long total = 0;
     if (build_rows(c, ptr<double>(c->h_built), 0, ptr<int>(c->targets), na, c->counts, c->d_off, c->d_nbr,
                    c->d_nbr_cap, &total))
         return c->err;
+    if (na > 0)
+        k_set_rows<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<long long>(c->d_off), 0,
+                                                    ptr<long long>(c->d_beg), ptr<long long>(c->d_end));
     Particles ps = view(c);
     DensityWork w{};
     w.todo = ptr<int>(c->targets);
     w.n_todo = na;
-    w.row_of = ptr<int>(c->row_of);
-    w.rows.off = ptr<long long>(c->d_off);
-    w.rows.nbr = ptr<int>(c->d_nbr);
+    w.beg = ptr<long long>(c->d_beg);
+    w.end = ptr<long long>(c->d_end);
+    w.nbr = ptr<int>(c->d_nbr);
     w.acc = ptr<double>(c->acc);
     if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
     else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);
@@ -850,15 +945,7 @@ int gz_status(gz_context *c, gz_status_info *info)
     info->pairs_density = c->pairs_density;
     info->pairs_symmetric = c->pairs_symmetric;
     size_t bytes = 0;
-    DevBuf *all[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
-                     &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
-                     &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
-                     &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
-                     &c->targets, &c->targets_tmp, &c->cell_start, &c->hmax, &c->bmax, &c->acc, &c->h_built, &c->scratch,
-                     &c->keep, &c->todo_a, &c->todo_b, &c->row_of, &c->flag, &c->counts, &c->d_off, &c->d_nbr,
-                     &c->n_sel, &c->s_off, &c->s_nbr, &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u,
-                     &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
-    for (DevBuf *b : all) bytes += b->bytes;
+    for (DevBuf *b : all_buffers(c)) bytes += b->bytes;
     info->device_bytes = (int64_t)bytes;
     snprintf(info->message, sizeof(info->message), "%s", c->msg);
     return GZ_OK;

@@ -1,22 +1,25 @@
-// gizmo_b200/csrc/grid.cu -- Morton neighbour grid and exact neighbour rows.
+// gizmo_b200/csrc/grid.cu -- Morton-sorted octree and exact neighbour rows.
 //
 // Replaces the reference's SIDX spatial index + BVH walk + two-pass CSR
 // (src/mesh/gpu_neighbor_list.cc:1134-1169, 1736-1816;
 // src/mesh/gpu_neighbor_list.h:207-264). Particles are sorted by a 63-bit
-// Morton key (21 bits per axis), which makes an implicit octree of 21 levels
-// in which every node is one contiguous run of the sorted arrays. The top D
-// levels have a dense table of node starts and node maxima of h; a deeper
-// node's children are found by binary search inside the parent's run, so a
-// 1e5 density contrast costs a few extra levels, not a finer table. Maxima
-// of h below level D come from per-32-particle block maxima.
+// Morton key (21 bits per axis); every octree node is then one contiguous
+// run of the sorted arrays. The tree is explicit: it is split top-down one
+// level per launch (a node with more than kLeafMax particles gets its
+// non-empty children, stored contiguously), then a single bottom-up launch
+// gives every node the tight bounding box of its particles and the maximum
+// of their h. A 1e5 density contrast only adds levels where the particles
+// are, and the walk never searches: a node's children are one index range.
 //
-// Neighbour rows are produced by a warp-cooperative walk: one warp takes 32
-// consecutive sorted targets, descends the octree once for the whole group
-// (a node survives when any lane's search sphere reaches it), and streams
-// each surviving leaf through the warp 32 candidates at a time, every lane
-// testing its own target. Membership uses the reference
-// predicates on FP64 minimum-image separations rounded exactly as the CPU
-// does, so the rows are bit-identical to an exact CPU search:
+// Neighbour rows come from a warp-cooperative walk: one warp takes 32
+// consecutive sorted targets and descends the tree once for the group. A node
+// is opened when the search sphere of at least one lane reaches its box (each
+// lane tests its own target), so 32 targets on both sides of a jump of the
+// Morton curve cost two small searches, not one search of their joint
+// bounding box. Leaf particles are staged through shared memory, and every
+// lane whose sphere reached the leaf tests them. Membership uses the
+// reference predicates on FP64 minimum-image separations rounded exactly as
+// the CPU does, so the rows are bit-identical to an exact CPU search:
 //   one-way   r2 < R_i^2                                (density, R = buffered h)
 //   symmetric r2 > 0 and !(r2 >= h_i^2 and r2 >= h_j^2) (gradients, force)
 #include <cub/cub.cuh>
@@ -38,17 +41,6 @@ GZ_DEV unsigned long long spread21(unsigned long long x)
     return x;
 }
 
-GZ_DEV unsigned long long compact21(unsigned long long x)
-{
-    x &= 0x1249249249249249ull;
-    x = (x | (x >> 2)) & 0x10c30c30c30c30c3ull;
-    x = (x | (x >> 4)) & 0x100f00f00f00f00full;
-    x = (x | (x >> 8)) & 0x1f0000ff0000ffull;
-    x = (x | (x >> 16)) & 0x1f00000000ffffull;
-    x = (x | (x >> 32)) & 0x1fffffull;
-    return x;
-}
-
 __global__ void k_keys(int n, const double *__restrict__ pos, double box, unsigned long long *keys, int *idx)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -64,59 +56,6 @@ __global__ void k_keys(int n, const double *__restrict__ pos, double box, unsign
     idx[i] = i;
 }
 
-// first sorted position of every level-D node (lower bound of the key prefixes)
-__global__ void k_cell_start(int n, const unsigned long long *__restrict__ skeys, int shift, long long ncell, int *start)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const long long k = (long long)(skeys[i] >> shift);
-    const long long kp = (i == 0) ? -1 : (long long)(skeys[i - 1] >> shift);
-    for (long long c = kp + 1; c <= k; c++) start[c] = i;
-    if (i == n - 1)
-        for (long long c = k + 1; c <= ncell; c++) start[c] = n;
-}
-
-__global__ void k_fill_int(long long count, int *p, int v)
-{
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < count) p[i] = v;
-}
-
-__global__ void k_hmax_fine(int n, const unsigned long long *__restrict__ skeys, int shift, const double *__restrict__ h,
-                            unsigned long long *hmax_fine)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double hv = h[i] > 0 ? h[i] : 0.0;  // non-negative doubles order as their bit patterns
-    atomicMax(hmax_fine + (skeys[i] >> shift), (unsigned long long)__double_as_longlong(hv));
-}
-
-__global__ void k_hmax_level(long long nodes, const double *__restrict__ child, double *parent)
-{
-    const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (m >= nodes) return;
-    double v = 0;
-    for (int k = 0; k < 8; k++) v = fmax(v, child[8 * m + k]);
-    parent[m] = v;
-}
-
-__global__ void k_block_max(int n, const double *__restrict__ h, double *bmax)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const double v = (i < n && h[i] > 0) ? h[i] : 0.0;
-    const double m = warp_max(v, 0xffffffffu, 32);
-    if ((threadIdx.x & 31) == 0 && i < n) bmax[i >> 5] = m;
-}
-
-// periodic gap between a node interval [o, o+s) and a point on one axis
-GZ_DEV double point_gap(double x, double o, double s, double box)
-{
-    double d = fabs(x - (o + 0.5 * s));
-    if (d > 0.5 * box) d = box - d;
-    d -= 0.5 * s;
-    return d > 0 ? d : 0;
-}
-
 // first position in [a, b) whose key is >= key
 GZ_DEV int lower_bound_key(const unsigned long long *__restrict__ keys, int a, int b, unsigned long long key)
 {
@@ -127,70 +66,179 @@ GZ_DEV int lower_bound_key(const unsigned long long *__restrict__ keys, int a, i
     return a;
 }
 
-constexpr int kStack = 176;
-constexpr int kLeaf = 32;
+// The run [a, b) of a level-L node split into its 8 children (level L+1):
+// child d is [bound[d], bound[d+1]).
+GZ_DEV void child_bounds(const unsigned long long *__restrict__ keys, int a, int b, int L, int bound[9])
+{
+    const int shift = 3 * (kBits - L - 1);
+    const unsigned long long prefix = keys[a] >> (shift + 3);
+    bound[0] = a;
+    int lo = a;
+    for (int d = 0; d < 7; d++) {
+        lo = lower_bound_key(keys, lo, b, ((prefix << 3) + (unsigned long long)(d + 1)) << shift);
+        bound[d + 1] = lo;
+    }
+    bound[8] = b;
+}
 
-// Warp-cooperative octree walk. FILL=false counts rows; FILL=true writes them.
-// A node is descended when the search sphere of at least one lane reaches
-// it (each lane tests its own target against the node box), so 32 targets
-// that straddle a jump of the Morton curve cost two small searches, not one
-// search of their joint bounding box. Leaf candidates are staged in shared
-// memory and read back by every lane as broadcasts.
+// number of non-empty children of every node of one level
+__global__ void k_tree_count(const unsigned long long *__restrict__ keys, int L, const int4 *__restrict__ node,
+                             int beg, int cnt, int *nch)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    const int4 nd = node[beg + i];
+    int c = 0;
+    if (nd.y > kLeafMax && L < kBits) {
+        int bound[9];
+        child_bounds(keys, nd.x, nd.x + nd.y, L, bound);
+        for (int d = 0; d < 8; d++) c += bound[d + 1] > bound[d];
+    }
+    nch[i] = c;
+}
+
+// children of one level written at next + cpos[i] (cpos: inclusive scan of nch)
+__global__ void k_tree_write(const unsigned long long *__restrict__ keys, int L, int4 *node, int *parent, int beg,
+                             int cnt, const long long *__restrict__ cpos, int next)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    int4 nd = node[beg + i];
+    const int first_child = next + (int)cpos[i];
+    const int c = (int)(cpos[i + 1] - cpos[i]);
+    if (c == 0) {
+        nd.z = -1;
+        nd.w = 0;
+    } else {
+        int bound[9];
+        child_bounds(keys, nd.x, nd.x + nd.y, L, bound);
+        int k = 0;
+        for (int d = 0; d < 8; d++) {
+            if (bound[d + 1] > bound[d]) {
+                node[first_child + k] = make_int4(bound[d], bound[d + 1] - bound[d], -1, 0);
+                parent[first_child + k] = beg + i;
+                k++;
+            }
+        }
+        nd.z = first_child;
+        nd.w = c;
+    }
+    node[beg + i] = nd;
+}
+
+// L2-coherent 32-byte load/store (values written by other blocks of this launch)
+GZ_DEV double4 ld_cg4(const double4 *p)
+{
+    const double2 a = __ldcg((const double2 *)p), b = __ldcg((const double2 *)p + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+GZ_DEV void st_cg4(double4 *p, double4 v)
+{
+    __stcg((double2 *)p, make_double2(v.x, v.y));
+    __stcg((double2 *)p + 1, make_double2(v.z, v.w));
+}
+
+// Bottom-up bounding boxes and h maxima in one launch: a leaf reduces its
+// particles, and the last child to finish (atomic count per parent) reduces
+// the parent's children, and so on to the root. With boxes == 0 only the h
+// maxima (lo.w) are refreshed.
+__global__ void k_tree_up(int n_nodes, const int4 *__restrict__ node, const int *__restrict__ parent,
+                          const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
+                          const double *__restrict__ h, double4 *lo, double4 *hi, int *done, int boxes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) return;
+    const int4 nd = node[i];
+    if (nd.z >= 0) return;  // internal: reduced by its last child
+    double4 l = make_double4(1e300, 1e300, 1e300, 0.0), u = make_double4(-1e300, -1e300, -1e300, 0.0);
+    for (int j = nd.x; j < nd.x + nd.y; j++) {
+        if (boxes) {
+            const double px = x[j], py = y[j], pz = z[j];
+            l.x = fmin(l.x, px); l.y = fmin(l.y, py); l.z = fmin(l.z, pz);
+            u.x = fmax(u.x, px); u.y = fmax(u.y, py); u.z = fmax(u.z, pz);
+        }
+        const double hv = h[j];
+        if (hv > l.w) l.w = hv;
+    }
+    if (boxes) { lo[i] = l; hi[i] = u; } else { lo[i].w = l.w; }
+    int p = parent[i];
+    while (p >= 0) {
+        __threadfence();
+        const int4 pn = node[p];
+        if (atomicAdd(done + p, 1) != pn.w - 1) return;
+        __threadfence();
+        l = make_double4(1e300, 1e300, 1e300, 0.0);
+        u = make_double4(-1e300, -1e300, -1e300, 0.0);
+        for (int c = pn.z; c < pn.z + pn.w; c++) {
+            const double4 cl = ld_cg4(lo + c);
+            if (boxes) {
+                const double4 cu = ld_cg4(hi + c);
+                l.x = fmin(l.x, cl.x); l.y = fmin(l.y, cl.y); l.z = fmin(l.z, cl.z);
+                u.x = fmax(u.x, cu.x); u.y = fmax(u.y, cu.y); u.z = fmax(u.z, cu.z);
+            }
+            l.w = fmax(l.w, cl.w);
+        }
+        if (boxes) { st_cg4(lo + p, l); st_cg4(hi + p, u); } else { __stcg(&lo[p].w, l.w); }
+        p = parent[p];
+    }
+}
+
+// Periodic gap between a point and a box [l, u] on one axis (both inside
+// [0, box)), minus an absolute allowance for the rounding of the subtractions.
+GZ_DEV double axis_gap(double x, double l, double u, double box, double eps)
+{
+    double g;
+    if (x < l) g = fmin(l - x, x + box - u);
+    else if (x > u) g = fmin(x - u, l + box - x);
+    else return 0.0;
+    g -= eps;
+    return g > 0 ? g : 0.0;
+}
+
+constexpr int kStack = 160;  // >= 7 x 22 levels + 8
+
+// Warp-cooperative tree walk. FILL=false counts rows; FILL=true writes them.
 template <bool SYM, bool FILL>
-__global__ void __launch_bounds__(256) k_walk(Grid g, const double *__restrict__ x, const double *__restrict__ y,
+__global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
                                               const double *__restrict__ z, const double *__restrict__ reach,
                                               const double *__restrict__ hsym, const int *__restrict__ targets,
                                               int n_targets, int *counts, const long long *__restrict__ off,
                                               int *nbr, DevStatus *st)
 {
-    __shared__ unsigned long long s_m[8][kStack];
-    __shared__ int2 s_ab[8][kStack];
-    __shared__ unsigned char s_L[8][kStack];
+    __shared__ int s_stack[8][kStack];
     __shared__ double4 s_c[8][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int slot = group * 32 + lane;
-    if (group * 32 >= n_targets) return;
+    if (group * 32 >= n_targets) return;  // whole warp
     const bool valid = slot < n_targets;
-    const int t = valid ? targets[slot] : -1;
-    const double box = g.box, half = 0.5 * box;
+    const int tg = valid ? targets[slot] : -1;
+    const double box = t.box, half = 0.5 * box, eps = 4e-16 * box;
     double xi = 0, yi = 0, zi = 0, ri = 0;
-    if (valid) { xi = x[t]; yi = y[t]; zi = z[t]; ri = reach[t]; }
+    if (valid) { xi = x[tg]; yi = y[tg]; zi = z[tg]; ri = reach[tg]; }
     const unsigned full = 0xffffffffu;
     const double ri2 = ri * ri;
     long long base = 0;
     if (FILL && valid) base = off[slot];
     int cnt = 0;
-    if (lane == 0) { s_m[wib][0] = 0ull; s_ab[wib][0] = make_int2(0, g.n); s_L[wib][0] = 0; }
+    if (lane == 0) s_stack[wib][0] = 0;
     int sp = 1;
     __syncwarp();
-    const int D = g.D;
     while (sp > 0) {
         sp--;
-        const unsigned long long m = s_m[wib][sp];
-        const int2 ab = s_ab[wib][sp];
-        const int L = s_L[wib][sp];
+        const int ni = s_stack[wib][sp];
         __syncwarp();
-        const int a = ab.x, b = ab.y;
-        double R = ri;
-        if (SYM) {
-            double hn;
-            if (L <= D) {
-                hn = g.hmax[g.level_off[L] + (long long)m];
-            } else {
-                double v = 0;
-                for (int blk = (a >> 5) + lane; blk <= ((b - 1) >> 5); blk += 32) v = fmax(v, g.bmax[blk]);
-                hn = warp_max(v, full, 32);
-            }
-            R = fmax(R, hn);
-        }
-        const double s = box / (double)(1ll << L);
-        const double gx = point_gap(xi, (double)compact21(m) * s, s, box);
-        const double gy = point_gap(yi, (double)compact21(m >> 1) * s, s, box);
-        const double gz = point_gap(zi, (double)compact21(m >> 2) * s, s, box);
-        const bool need = valid && (gx * gx + gy * gy + gz * gz <= R * R * (1.0 + 1e-9) + 1e-300);
+        const int4 nd = t.node[ni];
+        const double4 bl = t.lo[ni], bu = t.hi[ni];
+        const double R = SYM ? fmax(ri, bl.w) : ri;
+        const double gx = axis_gap(xi, bl.x, bu.x, box, eps);
+        const double gy = axis_gap(yi, bl.y, bu.y, box, eps);
+        const double gz = axis_gap(zi, bl.z, bu.z, box, eps);
+        const bool need = valid && (gx * gx + gy * gy + gz * gz <= R * R * (1.0 + 1e-9));
         if (!__any_sync(full, need)) continue;
-        if (L == kBits || b - a <= kLeaf) {
+        if (nd.z < 0) {
+            // leaf: stream its particles through shared memory, 32 at a time
+            const int a = nd.x, b = nd.x + nd.y;
             for (int c0 = a; c0 < b; c0 += 32) {
                 const int jl = c0 + lane;
                 if (jl < b) s_c[wib][lane] = make_double4(x[jl], y[jl], z[jl], SYM ? hsym[jl] : 0.0);
@@ -214,36 +262,13 @@ __global__ void __launch_bounds__(256) k_walk(Grid g, const double *__restrict__
             }
             continue;
         }
-        // expand into the 8 children (level L+1): ranges from the dense table
-        // above level D, by binary search inside [a, b) below it
-        if (sp + 8 > kStack) {
-            if (lane == 0) record_status(st, 5 /* GZ_ERR_CAPACITY */, t);
+        if (sp + nd.w > kStack) {
+            if (lane == 0) record_status(st, 5 /* GZ_ERR_CAPACITY */, tg);
             break;
         }
-        const unsigned long long child = 8ull * m + (unsigned long long)(lane & 7);
-        int ca, cb;
-        if (L + 1 <= D) {
-            const int sh = 3 * (D - L - 1);
-            ca = g.cell_start[child << sh];
-            cb = g.cell_start[(child + 1) << sh];
-        } else {
-            const int sh = 3 * (kBits - L - 1);
-            int lo = a;
-            if (lane < 8 && (lane & 7) != 0) lo = lower_bound_key(g.keys, a, b, child << sh);
-            ca = (lane & 7) == 0 ? a : lo;
-            const int nxt = __shfl_down_sync(full, ca, 1);
-            cb = ((lane & 7) == 7) ? b : nxt;
-        }
-        const unsigned nonempty = __ballot_sync(full, lane < 8 && cb > ca);
-        const int npush = __popc(nonempty);
-        // push the non-empty children so that child 0 is popped first
-        if (lane < 8 && cb > ca) {
-            const int pos = sp + __popc(nonempty >> (lane + 1));
-            s_m[wib][pos] = child;
-            s_ab[wib][pos] = make_int2(ca, cb);
-            s_L[wib][pos] = (unsigned char)(L + 1);
-        }
-        sp += npush;
+        // push the children so that the first child is popped first
+        if (lane < nd.w) s_stack[wib][sp + nd.w - 1 - lane] = nd.z + lane;
+        sp += nd.w;
         __syncwarp();
     }
     if (!FILL && valid) counts[slot] = cnt;
@@ -254,37 +279,26 @@ void grid_keys(int n, const double *pos, double box, unsigned long long *keys, i
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
 }
 
-void grid_cell_start(int n, const unsigned long long *skeys, int D, int *start, cudaStream_t s)
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, int *nch, cudaStream_t s)
 {
-    const long long ncell = 1ll << (3 * D);
-    if (n == 0) {
-        k_fill_int<<<(unsigned)((ncell + 1 + 255) / 256), 256, 0, s>>>(ncell + 1, start, 0);
-        return;
-    }
-    k_cell_start<<<(n + 255) / 256, 256, 0, s>>>(n, skeys, 3 * (kBits - D), ncell, start);
+    if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch);
 }
 
-int grid_hmax(int n, const unsigned long long *skeys, const double *h, int D, double *hmax, const long long *level_off,
-              double *bmax, cudaStream_t s)
+void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
+                const long long *cpos, int next, cudaStream_t s)
 {
-    double *fine = hmax + level_off[D];
-    const long long ncell = 1ll << (3 * D);
-    cudaMemsetAsync(fine, 0, sizeof(double) * (size_t)ncell, s);
-    int launches = 0;
-    if (n > 0) {
-        k_hmax_fine<<<(n + 255) / 256, 256, 0, s>>>(n, skeys, 3 * (kBits - D), h, (unsigned long long *)fine);
-        k_block_max<<<(n + 255) / 256, 256, 0, s>>>(n, h, bmax);
-        launches += 2;
-    }
-    for (int L = D - 1; L >= 0; L--) {
-        const long long nodes = 1ll << (3 * L);
-        k_hmax_level<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(nodes, hmax + level_off[L + 1], hmax + level_off[L]);
-        launches++;
-    }
-    return launches;
+    if (cnt > 0) k_tree_write<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, parent, beg, cnt, cpos, next);
 }
 
-void walk_rows(const Grid &g, const double *x, const double *y, const double *z, const double *reach,
+void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,
+             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s)
+{
+    if (n_nodes <= 0) return;
+    cudaMemsetAsync(done, 0, sizeof(int) * (size_t)n_nodes, s);
+    k_tree_up<<<(n_nodes + 127) / 128, 128, 0, s>>>(n_nodes, node, parent, x, y, z, h, lo, hi, done, boxes);
+}
+
+void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
                const long long *off, int *nbr, DevStatus *st, cudaStream_t s)
 {
@@ -292,11 +306,11 @@ void walk_rows(const Grid &g, const double *x, const double *y, const double *z,
     const int warps = (n_targets + 31) / 32;
     const int blocks = (warps + 7) / 8;
     if (symmetric) {
-        if (nbr) k_walk<true, true><<<blocks, 256, 0, s>>>(g, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
-        else k_walk<true, false><<<blocks, 256, 0, s>>>(g, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        if (nbr) k_walk<true, true><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        else k_walk<true, false><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
     } else {
-        if (nbr) k_walk<false, true><<<blocks, 256, 0, s>>>(g, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
-        else k_walk<false, false><<<blocks, 256, 0, s>>>(g, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        if (nbr) k_walk<false, true><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        else k_walk<false, false><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
     }
 }
 

@@ -10,10 +10,12 @@ namespace gz {
 
 // grid.cu
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s);
-void grid_cell_start(int n, const unsigned long long *skeys, int D, int *start, cudaStream_t s);
-int grid_hmax(int n, const unsigned long long *skeys, const double *h, int D, double *hmax, const long long *level_off,
-              double *bmax, cudaStream_t s);
-void walk_rows(const Grid &g, const double *x, const double *y, const double *z, const double *reach,
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, int *nch, cudaStream_t s);
+void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
+                const long long *cpos, int next, cudaStream_t s);
+void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,
+             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s);
+void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
                const long long *off, int *nbr, DevStatus *st, cudaStream_t s);
 
@@ -21,13 +23,15 @@ void walk_rows(const Grid &g, const double *x, const double *y, const double *z,
 struct DensityWork {
     const int *todo;        // sorted indices still iterating
     int n_todo;
-    const int *row_of;      // sorted index -> row of the density neighbour rows
-    Csr rows;
+    const long long *beg;   // sorted index -> its density row [beg, end) in nbr
+    const long long *end;
+    const int *nbr;
     double *acc;            // [17][n] per-particle accumulator (sorted index)
     double *h_built;        // search radius each row was built with
     DensityScratch *scratch;
-    unsigned char *keep;    // per todo slot
-    int *rebuild;           // set when a radius outgrows its row
+    unsigned char *keep;    // per todo slot: still iterating
+    unsigned char *regrow;  // per todo slot: its radius outgrew its row
+    int *rebuild;           // set when any radius outgrows its row
     int iter;
 };
 

@@ -24,7 +24,6 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
     if (slot >= w.n_todo) return;
     const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
     const int t = w.todo[slot];
-    const int row = w.row_of[t];
     const double xi = ps.x[t], yi = ps.y[t], zi = ps.z[t];
     const double hd = ps.h[t];
     const double h2 = hd * hd;
@@ -36,9 +35,9 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
     double a[17];
 #pragma unroll
     for (int k = 0; k < 17; k++) a[k] = 0;
-    const long long b0 = w.rows.off[row], b1 = w.rows.off[row + 1];
+    const long long b0 = w.beg[t], b1 = w.end[t];
     for (long long e = b0 + lane; e < b1; e += TPT) {
-        const int j = w.rows.nbr[e];
+        const int j = w.nbr[e];
         const double mjd = ps.m[j];
         if (mjd <= 0) continue;
         double dx, dy, dz;

@@ -40,13 +40,14 @@ __global__ void k_after_iter(PassParams p, Particles ps, DensityWork w, DevStatu
     w.scratch[t] = sc;
     ps.iters[t] = w.iter + 1;
     if (stop) record_status(st, stop, t);
-    if (conv) {
-        w.keep[s] = 0;
-    } else {
+    int regrow = 0;
+    if (!conv) {
         ps.h[t] = nh;
-        w.keep[s] = 1;
-        if (nh > w.h_built[t]) atomicExch(w.rebuild, 1);
+        regrow = nh > w.h_built[t];
+        if (regrow) atomicExch(w.rebuild, 1);
     }
+    w.keep[s] = conv ? 0 : 1;
+    w.regrow[s] = (unsigned char)regrow;
 }
 
 void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s)
@@ -70,7 +71,7 @@ __global__ void k_density_finalize(PassParams p, Particles ps, const double *__r
     if (NumNgb > 0) {
         Drk *= h / (3 * NumNgb);
         DivV /= NumNgb;
-        NumNgb *= kVolNorm * pow(h, 3.0);
+        NumNgb *= kVolNorm * cr::pow(h, 3.0);
     } else { NumNgb = Drk = DivV = 0; }
     if (Drk > -0.9) Drk = 1.0 / (1.0 + Drk); else Drk = 1.0;
     DivV *= Drk;
@@ -91,14 +92,14 @@ __global__ void k_density_finalize(PassParams p, Particles ps, const double *__r
             const double v[3] = {ps.vx[i], ps.vy[i], ps.vz[i]};
             for (int k = 0; k < 3; k++) pvl[k] = v[k] * (1.0 - eps) + pvl[k] * (eps / rho);
         }
-        if ((h > 0) && (NumNgb > 0)) rho = m * NumNgb / (kVolNorm * pow(h, 3.0));
+        if ((h > 0) && (NumNgb > 0)) rho = m * NumNgb / (kVolNorm * cr::pow(h, 3.0));
         else if (h <= 0) rho = 0;
-        else rho = m / (kVolNorm * pow(h, 3.0));
+        else rho = m / (kVolNorm * cr::pow(h, 3.0));
         ps.pressure[i] = (p.gamma - 1) * ps.u[i] * rho;
     }
     ps.rho[i] = rho;
     for (int k = 0; k < 3; k++) ps.pv[k * n + i] = pvl[k];
-    ps.num_ngb[i] = (NumNgb > 0) ? pow(NumNgb, 1.0 / 3) : 0;
+    ps.num_ngb[i] = (NumNgb > 0) ? cr::pow(NumNgb, 1.0 / 3) : 0;
 }
 
 void density_finalize(const PassParams &p, const Particles &ps, const double *acc, const int *targets, int n_targets,

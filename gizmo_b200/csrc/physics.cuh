@@ -11,6 +11,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "crmath.cuh"
 
 namespace gz {
 
@@ -114,8 +115,8 @@ GZ_HD double invert3(const double T[3][3], double Ti[3][3])
 GZ_HD void nvt_invert(double h, double NumNgb, const double *acc_nvt, const double *acc_face, double &CN,
                        double Tn[3][3], double &fce)
 {
-    const double V_i = kVolNorm * pow(h, 3.0) / (NumNgb > 0 ? NumNgb : 1.0);
-    const double norm = pow(h, -1.0);
+    const double V_i = kVolNorm * cr::pow(h, 3.0) / (NumNgb > 0 ? NumNgb : 1.0);
+    const double norm = cr::pow(h, -1.0);
     double raw[3][3], T[3][3], Tinv[3][3];
     raw[0][0] = acc_nvt[0]; raw[1][1] = acc_nvt[1]; raw[2][2] = acc_nvt[2];
     raw[0][1] = raw[1][0] = acc_nvt[3];
@@ -141,7 +142,7 @@ GZ_HD void nvt_invert(double h, double NumNgb, const double *acc_nvt, const doub
         for (int b = 0; b < 3; b++) fo[a] += 2.0 * V_i * Tn[a][b] * acc_face[b];
     double leak = 0;
     for (int a = 0; a < 3; a++) leak += fabs(fo[a]) / 3.0;
-    fce = leak / (2.0 * 3.0 * pow(dx_i, 2.0));
+    fce = leak / (2.0 * 3.0 * cr::pow(dx_i, 2.0));
 }
 
 // ------------------------------------------------------- density after_iter
@@ -168,7 +169,7 @@ GZ_HD int after_iter(const PassParams &p, int iter, double h, const double *acc,
     double NumNgb = acc[0], Drk = acc[2];
     if (NumNgb > 0) {
         Drk *= h / (3 * NumNgb);
-        NumNgb *= kVolNorm * pow(h, 3.0);
+        NumNgb *= kVolNorm * cr::pow(h, 3.0);
     } else { NumNgb = 0; Drk = 0; }
     if (Drk > -0.9) Drk = 1.0 / (1.0 + Drk); else Drk = 1.0;
     double CN, fce, Tn[3][3];
@@ -197,7 +198,7 @@ GZ_HD int after_iter(const PassParams &p, int iter, double h, const double *acc,
     desnumngb = p.des_num_ngb * ncorr;
     desnumngbdev = desnumngbdev_0 * ncorr;
     if (iter > 1)
-        desnumngbdev = dmin(0.25 * desnumngb, desnumngbdev * exp(0.1 * log(desnumngb / (16.0 * desnumngbdev)) * (double)iter));
+        desnumngbdev = dmin(0.25 * desnumngb, desnumngbdev * cr::exp(0.1 * cr::log(desnumngb / (16.0 * desnumngbdev)) * (double)iter));
     const double minsoft = p.min_kernel_radius, maxsoft = p.max_kernel_radius;
     int redo = 0, setmin = 0, setmax = 0;
     double new_h = h;
@@ -226,50 +227,50 @@ GZ_HD int after_iter(const PassParams &p, int iter, double h, const double *acc,
             }
             if (sc.right > 0 && sc.left > 0) {
                 double maxjump = 0;
-                if (iter > 1) maxjump = 0.2 * log(sc.right / sc.left);
+                if (iter > 1) maxjump = 0.2 * cr::log(sc.right / sc.left);
                 if (NumNgb > 1) {
-                    double jumpvar = Drk * log(desnumngb / NumNgb) / 3;
+                    double jumpvar = Drk * cr::log(desnumngb / NumNgb) / 3;
                     if (iter > 1) { if (fabs(jumpvar) < maxjump) { if (jumpvar < 0) jumpvar = -maxjump; else jumpvar = maxjump; } }
-                    new_h *= exp(jumpvar);
+                    new_h *= cr::exp(jumpvar);
                 } else {
                     new_h *= 2.0;
                 }
                 if ((new_h < sc.right) && (new_h > sc.left)) {
                     if (iter > 1) {
-                        const double hfac = exp(maxjump);
+                        const double hfac = cr::exp(maxjump);
                         if (new_h > sc.right / hfac) new_h = sc.right / hfac;
                         if (new_h < sc.left * hfac) new_h = sc.left * hfac;
                     }
                 } else {
                     if (new_h > sc.right) new_h = sc.right;
                     if (new_h < sc.left) new_h = sc.left;
-                    new_h = pow(new_h * sc.left * sc.right, 1.0 / 3.0);
+                    new_h = cr::pow(new_h * sc.left * sc.right, 1.0 / 3.0);
                 }
             } else {
                 if (sc.right == 0 && sc.left == 0) { stop = 90001009; new_h_out = new_h; return 1; }
                 if (sc.right == 0 && sc.left > 0) {
-                    double fac_lim = (NumNgb > 1) ? log(desnumngb / NumNgb) / 3 : 1.4;
+                    double fac_lim = (NumNgb > 1) ? cr::log(desnumngb / NumNgb) / 3 : 1.4;
                     if ((NumNgb < 2.0 * desnumngb) && (NumNgb > 0.1 * desnumngb)) {
                         double slope = Drk;
                         if (iter > 2 && slope < 1.0) slope = 0.5 * (slope + 1.0);
                         double fac = fac_lim * slope;
                         if (iter >= 4) { if (Drk == 1.0) fac *= 10.0; }
-                        if (fac < fac_lim + 0.231) new_h *= exp(fac); else new_h *= exp(fac_lim + 0.231);
+                        if (fac < fac_lim + 0.231) new_h *= cr::exp(fac); else new_h *= cr::exp(fac_lim + 0.231);
                     } else {
-                        new_h *= exp(fac_lim);
+                        new_h *= cr::exp(fac_lim);
                     }
                 }
                 if (sc.right > 0 && sc.left == 0) {
-                    double fac_lim = (NumNgb > 1) ? log(desnumngb / NumNgb) / 3 : 1.4;
+                    double fac_lim = (NumNgb > 1) ? cr::log(desnumngb / NumNgb) / 3 : 1.4;
                     if (fac_lim < -1.535) fac_lim = -1.535;
                     if ((NumNgb < 2.0 * desnumngb) && (NumNgb > 0.1 * desnumngb)) {
                         double slope = Drk;
                         if (iter > 2 && slope < 1.0) slope = 0.5 * (slope + 1.0);
                         double fac = fac_lim * slope;
                         if (iter >= 4) { if (Drk == 1.0) fac *= 10.0; }
-                        if (fac > fac_lim - 0.231) new_h *= exp(fac); else new_h *= exp(fac_lim - 0.231);
+                        if (fac > fac_lim - 0.231) new_h *= cr::exp(fac); else new_h *= cr::exp(fac_lim - 0.231);
                     } else {
-                        new_h *= exp(fac_lim);
+                        new_h *= cr::exp(fac_lim);
                     }
                 }
             }
@@ -650,9 +651,11 @@ template <typename T> GZ_HD void face_to_flux(ROut<T> &o, const T *n, const GCon
     for (int k = 0; k < 3; k++) o.F.v[k] = v[k] * o.F.rho + n[k] * P;
 }
 
-// Riemann_solver_exact (reimann.h:625-664)
+// Riemann_solver_exact (reimann.h:625-664). Taken on a small fraction of
+// faces only, so it stays out of line: its iteration does not raise the
+// register budget of the common HLLC path.
 template <typename T>
-GZ_HD void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
+__host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
                           int &stop)
 {
     if ((rv.L.p == T(0) && rv.R.p == T(0)) || (rv.L.rho == T(0) && rv.R.rho == T(0))) {

@@ -31,20 +31,18 @@ struct Particles {
     const unsigned char *active;    // 1 for particles of the current active set
 };
 
-// Implicit octree over the Morton-sorted particles (63-bit keys, 21 levels):
-// node (level L, Morton index m) owns the sorted run of keys with prefix m.
-// The top D levels have a dense table of node starts (cell_start, level D)
-// and node maxima of h (hmax, levels 0..D); below D, children are found by
-// binary search in `keys` and h maxima come from 32-particle block maxima.
-struct Grid {
-    int D;
-    int n;
+// Octree over the Morton-sorted particles (63-bit keys, 21 levels): node i
+// owns the sorted run [first, first + count); an internal node's children
+// are the nodes [child, child + nchild); a leaf (child = -1) has at most
+// kLeafMax particles unless it is at the deepest level (coincident keys).
+constexpr int kLeafMax = 32;
+
+struct Tree {
     double box;
-    const unsigned long long *keys; // sorted keys [n]
-    const int *cell_start;          // [8^D + 1]
-    const double *hmax;             // node maxima of h, levels 0..D
-    const double *bmax;             // [ceil(n/32)] block maxima of h
-    long long level_off[12];
+    int n_nodes;
+    const int4 *node;               // {first, count, child or -1, nchild}
+    const double4 *lo;              // tight box minimum xyz; w = maximum h in the node
+    const double4 *hi;              // tight box maximum xyz
 };
 
 // Compressed neighbour rows: row r of `slot_of` targets.

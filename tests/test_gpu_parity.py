@@ -6,8 +6,13 @@ Tolerances (written here, checked per field):
     DrkernNgb cancels, so its roundoff reaches ~1e-12);
   * each FP64 pass vs the oracle on the same inputs: relative 1e-10
     (element-wise; force fields use a floor of 1e-3 x the field maximum, since
-    their sums cancel); h-iteration counts equal for >= 99.5% of particles (a
-    bracket decision may flip on the last ulp of exp/log/pow);
+    their sums cancel). The h-iteration takes discontinuous decisions (band,
+    bracket, clamp) whose inputs carry the roundoff of summation order and of
+    the CPU libm, which misrounds ~1e-3 of exp/log/pow calls (the device
+    computes them correctly rounded): >= 99.9% of particles take the oracle's
+    path exactly (same iteration count, h within 1e-10), and a particle that
+    takes another path still converges inside the neighbour-count band
+    (h within 3e-3);
   * mixed form vs the FP64 form: h and density per particle 1e-5;
   * conservation per pass, both forms: |sum of pair fluxes| <= 1e-12 x sum |fluxes|
     for mass (MFV), momentum and energy.
@@ -99,9 +104,10 @@ def passwise(wl, active=None, prior_full=False):
 def check_passwise(wl, active=None, prior_full=False):
     (gd, od), (gg, og), (gf, of) = passwise(wl, active, prior_full)
     rows = np.arange(wl.n) if active is None else np.asarray(active)
-    same = gd["iters"][rows] == od["iters"][rows]
-    # an h-iteration branch may flip on the last ulp of exp/log/pow: rare, bounded
-    assert same.mean() >= 0.995, same.mean()
+    h_rel = np.abs(gd["h"][rows] - od["h"][rows]) / od["h"][rows]
+    same = (gd["iters"][rows] == od["iters"][rows]) & (h_rel <= 1e-10)
+    assert same.mean() >= 0.999, (same.mean(), int((~same).sum()))
+    assert h_rel.max() <= 3e-3, h_rel.max()
     keep = rows[same]
     for f in DENSITY_FIELDS:
         assert rel_err(gd[f][keep], od[f][keep], 1e-6) < 1e-10, f
@@ -189,11 +195,34 @@ def test_conservation_per_pass(name, precision):
         assert v <= 1e-12, (k, v)
 
 
-def test_tiny_and_duplicate_particles():
-    wl = ics.sedov(4, seed=2)
-    wl.pos[5] = wl.pos[4]  # two particles at the same place: r = 0 pairs
-    wl.params.des_num_ngb = 8.0
+def test_tiny_set():
+    wl = ics.sedov(4, seed=2)  # 64 particles: every row spans a large part of the box
+    wl.params.des_num_ngb = 16.0
+    wl.params.max_num_ngb_dev = 0.5
+    wl.params.max_kernel_radius = 0.45
     check_passwise(wl)
+
+
+def test_duplicate_particles():
+    wl = ics.sedov(8, seed=2)
+    wl.pos[5] = wl.pos[4]  # two particles at the same place: r = 0 pairs
+    check_passwise(wl)
+
+
+def test_nonconvergence_stops_like_the_reference():
+    # two coincident particles with 8 desired neighbours: their own pair already
+    # exceeds the target, so h shrinks towards 0 and the iteration runs out
+    wl = ics.sedov(4, seed=2)
+    wl.pos[5] = wl.pos[4]
+    wl.params.des_num_ngb = 8.0
+    wl.params.max_kernel_radius = 0.45
+    st = O.new_state(wl.n, wl.inputs())
+    assert O.Oracle(wl.params, "port").density(st) == abi.ERR_DENSITY_MAXITER
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        with pytest.raises(GizmoHydroError) as e:
+            hp.density()
+        assert e.value.code == abi.ERR_DENSITY_MAXITER
 
 
 def test_empty_bracket_stop_code_and_index():
