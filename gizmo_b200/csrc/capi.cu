@@ -169,6 +169,7 @@ Tree tree_view(gz_context *c)
     Tree t{};
     t.box = c->prm.box_size;
     t.n_nodes = c->t_nodes;
+    t.n_particles = c->n;
     t.node = ptr<int4>(c->t_node);
     t.lo = ptr<double4>(c->t_lo);
     t.hi = ptr<double4>(c->t_hi);
@@ -307,6 +308,8 @@ int sort_targets(gz_context *c, const int *active, int n_active, int *n_out)
     return 0;
 }
 
+// off[0] = 0, off[r + 1] = counts[0] + ... + counts[r]; counts are 64-bit so
+// that the scan accumulates in 64 bits (row totals can pass 2^31).
 int exclusive_scan_counts(gz_context *c, int rows, DevBuf &counts, DevBuf &off, long long *total)
 {
     cudaStream_t s = c->stream;
@@ -314,9 +317,9 @@ int exclusive_scan_counts(gz_context *c, int rows, DevBuf &counts, DevBuf &off, 
     GZ_CUDA(c, cudaMemsetAsync(off.p, 0, sizeof(long long), s));
     if (rows > 0) {
         size_t tmp = 0;
-        cub::DeviceScan::InclusiveSum(nullptr, tmp, ptr<int>(counts), ptr<long long>(off) + 1, rows, s);
+        cub::DeviceScan::InclusiveSum(nullptr, tmp, ptr<long long>(counts), ptr<long long>(off) + 1, rows, s);
         if (ensure(c, c->cub_tmp, tmp)) return c->err;
-        cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, ptr<int>(counts), ptr<long long>(off) + 1, rows, s);
+        cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, ptr<long long>(counts), ptr<long long>(off) + 1, rows, s);
     }
     GZ_CUDA(c, cudaMemcpyAsync(total, ptr<long long>(off) + rows, sizeof(long long), cudaMemcpyDeviceToHost, s));
     GZ_CUDA(c, cudaStreamSynchronize(s));
@@ -330,9 +333,9 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
 {
     cudaStream_t s = c->stream;
     Tree t = tree_view(c);
-    if (ensure(c, counts, sizeof(int) * (size_t)std::max(rows, 1))) return c->err;
+    if (ensure(c, counts, sizeof(long long) * (size_t)std::max(rows, 1))) return c->err;
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<int>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), s);
+              rows, ptr<long long>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
@@ -348,7 +351,7 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
         cap = (long long)(nbr.bytes / sizeof(int));
     }
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<int>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status), s);
+              rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     return 0;
@@ -409,8 +412,8 @@ int build_tree(gz_context *c)
     int beg = 0, cnt = 1, L = 0;
     const unsigned long long *keys = ptr<unsigned long long>(c->keys_sorted);
     while (cnt > 0) {
-        if (ensure(c, c->t_nch, sizeof(int) * (size_t)cnt)) return c->err;
-        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<int>(c->t_nch), s);
+        if (ensure(c, c->t_nch, sizeof(long long) * (size_t)cnt)) return c->err;
+        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<long long>(c->t_nch), s);
         c->launches++;
         long long next = 0;
         if (exclusive_scan_counts(c, cnt, c->t_nch, c->t_cpos, &next)) return c->err;

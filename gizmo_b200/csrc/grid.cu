@@ -83,7 +83,7 @@ GZ_DEV void child_bounds(const unsigned long long *__restrict__ keys, int a, int
 
 // number of non-empty children of every node of one level
 __global__ void k_tree_count(const unsigned long long *__restrict__ keys, int L, const int4 *__restrict__ node,
-                             int beg, int cnt, int *nch)
+                             int beg, int cnt, long long *nch)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
@@ -196,82 +196,162 @@ GZ_DEV double axis_gap(double x, double l, double u, double box, double eps)
 }
 
 constexpr int kStack = 160;  // >= 7 x 22 levels + 8
+constexpr int kWarps = 8;    // warps per block of the walks
+
+// A node waiting on a warp's stack: its run, its children and the lanes whose
+// search sphere reached its box (tested when its parent was opened).
+struct StackNode {
+    int first, count, child, nchild;
+    unsigned lanes;
+};
 
 // Warp-cooperative tree walk. FILL=false counts rows; FILL=true writes them.
-template <bool SYM, bool FILL>
+//   SOLO=false: the warp's 32 lanes hold 32 consecutive targets; a node is
+//     opened if any lane's sphere reaches it and a leaf particle is tested by
+//     every lane that reached the leaf.
+//   SOLO=true: the warp walks one target (for sparse target lists, whose
+//     targets are far apart); the lanes test 32 leaf particles at once and a
+//     ballot compacts the accepted ones, so the row (content and order) is the
+//     one the other mode writes.
+// Opening a node loads its children's records in one coalesced access
+// (children are contiguous) and tests them there, so only reached children
+// are pushed and a pop costs no memory round trip.
+template <bool SYM, bool FILL, bool SOLO>
 __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
                                               const double *__restrict__ z, const double *__restrict__ reach,
                                               const double *__restrict__ hsym, const int *__restrict__ targets,
-                                              int n_targets, int *counts, const long long *__restrict__ off,
+                                              int n_targets, long long *counts, const long long *__restrict__ off,
                                               int *nbr, DevStatus *st)
 {
-    __shared__ int s_stack[8][kStack];
-    __shared__ double4 s_c[8][32];
+    __shared__ StackNode s_stack[kWarps][kStack];
+    __shared__ double4 s_c[kWarps][32];
+    __shared__ double4 s_lo[kWarps][8], s_hi[kWarps][8];
+    __shared__ int4 s_nd[kWarps][8];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int slot = group * 32 + lane;
-    if (group * 32 >= n_targets) return;  // whole warp
+    const unsigned full = 0xffffffffu;
+    int slot;
+    if (SOLO) {
+        slot = group;
+        if (slot >= n_targets) return;  // whole warp
+    } else {
+        slot = group * 32 + lane;
+        if (group * 32 >= n_targets) return;  // whole warp
+    }
     const bool valid = slot < n_targets;
     const int tg = valid ? targets[slot] : -1;
     const double box = t.box, half = 0.5 * box, eps = 4e-16 * box;
     double xi = 0, yi = 0, zi = 0, ri = 0;
     if (valid) { xi = x[tg]; yi = y[tg]; zi = z[tg]; ri = reach[tg]; }
-    const unsigned full = 0xffffffffu;
     const double ri2 = ri * ri;
     long long base = 0;
     if (FILL && valid) base = off[slot];
-    int cnt = 0;
-    if (lane == 0) s_stack[wib][0] = 0;
-    int sp = 1;
+    long long cnt = 0;  // SOLO: the row length so far (uniform); else this lane's
+    // does this lane's sphere reach box [l, u] holding h up to l.w?
+    auto reaches = [&](const double4 &l, const double4 &u) -> bool {
+        const double R = SYM ? fmax(ri, l.w) : ri;
+        const double gx = axis_gap(xi, l.x, u.x, box, eps);
+        const double gy = axis_gap(yi, l.y, u.y, box, eps);
+        const double gz = axis_gap(zi, l.z, u.z, box, eps);
+        return valid && (gx * gx + gy * gy + gz * gz <= R * R * (1.0 + 1e-9));
+    };
+    int sp = 0;
+    {
+        const double4 l = t.lo[0], u = t.hi[0];
+        const unsigned m = __ballot_sync(full, reaches(l, u));
+        if (m) {
+            if (lane == 0) {
+                const int4 nd = t.node[0];
+                s_stack[wib][0] = StackNode{nd.x, nd.y, nd.z, nd.w, m};
+            }
+            sp = 1;
+        }
+    }
     __syncwarp();
     while (sp > 0) {
         sp--;
-        const int ni = s_stack[wib][sp];
+        const StackNode e = s_stack[wib][sp];
         __syncwarp();
-        const int4 nd = t.node[ni];
-        const double4 bl = t.lo[ni], bu = t.hi[ni];
-        const double R = SYM ? fmax(ri, bl.w) : ri;
-        const double gx = axis_gap(xi, bl.x, bu.x, box, eps);
-        const double gy = axis_gap(yi, bl.y, bu.y, box, eps);
-        const double gz = axis_gap(zi, bl.z, bu.z, box, eps);
-        const bool need = valid && (gx * gx + gy * gy + gz * gz <= R * R * (1.0 + 1e-9));
-        if (!__any_sync(full, need)) continue;
-        if (nd.z < 0) {
-            // leaf: stream its particles through shared memory, 32 at a time
-            const int a = nd.x, b = nd.x + nd.y;
+        const bool mine = (e.lanes >> lane) & 1u;
+        if (e.child < 0) {
+            // leaf: its particles, 32 at a time
+            const int a = e.first, b = e.first + e.count;
             for (int c0 = a; c0 < b; c0 += 32) {
                 const int jl = c0 + lane;
-                if (jl < b) s_c[wib][lane] = make_double4(x[jl], y[jl], z[jl], SYM ? hsym[jl] : 0.0);
-                __syncwarp();
-                const int nk = min(32, b - c0);
-                if (need) {
-                    for (int k = 0; k < nk; k++) {
-                        const double4 cj = s_c[wib][k];
+                if (SOLO) {
+                    bool acc = false;
+                    if (jl < b) {
                         double dx, dy, dz;
-                        const double r2 = sep2(xi, yi, zi, cj.x, cj.y, cj.z, box, half, dx, dy, dz);
-                        bool acc;
-                        if (SYM) acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(cj.w, cj.w)));
-                        else acc = r2 < ri2;
-                        if (acc) {
-                            if (FILL) nbr[base + cnt] = c0 + k;
-                            cnt++;
+                        const double r2 = sep2(xi, yi, zi, x[jl], y[jl], z[jl], box, half, dx, dy, dz);
+                        if (SYM) {
+                            const double hj = hsym[jl];
+                            acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(hj, hj)));
+                        } else {
+                            acc = r2 < ri2;
                         }
                     }
+                    const unsigned bal = __ballot_sync(full, acc);
+                    if (FILL && acc) nbr[base + cnt + __popc(bal & ((1u << lane) - 1u))] = jl;
+                    cnt += __popc(bal);
+                } else {
+                    if (jl < b) s_c[wib][lane] = make_double4(x[jl], y[jl], z[jl], SYM ? hsym[jl] : 0.0);
+                    __syncwarp();
+                    const int nk = min(32, b - c0);
+                    if (mine) {
+                        for (int k = 0; k < nk; k++) {
+                            const double4 cj = s_c[wib][k];
+                            double dx, dy, dz;
+                            const double r2 = sep2(xi, yi, zi, cj.x, cj.y, cj.z, box, half, dx, dy, dz);
+                            bool acc;
+                            if (SYM) acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(cj.w, cj.w)));
+                            else acc = r2 < ri2;
+                            if (acc) {
+                                if (FILL) nbr[base + cnt] = c0 + k;
+                                cnt++;
+                            }
+                        }
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
             continue;
         }
-        if (sp + nd.w > kStack) {
+        // open the node: its children's records in one access, tested here
+        const int nc = e.nchild;
+        if (lane < nc) {
+            s_nd[wib][lane] = t.node[e.child + lane];
+            s_lo[wib][lane] = t.lo[e.child + lane];
+            s_hi[wib][lane] = t.hi[e.child + lane];
+        }
+        __syncwarp();
+        unsigned need[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) need[c] = (c < nc) ? __ballot_sync(full, mine && reaches(s_lo[wib][c], s_hi[wib][c])) : 0u;
+        int npush = 0;
+#pragma unroll
+        for (int c = 0; c < 8; c++) npush += need[c] != 0u;
+        if (sp + npush > kStack) {
             if (lane == 0) record_status(st, 5 /* GZ_ERR_CAPACITY */, tg);
             break;
         }
-        // push the children so that the first child is popped first
-        if (lane < nd.w) s_stack[wib][sp + nd.w - 1 - lane] = nd.z + lane;
-        sp += nd.w;
+        // push the reached children so that the first child is popped first
+        if (lane == 0) {
+            int pos = sp + npush - 1;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                if (need[c]) {
+                    const int4 nd = s_nd[wib][c];
+                    s_stack[wib][pos--] = StackNode{nd.x, nd.y, nd.z, nd.w, need[c]};
+                }
+            }
+        }
+        sp += npush;
         __syncwarp();
     }
-    if (!FILL && valid) counts[slot] = cnt;
+    if (!FILL) {
+        if (SOLO) { if (lane == 0) counts[slot] = cnt; }
+        else if (valid) counts[slot] = cnt;
+    }
 }
 
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s)
@@ -279,7 +359,7 @@ void grid_keys(int n, const double *pos, double box, unsigned long long *keys, i
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
 }
 
-void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, int *nch, cudaStream_t s)
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch, cudaStream_t s)
 {
     if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch);
 }
@@ -299,19 +379,24 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
 }
 
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
-               const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
+               const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
                const long long *off, int *nbr, DevStatus *st, cudaStream_t s)
 {
     if (n_targets <= 0) return;
-    const int warps = (n_targets + 31) / 32;
-    const int blocks = (warps + 7) / 8;
+    // a target list much sparser than the particle set has its targets far
+    // apart: one warp per target; otherwise 32 consecutive targets per warp
+    const bool solo = (long long)n_targets * 8 < (long long)t.n_particles;
+    const long long warps = solo ? n_targets : (n_targets + 31) / 32;
+    const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
+#define GZ_WALK(S, F, O) k_walk<S, F, O><<<blocks, 32 * kWarps, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st)
     if (symmetric) {
-        if (nbr) k_walk<true, true><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
-        else k_walk<true, false><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        if (solo) { if (nbr) GZ_WALK(true, true, true); else GZ_WALK(true, false, true); }
+        else { if (nbr) GZ_WALK(true, true, false); else GZ_WALK(true, false, false); }
     } else {
-        if (nbr) k_walk<false, true><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
-        else k_walk<false, false><<<blocks, 256, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st);
+        if (solo) { if (nbr) GZ_WALK(false, true, true); else GZ_WALK(false, false, true); }
+        else { if (nbr) GZ_WALK(false, true, false); else GZ_WALK(false, false, false); }
     }
+#undef GZ_WALK
 }
 
 }  // namespace gz

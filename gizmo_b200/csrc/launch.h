@@ -10,13 +10,13 @@ namespace gz {
 
 // grid.cu
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s);
-void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, int *nch, cudaStream_t s);
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch, cudaStream_t s);
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
                 const long long *cpos, int next, cudaStream_t s);
 void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,
              const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s);
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
-               const double *hsym, int symmetric, const int *targets, int n_targets, int *counts,
+               const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
                const long long *off, int *nbr, DevStatus *st, cudaStream_t s);
 
 // Work description of the density iteration.

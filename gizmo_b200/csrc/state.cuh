@@ -40,6 +40,7 @@ constexpr int kLeafMax = 32;
 struct Tree {
     double box;
     int n_nodes;
+    int n_particles;
     const int4 *node;               // {first, count, child or -1, nchild}
     const double4 *lo;              // tight box minimum xyz; w = maximum h in the node
     const double4 *hi;              // tight box maximum xyz

@@ -132,13 +132,13 @@ int gz_destroy(gz_context *ctx);
 /* Replace the run-time configuration (keeps particle data). */
 int gz_set_params(gz_context *ctx, const gz_params *params);
 
-/* Copy inputs host -> device, build the neighbour grid (Morton sort) and the
- * sorted particle mirror. Replaces the arena acquire of
+/* Copy inputs host -> device, sort the particles by Morton key, build the
+ * octree and the sorted particle mirror. Replaces the arena acquire of
  * neighbor_loop_runner.cc:2297-2302 and the spatial-index build of
  * gpu_neighbor_list.cc:1134-1169. */
 int gz_upload(gz_context *ctx, const gz_particles *in);
 
-/* Rebuild the grid and the sorted mirror from the inputs already resident
+/* Rebuild the octree and the sorted mirror from the inputs already resident
  * on the device (the last gz_upload), resetting kernel lengths and condition
  * numbers to the uploaded values: the start of a pass without host traffic. */
 int gz_restage(gz_context *ctx);

@@ -136,12 +136,18 @@ def test_neighbour_sets_bit_exact(name):
         rng = np.random.default_rng(5)
         sub = rng.choice(wl.n, size=wl.n // 5, replace=False).astype(np.int32)
         g1s = hp.neighbors(1, sub)
+        # a sparse list (under 1/8 of the particles) takes the one-warp-per-target walk
+        few = rng.choice(wl.n, size=wl.n // 20, replace=False).astype(np.int32)
+        g0f = hp.neighbors(0, few)
+        g1f = hp.neighbors(1, few)
     st = O.new_state(wl.n, wl.inputs())
     st["h"][:] = h
     o0 = O.neighbors(wl.params, st, 0)
     o1 = O.neighbors(wl.params, st, 1)
     o1s = O.neighbors(wl.params, st, 1, sub)
-    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g1s, o1s)]:
+    o0f = O.neighbors(wl.params, st, 0, few)
+    o1f = O.neighbors(wl.params, st, 1, few)
+    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g1s, o1s), (g0f, o0f), (g1f, o1f)]:
         assert np.array_equal(go, oo)
         assert np.array_equal(gn, on)
     assert g0[0][-1] > 20 * wl.n  # rows are populated
