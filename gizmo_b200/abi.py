@@ -68,10 +68,12 @@ OUTPUT_FIELDS = [
     ("grad_v", 9), ("accel", 3), ("dudt", 1), ("vsig", 1), ("dtmass", 1), ("dmass", 1),
     ("gravwork", 3),
 ]
+# downloaded only when asked for by name (no reference counterpart)
+DIAGNOSTIC_FIELDS = [("flux_abs", 3)]
 
 
 class GzOutputs(C.Structure):
-    _fields_ = [(name, _dp) for name, _ in OUTPUT_FIELDS] + [("iters", _ip)]
+    _fields_ = [(name, _dp) for name, _ in OUTPUT_FIELDS] + [("iters", _ip), ("flux_abs", _dp)]
 
 
 class GzStatusInfo(C.Structure):

@@ -34,12 +34,13 @@ struct gz_context {
     int n = 0;
     // sorted SoA mirror
     DevBuf x, y, z, vx, vy, vz, m, u, dt, h, cond, num_ngb, drkern, divvel, rho, pressure, fce, nvt, pv, grad, accel,
-        dudt, vsig, dtmass, dmass, gw, iters, active;
+        dudt, vsig, dtmass, dmass, gw, fabs3, iters, active;
     // original-order staging and permutation
     DevBuf stage, stage3, perm, inv, keys, keys_sorted, idx, cub_tmp, targets_orig, targets, targets_tmp;
     // resident copies of the uploaded inputs, original order (gz_restage source)
     DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
     DevBuf dl;                       // download staging, [9][n] doubles (widest output field)
+    DevBuf rec;                      // packed neighbour records of the running pass
     long long launches = 0;          // kernels of this library launched by the context
     // octree over the sorted particles
     DevBuf t_node, t_lo, t_hi, t_parent, t_done, t_nch, t_cpos;
@@ -147,6 +148,7 @@ Particles view(gz_context *c)
     ps.nvt = ptr<double>(c->nvt); ps.pv = ptr<double>(c->pv); ps.grad = ptr<double>(c->grad);
     ps.accel = ptr<double>(c->accel); ps.dudt = ptr<double>(c->dudt); ps.vsig = ptr<double>(c->vsig);
     ps.dtmass = ptr<double>(c->dtmass); ps.dmass = ptr<double>(c->dmass); ps.gw = ptr<double>(c->gw);
+    ps.fabs = ptr<double>(c->fabs3);
     ps.iters = ptr<int>(c->iters);
     ps.active = ptr<unsigned char>(c->active);
     return ps;
@@ -156,12 +158,12 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
 {
     return {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->m, &c->u, &c->dt, &c->h, &c->cond, &c->num_ngb,
             &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->nvt, &c->pv, &c->grad, &c->accel,
-            &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->iters, &c->active, &c->stage, &c->stage3,
+            &c->dudt, &c->vsig, &c->dtmass, &c->dmass, &c->gw, &c->fabs3, &c->iters, &c->active, &c->stage, &c->stage3,
             &c->perm, &c->inv, &c->keys, &c->keys_sorted, &c->idx, &c->cub_tmp, &c->targets_orig,
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -559,6 +561,7 @@ static int stage_inputs(gz_context *c)
         GZ_CUDA(c, cudaMemsetAsync(c->grad.p, 0, sizeof(double) * 15 * (size_t)n, s));
         GZ_CUDA(c, cudaMemsetAsync(c->accel.p, 0, sizeof(double) * 3 * (size_t)n, s));
         GZ_CUDA(c, cudaMemsetAsync(c->gw.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->fabs3.p, 0, sizeof(double) * 3 * (size_t)n, s));
         GZ_CUDA(c, cudaMemsetAsync(c->iters.p, 0, sizeof(int) * (size_t)n, s));
         GZ_CUDA(c, cudaGetLastError());
         if (build_tree(c)) return c->err;
@@ -585,12 +588,15 @@ int gz_upload(gz_context *c, const gz_particles *in)
         if (ensure(c, *b, sizeof(double) * N)) return c->err;
     if (ensure(c, c->nvt, sizeof(double) * 6 * N) || ensure(c, c->pv, sizeof(double) * 3 * N) ||
         ensure(c, c->grad, sizeof(double) * 15 * N) || ensure(c, c->accel, sizeof(double) * 3 * N) ||
-        ensure(c, c->gw, sizeof(double) * 3 * N) || ensure(c, c->iters, sizeof(int) * N) ||
+        ensure(c, c->gw, sizeof(double) * 3 * N) || ensure(c, c->fabs3, sizeof(double) * 3 * N) ||
+        ensure(c, c->iters, sizeof(int) * N) ||
         ensure(c, c->active, N) || ensure(c, c->stage, sizeof(double) * 3 * N) ||
         ensure(c, c->stage3, sizeof(double) * 3 * N) || ensure(c, c->o_vel, sizeof(double) * 3 * N) ||
         ensure(c, c->perm, sizeof(int) * N) || ensure(c, c->inv, sizeof(int) * N) ||
         ensure(c, c->acc, sizeof(double) * 17 * N) || ensure(c, c->scratch, sizeof(DensityScratch) * N) ||
-        ensure(c, c->d_beg, sizeof(long long) * N) || ensure(c, c->d_end, sizeof(long long) * N))
+        ensure(c, c->d_beg, sizeof(long long) * N) || ensure(c, c->d_end, sizeof(long long) * N) ||
+        ensure(c, c->rec, std::max({sizeof(DensRec), gradient_record_bytes(0), gradient_record_bytes(1),
+                                    force_record_bytes(0), force_record_bytes(1)}) * N))
         return c->err;
     if (n > 0) {
         GZ_CUDA(c, cudaMemcpyAsync(c->stage3.p, in->pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
@@ -638,6 +644,8 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         c->launches++;
     }
     GZ_CUDA(c, cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToDevice, s));
+    density_pack(ps, ptr<DensRec>(c->rec), s);
+    c->launches++;
     int n_todo = na;
     int *todo = ptr<int>(c->todo_a), *todo_next = ptr<int>(c->todo_b);
     // Rows at the buffered radius (DensitySpec's CSR buffer factor) are built
@@ -669,6 +677,7 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         w.beg = ptr<long long>(c->d_beg);
         w.end = ptr<long long>(c->d_end);
         w.nbr = ptr<int>(c->d_nbr);
+        w.rec = ptr<DensRec>(c->rec);
         w.acc = ptr<double>(c->acc);
         w.h_built = ptr<double>(c->h_built);
         w.scratch = ptr<DensityScratch>(c->scratch);
@@ -731,8 +740,8 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
-    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->stream);
-    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->stream);
+    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->rec.p, c->stream);
+    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->rec.p, c->stream);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -762,8 +771,8 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     Particles ps = view(c);
     force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
     if (c->prm.precision == GZ_PRECISION_MIXED)
-        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->stream);
-    else force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->stream);
+        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, c->stream);
+    else force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, c->stream);
     if (na > 0) c->launches += 2;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -782,7 +791,8 @@ int gz_download(gz_context *c, const gz_outputs *o)
         {o->h, &c->h, 1}, {o->num_ngb, &c->num_ngb, 1}, {o->drkern, &c->drkern, 1}, {o->divvel, &c->divvel, 1},
         {o->rho, &c->rho, 1}, {o->pressure, &c->pressure, 1}, {o->nvt, &c->nvt, 6}, {o->cond, &c->cond, 1},
         {o->fce, &c->fce, 1}, {o->pvel, &c->pv, 3}, {o->accel, &c->accel, 3}, {o->dudt, &c->dudt, 1},
-        {o->vsig, &c->vsig, 1}, {o->dtmass, &c->dtmass, 1}, {o->dmass, &c->dmass, 1}, {o->gravwork, &c->gw, 3}};
+        {o->vsig, &c->vsig, 1}, {o->dtmass, &c->dtmass, 1}, {o->dmass, &c->dmass, 1}, {o->gravwork, &c->gw, 3},
+        {o->flux_abs, &c->fabs3, 3}};
     for (auto &e : f) {
         if (!e.dst) continue;
         const long long cnt = (long long)n * e.k;
@@ -905,6 +915,8 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     w.beg = ptr<long long>(c->d_beg);
     w.end = ptr<long long>(c->d_end);
     w.nbr = ptr<int>(c->d_nbr);
+    w.rec = ptr<DensRec>(c->rec);
+    density_pack(ps, ptr<DensRec>(c->rec), s);
     w.acc = ptr<double>(c->acc);
     if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
     else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);

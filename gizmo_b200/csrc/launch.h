@@ -26,6 +26,7 @@ struct DensityWork {
     const long long *beg;   // sorted index -> its density row [beg, end) in nbr
     const long long *end;
     const int *nbr;
+    const DensRec *rec;     // packed neighbour records (sorted index)
     double *acc;            // [17][n] per-particle accumulator (sorted index)
     double *h_built;        // search radius each row was built with
     DensityScratch *scratch;
@@ -40,19 +41,24 @@ struct PassLaunch {
     int tpt_density, tpt_gradient, tpt_force;
 };
 
+void density_pack(const Particles &ps, DensRec *rec, cudaStream_t s);
 void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
 void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
 void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s);
 void density_finalize(const PassParams &p, const Particles &ps, const double *acc, const int *targets, int n_targets,
                       cudaStream_t s);
+// `rec` is scratch for the packed neighbour records: at least n x
+// record_bytes(pass) bytes, 16-byte aligned.
+size_t gradient_record_bytes(int mixed);
+size_t force_record_bytes(int mixed);
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                    cudaStream_t s);
+                    void *rec, cudaStream_t s);
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     cudaStream_t s);
+                     void *rec, cudaStream_t s);
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, cudaStream_t s);
+                DevStatus *st, void *rec, cudaStream_t s);
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, cudaStream_t s);
+                 DevStatus *st, void *rec, cudaStream_t s);
 void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
 
 }  // namespace gz

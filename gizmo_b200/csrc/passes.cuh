@@ -37,11 +37,11 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
     for (int k = 0; k < 17; k++) a[k] = 0;
     const long long b0 = w.beg[t], b1 = w.end[t];
     for (long long e = b0 + lane; e < b1; e += TPT) {
-        const int j = w.nbr[e];
-        const double mjd = ps.m[j];
+        const DensRec rj = w.rec[w.nbr[e]];
+        const double mjd = rj.m;
         if (mjd <= 0) continue;
         double dx, dy, dz;
-        const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
+        const double r2 = sep2(xi, yi, zi, rj.x, rj.y, rj.z, p.box, p.half, dx, dy, dz);
         if (r2 >= h2) continue;
         const T r = Real<T>::sqrt_(T(r2));
         const T u = r * hinv;
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
         const T mj_wk = mj * wk;
         a[0] += (double)wk;
         a[1] += (double)mj_wk;
-        const T vjx = T(ps.vx[j]), vjy = T(ps.vy[j]), vjz = T(ps.vz[j]);
+        const T vjx = T(rj.vx), vjy = T(rj.vy), vjz = T(rj.vz);
         if (mfv && r == T(0)) {
             a[14] += (double)(mj_wk * vjx);
             a[15] += (double)(mj_wk * vjy);
@@ -102,12 +102,30 @@ void launch_density_sums(const PassParams &p, const Particles &ps, const Density
 }
 
 // -------------------------------------------------------------- gradients
+// What a gradient row reads of each neighbour: FP64 position, h, mass and
+// density (membership and the j filters), pressure and velocity as pair
+// operands (64 bytes in FP32, 80 in FP64).
+template <typename T> struct __align__(16) GradRec {
+    double x, y, z, h, m, rho;
+    T P, vx, vy, vz;
+};
+
+template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *rec)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ps.n) return;
+    GradRec<T> r;
+    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
+    r.P = T(ps.pressure[i]); r.vx = T(ps.vx[i]); r.vy = T(ps.vy[i]); r.vz = T(ps.vz[i]);
+    rec[i] = r;
+}
+
 // gradient_accumulate_neighbor (gradient_functions.h:304-665) + the
 // finalize: construct_gradient (gradients_loop.cc:129-136) and
 // local_slopelimiter (gradients_loop.cc:1077-1130).
 template <typename T, int TPT>
 __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
-                                                   int n_targets, Csr rows)
+                                                   int n_targets, Csr rows, const GradRec<T> *__restrict__ rec)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -133,12 +151,12 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
     if (enabled) {
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         for (long long e = b0 + lane; e < b1; e += TPT) {
-            const int j = rows.nbr[e];
-            const double mj = ps.m[j], rhoj = ps.rho[j], hjd = ps.h[j];
+            const GradRec<T> rj = rec[rows.nbr[e]];
+            const double mj = rj.m, rhoj = rj.rho, hjd = rj.h;
             if (mj <= 0) continue;
             if (rhoj <= 0 || hjd <= 0) continue;
             double dx, dy, dz;
-            const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
+            const double r2 = sep2(xi, yi, zi, rj.x, rj.y, rj.z, p.box, p.half, dx, dy, dz);
             if (r2 <= 0) continue;
             if ((r2 >= hi2) && (r2 >= hjd * hjd)) continue;
             const T r = Real<T>::sqrt_(T(r2));
@@ -148,10 +166,10 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
             if ((double)r > maxdist) maxdist = (double)r;
             T d[5];
             d[0] = T(rhoj) - rho_i;
-            d[1] = T(ps.pressure[j]) - P_i;
-            d[2] = T(ps.vx[j]) - vi[0];
-            d[3] = T(ps.vy[j]) - vi[1];
-            d[4] = T(ps.vz[j]) - vi[2];
+            d[1] = rj.P - P_i;
+            d[2] = rj.vx - vi[0];
+            d[3] = rj.vy - vi[1];
+            d[4] = rj.vz - vi[2];
 #pragma unroll
             for (int q = 0; q < 5; q++) {
                 const double dq = (double)d[q];
@@ -209,16 +227,18 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
 
 template <typename T>
 void launch_gradients(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                      cudaStream_t s)
+                      void *recbuf, cudaStream_t s)
 {
     if (n_targets <= 0) return;
+    GradRec<T> *rec = (GradRec<T> *)recbuf;
+    k_pack_gradient<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 255) / 256);
     switch (tpt) {
-        case 4: k_gradients<T, 4><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
-        case 8: k_gradients<T, 8><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
-        case 32: k_gradients<T, 32><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
-        default: k_gradients<T, 16><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows); break;
+        case 4: k_gradients<T, 4><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 8: k_gradients<T, 8><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 32: k_gradients<T, 32><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        default: k_gradients<T, 16><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
     }
 }
 
@@ -246,6 +266,27 @@ template <typename T> GZ_DEV void load_side(const Particles &ps, int i, double g
     S.dt = ps.dt[i];
 }
 
+// What a force row reads of each neighbour: FP64 position, h, mass and
+// density (membership, the j filters, the MFV mass bookkeeping), the
+// particle's side of the face in the pair type, and whether it is active
+// (208 bytes in FP32, 352 in FP64).
+template <typename T> struct __align__(16) ForceRec {
+    double x, y, z, h, m, rho;
+    Side<T> s;
+    int active;
+};
+
+template <typename T> __global__ void k_pack_force(Particles ps, double gamma, ForceRec<T> *rec)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ps.n) return;
+    ForceRec<T> r;
+    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
+    load_side(ps, i, gamma, r.s);
+    r.active = ps.active[i];
+    rec[i] = r;
+}
+
 // Row i of the symmetric list: every pair is evaluated in one canonical
 // orientation (lower sorted index as the R side) so the flux seen from i and
 // from j are exact negatives -- mass and momentum are conserved to roundoff
@@ -255,7 +296,8 @@ template <typename T> GZ_DEV void load_side(const Particles &ps, int i, double g
 // hydro_toplevel.cc:133-253.
 template <typename T, int TPT>
 __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const int *__restrict__ targets,
-                                               int n_targets, Csr rows, DevStatus *st)
+                                               int n_targets, Csr rows, DevStatus *st,
+                                               const ForceRec<T> *__restrict__ rec)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -275,22 +317,23 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     const double mi = ps.m[i], rhoi = ps.rho[i];
     const bool enabled = (mi > 0 && rhoi > 0);
     const double xi = ps.x[i], yi = ps.y[i], zi = ps.z[i], hid = ps.h[i], dti = ps.dt[i];
-    Side<T> SI;
-    load_side(ps, i, p.gamma, SI);
+    const ForceRec<T> *rip = rec + i;
     double acc[3] = {0, 0, 0}, dtE = 0, dtm = 0, dm = 0, gw[3] = {0, 0, 0}, vs = 0;
+    double fa[3] = {0, 0, 0};  // scale of the sums: |F_rho|, |F_v|, |F_E| summed over the row
     int stop = 0;
     if (enabled) {
-        vs = (double)SI.cs;
+        vs = (double)rip->s.cs;
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         for (long long e = b0 + lane; e < b1; e += TPT) {
             const int j = rows.nbr[e];
-            const double mj = ps.m[j], rhoj = ps.rho[j];
+            const ForceRec<T> *rjp = rec + j;
+            const double mj = rjp->m, rhoj = rjp->rho;
             if (!(mj > 0 && rhoj > 0)) continue;
             double dx, dy, dz;
-            const double r2 = sep2(xi, yi, zi, ps.x[j], ps.y[j], ps.z[j], p.box, p.half, dx, dy, dz);
-            const double hjd = ps.h[j];
-            Side<T> SJ;
-            load_side(ps, j, p.gamma, SJ);
+            const double r2 = sep2(xi, yi, zi, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
+            const double hjd = rjp->h;
+            const double dtj = rjp->s.dt;
+            const int j_active = rjp->active;
             PairFlux<T> F;
             // one call site for both orientations: the lower sorted index is the
             // R side, so rows i and j run the identical instruction sequence on
@@ -298,26 +341,32 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
             const bool fwd = i < j;
             const double sign = fwd ? 1.0 : -1.0;
             const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
-            force_pair(p.kernel, mfv, p.selfgravity_off, gc, fwd ? SI : SJ, fwd ? SJ : SI, dp, r2, fwd ? hid : hjd,
-                       fwd ? hjd : hid, F, stop);
+            // both sides are read from the records in place (global memory, L1-resident)
+            const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
+            force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd, fwd ? hjd : hid, F,
+                       stop);
             if (!F.valid) continue;
             const double frho = sign * (double)F.rho;
             acc[0] += sign * (double)F.v[0];
             acc[1] += sign * (double)F.v[1];
             acc[2] += sign * (double)F.v[2];
             dtE += sign * (double)F.p;
+            fa[0] += fabs(frho);
+            fa[1] += sqrt((double)F.v[0] * (double)F.v[0] + (double)F.v[1] * (double)F.v[1] +
+                          (double)F.v[2] * (double)F.v[2]);
+            fa[2] += fabs((double)F.p);
             if ((double)F.vsig_ts > vs) vs = (double)F.vsig_ts;
             if (mfv) {
                 double self_dm, accepted, other_dm;
-                mfv_mass_side(frho, dti, SJ.dt, mi, mj, self_dm, accepted, other_dm);
+                mfv_mass_side(frho, dti, dtj, mi, mj, self_dm, accepted, other_dm);
                 dtm += frho;
                 dm += self_dm;
                 gw[0] += dx * accepted;
                 gw[1] += dy * accepted;
                 gw[2] += dz * accepted;
-                if (ps.active[j]) {
+                if (j_active) {
                     double sj, aj, oj;  // j's own evaluation writes onto i
-                    mfv_mass_side(-frho, SJ.dt, dti, mj, mi, sj, aj, oj);
+                    mfv_mass_side(-frho, dtj, dti, mj, mi, sj, aj, oj);
                     dm += oj;
                 } else if (other_dm != 0) {
                     atomicAdd(ps.dmass + j, other_dm);
@@ -327,7 +376,11 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     }
     if (stop) record_status(st, stop, i);
 #pragma unroll
-    for (int k = 0; k < 3; k++) { acc[k] = warp_sum(acc[k], mask, TPT); gw[k] = warp_sum(gw[k], mask, TPT); }
+    for (int k = 0; k < 3; k++) {
+        acc[k] = warp_sum(acc[k], mask, TPT);
+        gw[k] = warp_sum(gw[k], mask, TPT);
+        fa[k] = warp_sum(fa[k], mask, TPT);
+    }
     dtE = warp_sum(dtE, mask, TPT);
     dtm = warp_sum(dtm, mask, TPT);
     dm = warp_sum(dm, mask, TPT);
@@ -358,7 +411,7 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
         if (mfv) for (int k = 0; k < 3; k++) g3[k] *= inv;
         if (hid >= 0.99 * p.max_kernel_radius) du = 0;
     }
-    for (int k = 0; k < 3; k++) { ps.accel[k * n + i] = a3[k]; ps.gw[k * n + i] = g3[k]; }
+    for (int k = 0; k < 3; k++) { ps.accel[k * n + i] = a3[k]; ps.gw[k * n + i] = g3[k]; ps.fabs[k * n + i] = fa[k]; }
     ps.dudt[i] = du;
     ps.vsig[i] = vsig;
     ps.dtmass[i] = dtm;
@@ -367,16 +420,18 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
 
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, cudaStream_t s)
+                  DevStatus *st, void *recbuf, cudaStream_t s)
 {
     if (n_targets <= 0) return;
+    ForceRec<T> *rec = (ForceRec<T> *)recbuf;
+    k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec);
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);
     switch (tpt) {
-        case 4: k_force<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
-        case 8: k_force<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
-        case 32: k_force<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
-        default: k_force<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st); break;
+        case 4: k_force<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
+        case 8: k_force<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
+        case 32: k_force<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
+        default: k_force<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
     }
 }
 

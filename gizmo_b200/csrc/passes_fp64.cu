@@ -5,21 +5,39 @@
 
 namespace gz {
 
+size_t gradient_record_bytes(int mixed) { return mixed ? sizeof(GradRec<float>) : sizeof(GradRec<double>); }
+size_t force_record_bytes(int mixed) { return mixed ? sizeof(ForceRec<float>) : sizeof(ForceRec<double>); }
+
+__global__ void k_pack_density(Particles ps, DensRec *rec)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ps.n) return;
+    DensRec r;
+    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.m = ps.m[i];
+    r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i]; r.pad = 0.0;
+    rec[i] = r;
+}
+
+void density_pack(const Particles &ps, DensRec *rec, cudaStream_t s)
+{
+    if (ps.n > 0) k_pack_density<<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
+}
+
 void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s)
 {
     launch_density_sums<double>(p, ps, w, tpt, s);
 }
 
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                    cudaStream_t s)
+                    void *rec, cudaStream_t s)
 {
-    launch_gradients<double>(p, ps, targets, n_targets, rows, tpt, s);
+    launch_gradients<double>(p, ps, targets, n_targets, rows, tpt, rec, s);
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, cudaStream_t s)
+                DevStatus *st, void *rec, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, s);
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, s);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's

@@ -17,15 +17,15 @@ void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityW
 }
 
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     cudaStream_t s)
+                     void *rec, cudaStream_t s)
 {
-    launch_gradients<float>(p, ps, targets, n_targets, rows, tpt, s);
+    launch_gradients<float>(p, ps, targets, n_targets, rows, tpt, rec, s);
 }
 
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, cudaStream_t s)
+                 DevStatus *st, void *rec, cudaStream_t s)
 {
-    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, s);
+    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, s);
 }
 
 }  // namespace gz

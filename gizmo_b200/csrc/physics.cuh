@@ -655,8 +655,8 @@ template <typename T> GZ_HD void face_to_flux(ROut<T> &o, const T *n, const GCon
 // faces only, so it stays out of line: its iteration does not raise the
 // register budget of the common HLLC path.
 template <typename T>
-__host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
-                          int &stop)
+__host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR,
+                                                    const GConst<T> &gc, int &stop)
 {
     if ((rv.L.p == T(0) && rv.R.p == T(0)) || (rv.L.rho == T(0) && rv.R.rho == T(0))) {
         o.P_M = o.S_M = T(0);
@@ -830,8 +830,10 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         for (int k = 0; k < 3; k++) d_i[k] = dp[k] * rinv;
         for (int k = 0; k < 3; k++) { d_j[k] = d_i[k] * s_j; d_i[k] *= s_i; }
         T vframe[3];
-        const T *wj = mfv ? J.pv : J.v, *wi = mfv ? I.pv : I.v;
-        for (int k = 0; k < 3; k++) vframe[k] = (wj[k] * (-s_i) + wi[k] * s_j) * rinv;
+        for (int k = 0; k < 3; k++) {
+            const T wj = mfv ? J.pv[k] : J.v[k], wi = mfv ? I.pv[k] : I.v[k];  // values, not a pointer select
+            vframe[k] = (wj * (-s_i) + wi * s_j) * rinv;
+        }
         face_vel_i += dot3(I.v, n);
         face_vel_j += dot3(J.v, n);
         const T face_area_dot_vel = ((-s_i) * face_vel_j + s_j * face_vel_i) * rinv;

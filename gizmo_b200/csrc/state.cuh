@@ -27,6 +27,7 @@ struct Particles {
     double *accel;                  // [3][n]
     double *dudt, *vsig, *dtmass, *dmass;
     double *gw;                     // [3][n] GravWorkTerm
+    double *fabs;                   // [3][n] sums of |mass|, |momentum|, |energy| pair fluxes (diagnostic)
     int *iters;
     const unsigned char *active;    // 1 for particles of the current active set
 };
@@ -44,6 +45,13 @@ struct Tree {
     const int4 *node;               // {first, count, child or -1, nchild}
     const double4 *lo;              // tight box minimum xyz; w = maximum h in the node
     const double4 *hi;              // tight box maximum xyz
+};
+
+// What a density row reads of each neighbour, in one 64-byte record (sorted
+// order), packed once per pass: the pair loop then issues two 32-byte reads
+// per neighbour instead of seven scattered ones.
+struct __align__(16) DensRec {
+    double x, y, z, m, vx, vy, vz, pad;
 };
 
 // Compressed neighbour rows: row r of `slot_of` targets.

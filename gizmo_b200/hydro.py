@@ -129,7 +129,7 @@ class HydroPass:
         want = names if fields is None else list(fields)
         out = {}
         o = abi.GzOutputs()
-        for name, k in abi.OUTPUT_FIELDS:
+        for name, k in abi.OUTPUT_FIELDS + abi.DIAGNOSTIC_FIELDS:
             if name in want:
                 a = np.zeros((n,) if k == 1 else (n, k))
                 out[name] = a

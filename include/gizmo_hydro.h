@@ -110,6 +110,10 @@ typedef struct gz_outputs {
     double *dmass;     /* [n]    CellP.dMass (MFV) */
     double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
     int    *iters;     /* [n]    density iterations taken */
+    double *flux_abs;  /* [n][3] diagnostic, no reference counterpart: the sums over the
+                          force row of |mass flux|, |momentum flux| and |energy flux| of
+                          the pairs, the scale against which the cancelling sums dtmass,
+                          mass * accel and mass * dudt are accurate */
 } gz_outputs;
 
 typedef struct gz_status_info {

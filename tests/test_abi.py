@@ -37,7 +37,8 @@ def test_struct_layouts_match_c(tmp_path):
 #include "gizmo_hydro.h"
 int main(void) {
   printf("%zu %zu %zu %zu\n", sizeof(gz_params), sizeof(gz_particles), sizeof(gz_outputs), sizeof(gz_status_info));
-  printf("%zu %zu %zu\n", offsetof(gz_params, box_size), offsetof(gz_particles, cond), offsetof(gz_outputs, iters));
+  printf("%zu %zu %zu %zu\n", offsetof(gz_params, box_size), offsetof(gz_particles, cond), offsetof(gz_outputs, iters),
+         offsetof(gz_outputs, flux_abs));
   printf("%zu %zu\n", offsetof(gz_status_info, pairs_density), offsetof(gz_status_info, message));
   return 0; }
 ''')
@@ -47,6 +48,7 @@ int main(void) {
     got = [int(v) for v in out]
     want = [C.sizeof(abi.GzParams), C.sizeof(abi.GzParticles), C.sizeof(abi.GzOutputs), C.sizeof(abi.GzStatusInfo),
             abi.GzParams.box_size.offset, abi.GzParticles.cond.offset, abi.GzOutputs.iters.offset,
+            abi.GzOutputs.flux_abs.offset,
             abi.GzStatusInfo.pairs_density.offset, abi.GzStatusInfo.message.offset]
     assert got == want
 
