@@ -41,6 +41,7 @@ struct gz_context {
     DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
     DevBuf dl;                       // download staging, [9][n] doubles (widest output field)
     DevBuf rec;                      // packed neighbour records of the running pass
+    DevBuf work;                     // work counter of the persistent walks
     long long launches = 0;          // kernels of this library launched by the context
     // octree over the sorted particles
     DevBuf t_node, t_lo, t_hi, t_parent, t_done, t_nch, t_cpos;
@@ -163,7 +164,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -335,9 +336,10 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
 {
     cudaStream_t s = c->stream;
     Tree t = tree_view(c);
-    if (ensure(c, counts, sizeof(long long) * (size_t)std::max(rows, 1))) return c->err;
+    if (ensure(c, counts, sizeof(long long) * (size_t)std::max(rows, 1)) || ensure(c, c->work, sizeof(int)))
+        return c->err;
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<long long>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), s);
+              rows, ptr<long long>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
@@ -353,7 +355,8 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
         cap = (long long)(nbr.bytes / sizeof(int));
     }
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status), s);
+              rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status),
+              ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     return 0;

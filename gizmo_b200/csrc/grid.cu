@@ -217,27 +217,17 @@ struct StackNode {
 // (children are contiguous) and tests them there, so only reached children
 // are pushed and a pop costs no memory round trip.
 template <bool SYM, bool FILL, bool SOLO>
-__global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
-                                              const double *__restrict__ z, const double *__restrict__ reach,
-                                              const double *__restrict__ hsym, const int *__restrict__ targets,
-                                              int n_targets, long long *counts, const long long *__restrict__ off,
-                                              int *nbr, DevStatus *st)
+__device__ __forceinline__ void walk_group(const int group, const Tree &t, const double *__restrict__ x,
+                                           const double *__restrict__ y, const double *__restrict__ z,
+                                           const double *__restrict__ reach, const double *__restrict__ hsym,
+                                           const int *__restrict__ targets, int n_targets, long long *counts,
+                                           const long long *__restrict__ off, int *nbr, DevStatus *st,
+                                           StackNode (*s_stack)[kStack], double4 (*s_c)[32], double4 (*s_lo)[8],
+                                           double4 (*s_hi)[8], int4 (*s_nd)[8])
 {
-    __shared__ StackNode s_stack[kWarps][kStack];
-    __shared__ double4 s_c[kWarps][32];
-    __shared__ double4 s_lo[kWarps][8], s_hi[kWarps][8];
-    __shared__ int4 s_nd[kWarps][8];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned full = 0xffffffffu;
-    int slot;
-    if (SOLO) {
-        slot = group;
-        if (slot >= n_targets) return;  // whole warp
-    } else {
-        slot = group * 32 + lane;
-        if (group * 32 >= n_targets) return;  // whole warp
-    }
+    const int slot = SOLO ? group : group * 32 + lane;
     const bool valid = slot < n_targets;
     const int tg = valid ? targets[slot] : -1;
     const double box = t.box, half = 0.5 * box, eps = 4e-16 * box;
@@ -298,6 +288,7 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
                     __syncwarp();
                     const int nk = min(32, b - c0);
                     if (mine) {
+#pragma unroll 4
                         for (int k = 0; k < nk; k++) {
                             const double4 cj = s_c[wib][k];
                             double dx, dy, dz;
@@ -354,6 +345,33 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
     }
 }
 
+// Persistent form: every warp takes the next group (32 consecutive targets,
+// or one target in SOLO mode) from a counter until none is left, so warps
+// that draw a group on both sides of a Morton jump do not hold up a wave.
+template <bool SYM, bool FILL, bool SOLO>
+__global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
+                                              const double *__restrict__ z, const double *__restrict__ reach,
+                                              const double *__restrict__ hsym, const int *__restrict__ targets,
+                                              int n_targets, long long *counts, const long long *__restrict__ off,
+                                              int *nbr, DevStatus *st, int *next_group)
+{
+    __shared__ StackNode s_stack[kWarps][kStack];
+    __shared__ double4 s_c[kWarps][32];
+    __shared__ double4 s_lo[kWarps][8], s_hi[kWarps][8];
+    __shared__ int4 s_nd[kWarps][8];
+    const int lane = threadIdx.x & 31;
+    const int n_groups = SOLO ? n_targets : (n_targets + 31) / 32;
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(next_group, 1);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= n_groups) break;
+        walk_group<SYM, FILL, SOLO>(g, t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st, s_stack,
+                                    s_c, s_lo, s_hi, s_nd);
+        __syncwarp();
+    }
+}
+
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s)
 {
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
@@ -378,17 +396,36 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
     k_tree_up<<<(n_nodes + 127) / 128, 128, 0, s>>>(n_nodes, node, parent, x, y, z, h, lo, hi, done, boxes);
 }
 
+template <bool SYM, bool FILL, bool SOLO>
+static void launch_walk(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                        const double *hsym, const int *targets, int n_targets, long long *counts, const long long *off,
+                        int *nbr, DevStatus *st, int *next_group, cudaStream_t s)
+{
+    static int resident = 0;  // blocks of this instance resident per SM x SMs (device 0-independent enough)
+    if (resident == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<SYM, FILL, SOLO>, 32 * kWarps, 0);
+        resident = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+    }
+    const long long groups = SOLO ? n_targets : (n_targets + 31) / 32;
+    const long long need = (groups + kWarps - 1) / kWarps;
+    const unsigned blocks = (unsigned)(need < resident ? need : resident);
+    cudaMemsetAsync(next_group, 0, sizeof(int), s);
+    k_walk<SYM, FILL, SOLO><<<blocks, 32 * kWarps, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off,
+                                                            nbr, st, next_group);
+}
+
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
-               const long long *off, int *nbr, DevStatus *st, cudaStream_t s)
+               const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     // a target list much sparser than the particle set has its targets far
     // apart: one warp per target; otherwise 32 consecutive targets per warp
     const bool solo = (long long)n_targets * 8 < (long long)t.n_particles;
-    const long long warps = solo ? n_targets : (n_targets + 31) / 32;
-    const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
-#define GZ_WALK(S, F, O) k_walk<S, F, O><<<blocks, 32 * kWarps, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st)
+#define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st, next_group, s)
     if (symmetric) {
         if (solo) { if (nbr) GZ_WALK(true, true, true); else GZ_WALK(true, false, true); }
         else { if (nbr) GZ_WALK(true, true, false); else GZ_WALK(true, false, false); }

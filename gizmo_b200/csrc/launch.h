@@ -17,7 +17,7 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
              const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s);
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
-               const long long *off, int *nbr, DevStatus *st, cudaStream_t s);
+               const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s);
 
 // Work description of the density iteration.
 struct DensityWork {

@@ -35,14 +35,13 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
     double a[17];
 #pragma unroll
     for (int k = 0; k < 17; k++) a[k] = 0;
-    const long long b0 = w.beg[t], b1 = w.end[t];
-    for (long long e = b0 + lane; e < b1; e += TPT) {
-        const DensRec rj = w.rec[w.nbr[e]];
+    // one neighbour's contribution; the lane visits its entries in row order
+    auto pair = [&](const DensRec &rj) {
         const double mjd = rj.m;
-        if (mjd <= 0) continue;
+        if (mjd <= 0) return;
         double dx, dy, dz;
         const double r2 = sep2(xi, yi, zi, rj.x, rj.y, rj.z, p.box, p.half, dx, dy, dz);
-        if (r2 >= h2) continue;
+        if (r2 >= h2) return;
         const T r = Real<T>::sqrt_(T(r2));
         const T u = r * hinv;
         T wk, dwk;
@@ -77,6 +76,18 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
             }
             a[3] -= (double)(dwk * (px * dvx + py * dvy + pz * dvz) / r);
         }
+    };
+    // two entries per step: both records are in flight before either is used
+    const long long b0 = w.beg[t], b1 = w.end[t];
+    for (long long e = b0 + lane; e < b1; e += 2 * TPT) {
+        const long long e1 = e + TPT;
+        const bool two = e1 < b1;
+        const int j0 = w.nbr[e];
+        const int j1 = two ? w.nbr[e1] : j0;
+        const DensRec r0 = w.rec[j0];
+        const DensRec r1 = w.rec[j1];
+        pair(r0);
+        if (two) pair(r1);
     }
 #pragma unroll
     for (int k = 0; k < 17; k++) a[k] = warp_sum(a[k], mask, TPT);
@@ -124,7 +135,7 @@ template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *
 // finalize: construct_gradient (gradients_loop.cc:129-136) and
 // local_slopelimiter (gradients_loop.cc:1077-1130).
 template <typename T, int TPT>
-__global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
+__global__ void __launch_bounds__(128) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
                                                    int n_targets, Csr rows, const GradRec<T> *__restrict__ rec)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,11 +154,13 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
     const T rho_i = T(rhoi), P_i = T(Pi);
     const T vi[3] = {T(ps.vx[i]), T(ps.vy[i]), T(ps.vz[i])};
     double gr[15];  // [k][q]: q = rho, P, v0, v1, v2
-    double mx[5], mn[5], maxdist = 0;
+    // the extrema and MaxDistance only ever hold values of type T (differences
+    // and distances computed in T), so they are kept in T
+    T mx[5], mn[5], maxdist = T(0);
 #pragma unroll
     for (int k = 0; k < 15; k++) gr[k] = 0;
 #pragma unroll
-    for (int k = 0; k < 5; k++) { mx[k] = 0; mn[k] = 0; }
+    for (int k = 0; k < 5; k++) { mx[k] = T(0); mn[k] = T(0); }
     if (enabled) {
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         for (long long e = b0 + lane; e < b1; e += TPT) {
@@ -163,7 +176,7 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
             T wk_i = T(0), dwk_i = T(0);
             const bool in_i = Real<T>::inside(r, r2, hi, hid);
             if (in_i) k_main(p.kernel, Real<T>::below_one(r * hinv), hinv3, hinv4, wk_i, dwk_i);
-            if ((double)r > maxdist) maxdist = (double)r;
+            if (r > maxdist) maxdist = r;
             T d[5];
             d[0] = T(rhoj) - rho_i;
             d[1] = rj.P - P_i;
@@ -172,8 +185,7 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
             d[4] = rj.vz - vi[2];
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                const double dq = (double)d[q];
-                if (dq < mn[q]) mn[q] = dq; else if (dq > mx[q]) mx[q] = dq;
+                if (d[q] < mn[q]) mn[q] = d[q]; else if (d[q] > mx[q]) mx[q] = d[q];
             }
             if (in_i) {
                 const T dp[3] = {T(dx), T(dy), T(dz)};
@@ -191,9 +203,10 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
     }
 #pragma unroll
     for (int k = 0; k < 15; k++) gr[k] = warp_sum(gr[k], mask, TPT);
+    double mxd[5], mnd[5];
 #pragma unroll
-    for (int q = 0; q < 5; q++) { mx[q] = warp_max(mx[q], mask, TPT); mn[q] = warp_min(mn[q], mask, TPT); }
-    maxdist = warp_max(maxdist, mask, TPT);
+    for (int q = 0; q < 5; q++) { mxd[q] = warp_max((double)mx[q], mask, TPT); mnd[q] = warp_min((double)mn[q], mask, TPT); }
+    const double maxdistd = warp_max((double)maxdist, mask, TPT);
     if (lane != 0) return;
     double g_rho[3] = {0, 0, 0}, g_p[3] = {0, 0, 0}, g_v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (enabled) {
@@ -208,15 +221,15 @@ __global__ void __launch_bounds__(256) k_gradients(PassParams p, Particles ps, c
             sym_matvec(nv, s_v, g_v[c]);
         }
         double stol = 0.0, h_lim = hid;
-        const double d_max = dmax(hid, maxdist);
+        const double d_max = dmax(hid, maxdistd);
         h_lim = d_max;
         double a_limiter = 0.25;
         const double CN = ps.cond[i];
         if (CN > 100) a_limiter = dmin(0.5, 0.25 + 0.25 * (CN - 100) / 100);
         if (p.selfgravity_off) { h_lim = hid; stol = 0.1; }
-        slopelimiter(g_rho, mx[0], mn[0], a_limiter, h_lim, 0, 1, d_max, rhoi);
-        slopelimiter(g_p, mx[1], mn[1], a_limiter, h_lim, stol, 1, d_max, Pi);
-        for (int c = 0; c < 3; c++) slopelimiter(g_v[c], mx[2 + c], mn[2 + c], a_limiter, h_lim, stol, 0, 0, 0);
+        slopelimiter(g_rho, mxd[0], mnd[0], a_limiter, h_lim, 0, 1, d_max, rhoi);
+        slopelimiter(g_p, mxd[1], mnd[1], a_limiter, h_lim, stol, 1, d_max, Pi);
+        for (int c = 0; c < 3; c++) slopelimiter(g_v[c], mxd[2 + c], mnd[2 + c], a_limiter, h_lim, stol, 0, 0, 0);
     }
     for (int k = 0; k < 3; k++) {
         ps.grad[(0 + k) * n + i] = g_rho[k];
@@ -233,12 +246,12 @@ void launch_gradients(const PassParams &p, const Particles &ps, const int *targe
     GradRec<T> *rec = (GradRec<T> *)recbuf;
     k_pack_gradient<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
     const long long threads = (long long)n_targets * tpt;
-    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    const unsigned blocks = (unsigned)((threads + 127) / 128);  // 128-thread blocks: finer register granularity
     switch (tpt) {
-        case 4: k_gradients<T, 4><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
-        case 8: k_gradients<T, 8><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
-        case 32: k_gradients<T, 32><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
-        default: k_gradients<T, 16><<<blocks, 256, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 4: k_gradients<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 8: k_gradients<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 32: k_gradients<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        default: k_gradients<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
     }
 }
 
