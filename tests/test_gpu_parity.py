@@ -270,3 +270,21 @@ def test_position_outside_box_is_reported():
             hp.density()
         assert e.value.code == abi.ERR_ARG
         assert hp.status()["index"] == 11
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_flux_scale_bounds_the_rates(precision):
+    """flux_abs (diagnostic) holds the row sums of |pair flux|: by the triangle
+    inequality it bounds the net rates it is the error scale of."""
+    wl = CASES["plummer16"](precision)
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.full_pass()
+        out = hp.download(["accel", "dudt", "dtmass", "flux_abs"])
+    fa = out["flux_abs"]
+    assert (fa >= 0).all() and (fa[:, 1] > 0).mean() > 0.99
+    slack = 1 + 1e-6
+    assert (np.abs(out["dtmass"]) <= fa[:, 0] * slack + 1e-300).all()
+    vmag = np.linalg.norm(wl.vel, axis=1)
+    net_mom = np.linalg.norm(wl.mass[:, None] * out["accel"] + wl.vel * out["dtmass"][:, None], axis=1)
+    assert (net_mom <= fa[:, 1] * slack + 1e-300).all()
