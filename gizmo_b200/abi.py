@@ -93,8 +93,9 @@ class GzStatusInfo(C.Structure):
 EXPORTED_SYMBOLS = [
     "gz_create", "gz_destroy", "gz_set_params", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream",
-    "gz_neighbors", "gz_density_sums",
+    "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc",
 ]
+NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libgizmo_hydro.so")
@@ -127,6 +128,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_stream.restype = vp
     lib.gz_neighbors.argtypes = [vp, _ip, C.c_int, C.c_int, C.POINTER(C.c_int64), _ip]
     lib.gz_density_sums.argtypes = [vp, _ip, C.c_int, _dp, _dp]
+    lib.gz_density_sums_noalloc.argtypes = [C.POINTER(GzParams), C.c_int, vp, vp, vp, vp, vp, vp, vp]
     for name in EXPORTED_SYMBOLS:
         if name != "gz_stream":
             getattr(lib, name).restype = C.c_int

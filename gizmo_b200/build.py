@@ -28,6 +28,7 @@ UNITS = {
     "capi.cu": [],
     "passes_fp64.cu": ["-fmad=false"],
     "passes_mixed.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "noalloc.cu": ["-fmad=false"],
 }
 
 

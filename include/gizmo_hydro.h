@@ -181,6 +181,33 @@ int gz_neighbors(gz_context *ctx, const int *active, int n_active, int mode,
  * DensitySpec::pair_kernel sums (density_loop.h:1140-1385). */
 int gz_density_sums(gz_context *ctx, const int *active, int n_active, double *acc, double *pv);
 
+/* No counterpart in the reference. Density sums as gz_density_sums computes
+ * them (same layout of acc[a][14] and pv[a][3], same pair arithmetic in
+ * FP64), for callers that cannot allocate device memory: a host code whose own
+ * memory pool already owns the device, or a loop that cannot afford the
+ * device-wide synchronisation that cudaMalloc/cudaFree implies. It needs no
+ * gz_context and allocates nothing:
+ *   - pos [n][3], vel [n][3], mass [n], h [n] (inputs, particles in [0, box)) and
+ *     acc [n][14], pv [n][3] (outputs; pv may be NULL) are DEVICE pointers that
+ *     the caller owns; rows follow the caller's order, every particle is a
+ *     target and a candidate;
+ *   - the only scratch is a static device array of GZ_NOALLOC_MAX_PARTICLES
+ *     packed records (4 MiB), held by every GPU that loads the library until
+ *     the process exits; n above that limit returns GZ_ERR_CAPACITY;
+ *   - work is queued on `stream` (a cudaStream_t, NULL for the default
+ *     stream) and the call returns without waiting: synchronise the stream
+ *     before reading acc;
+ *   - the first call on each device looks up that array's device address
+ *     (a one-time set-up on the current device): make that first call before
+ *     any stream capture;
+ *   - every call on a device uses the same array and rewrites it; two calls
+ *     whose work overlaps on the GPU (different streams, no ordering between
+ *     them) race on it and their results are undefined.
+ * The neighbour loop is all-pairs over the set, which is what bounds n. */
+#define GZ_NOALLOC_MAX_PARTICLES 65536
+int gz_density_sums_noalloc(const gz_params *params, int n, const double *pos, const double *vel,
+                            const double *mass, const double *h, double *acc, double *pv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
