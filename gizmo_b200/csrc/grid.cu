@@ -283,6 +283,34 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                     const unsigned bal = __ballot_sync(full, acc);
                     if (FILL && acc) nbr[base + cnt + __popc(bal & ((1u << lane) - 1u))] = jl;
                     cnt += __popc(bal);
+                } else if (__popc(e.lanes) * 7 < min(32, b - c0) * 5) {
+                    // few of the warp's targets reached this leaf: the lanes hold
+                    // the candidates and the warp loops over the reaching targets
+                    // (each target's row gets its hits in candidate order, as below)
+                    double cx = 0, cy = 0, cz = 0, ch2 = 0;
+                    if (jl < b) {
+                        cx = x[jl]; cy = y[jl]; cz = z[jl];
+                        if (SYM) { const double hj = hsym[jl]; ch2 = __dmul_rn(hj, hj); }
+                    }
+                    unsigned rem = e.lanes;
+                    while (rem) {
+                        const int tl = __ffs(rem) - 1;
+                        rem &= rem - 1u;
+                        const double tx = __shfl_sync(full, xi, tl), ty = __shfl_sync(full, yi, tl);
+                        const double tz = __shfl_sync(full, zi, tl), tr2 = __shfl_sync(full, ri2, tl);
+                        bool acc = false;
+                        if (jl < b) {
+                            double dx, dy, dz;
+                            const double r2 = sep2(tx, ty, tz, cx, cy, cz, box, half, dx, dy, dz);
+                            acc = SYM ? ((r2 > 0) && !((r2 >= tr2) && (r2 >= ch2))) : (r2 < tr2);
+                        }
+                        const unsigned bal = __ballot_sync(full, acc);
+                        if (FILL) {
+                            const long long at = __shfl_sync(full, base + cnt, tl);
+                            if (acc) nbr[at + __popc(bal & ((1u << lane) - 1u))] = jl;
+                        }
+                        if (lane == tl) cnt += __popc(bal);
+                    }
                 } else {
                     if (jl < b) s_c[wib][lane] = make_double4(x[jl], y[jl], z[jl], SYM ? hsym[jl] : 0.0);
                     __syncwarp();

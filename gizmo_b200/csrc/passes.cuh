@@ -277,6 +277,10 @@ template <typename T> GZ_DEV void load_side(const Particles &ps, int i, double g
     S.fce = T(ps.fce[i]);
     S.drk = T(ps.drkern[i]);
     S.dt = ps.dt[i];
+    S.Vd = ps.m[i] / rho;
+    S.condd = ps.cond[i];
+    S.fced = ps.fce[i];
+    S.prd = P / rho;
 }
 
 // What a force row reads of each neighbour: FP64 position, h, mass and

@@ -741,6 +741,12 @@ template <typename T> struct Side {
     T v[3], pv[3], nvt[6], grho[3], gp[3], gv[9];
     T m, rho, P, h, cs, cond, fce, drk;
     double dt;
+    // FP64 per-particle values for the pair's discontinuous decisions (volume
+    // contrast, condition-number fallback, reconstruction mode, entropic
+    // switch): V = m / rho, ConditionNumber, FaceClosureError, P / rho. In the
+    // FP64 form they equal what the pair would compute; in the mixed form they
+    // make those decisions exactly the FP64 form's.
+    double Vd, condd, fced, prd;
 };
 
 // Result of one canonical pair evaluation, i = the "local" (R) side.
@@ -780,7 +786,9 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
     if (Real<T>::inside(r, r2d, I.h, hi_d)) k_main(kf, Real<T>::below_one(r * hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
     k_hinv(J.h, hinv_j, hinv3_j, hinv4_j);
     if (Real<T>::inside(r, r2d, J.h, hj_d)) k_main(kf, Real<T>::below_one(r * hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
-    const T cnumcrit2 = T(kCnDanger) * T(kCnDanger) - I.cond * I.cond;
+    // explicitly rounded FP64 (no contraction in either build)
+    const double cnumcrit2 = cr::sub(cr::mul(kCnDanger, kCnDanger), cr::mul(I.condd, I.condd));
+    const double cnum2 = cr::mul(J.condd, J.condd);
     T eps_big = T(0.5), eps_small = T(1.e-3);
     if (!mfv && !selfgravity_off) { eps_small = T(1.e-2); eps_big = T(0.6); }
     const T vdotr2 = dot3(dp, dv);
@@ -795,12 +803,12 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
     RVec<T> rv = {};
     ROut<T> ro = {};
     do {
-        const T leak_vs_tol = T(0.5) * (I.fce + J.fce);
+        const double leak_vs_tol = cr::mul(0.5, cr::add(I.fced, J.fced));
         const T Pressure_i = I.P, Pressure_j = J.P;
         V_j = J.m / J.rho;
         {
             T wt_i = V_i, wt_j = V_j;
-            if ((fabs(V_i - V_j) / dmin(V_i, V_j)) / T(3) > T(1.25))
+            if (cr::div_(cr::div_(fabs(cr::sub(I.Vd, J.Vd)), dmin(I.Vd, J.Vd)), 3.0) > 1.25)
                 wt_i = wt_j = V_i * V_j * (wk_i + wk_j) / (V_i * wk_i + V_j * wk_j);
             T ai[3], aj[3];
             sym_matvec(I.nvt, dp, ai);
@@ -809,7 +817,7 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
             for (int k = 0; k < 3; k++) FA[k] = (ai[k] * si + aj[k] * sj) * (T(1.0) * T(1.0));
             FAN = nsq3(FA);
             const T fn_dot_dp = dot3(FA, dp);
-            if ((J.cond * J.cond > T(1.0e12) + cnumcrit2) || (fn_dot_dp < T(0))) {
+            if ((cnum2 > cr::add(1.0e12, cnumcrit2)) || (fn_dot_dp < T(0))) {
                 T fk = -(wt_i * V_i * dwk_i + wt_j * V_j * dwk_j) / r;
                 fk *= T(1.0) * T(1.0);
                 for (int k = 0; k < 3; k++) FA[k] = dp[k] * fk;
@@ -844,7 +852,7 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         const T vdotf2_phys = face_vel_i - face_vel_j;
         if (vdotf2_phys < T(0)) v2_approach = dmax(v2_approach, vdotf2_phys * vdotf2_phys);
         int recon_mode = 1;
-        if (leak_vs_tol > T(1)) recon_mode = 0;
+        if (leak_vs_tol > 1.0) recon_mode = 0;
         reconstruct(I.rho, I.grho, J.rho, J.grho, d_i, d_j, rv.L.rho, rv.R.rho, recon_mode);
         reconstruct(Pressure_i, I.gp, Pressure_j, J.gp, d_i, d_j, rv.L.p, rv.R.p, recon_mode);
         for (int k = 0; k < 3; k++)
@@ -855,19 +863,28 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         T ptl = T(1.1) * T(1.0) * dmax(press_i_tot, press_j_tot);
         if (mfv) ptl *= T(2.0);
         if (recon_mode == 0) ptl = dmax(ptl, dmax(dmax(Pressure_i, Pressure_j), T(2.) * dmax(I.rho, J.rho) * v2_approach));
-        riemann_solver(rv, ro, n, ptl, gc, stop);
-        if ((ro.P_M < T(0)) || Real<T>::isnan_(ro.P_M) || (ro.P_M > T(1.4) * ptl)) {
-            rv.R.p = Pressure_i; rv.L.p = Pressure_j;
-            rv.R.rho = I.rho; rv.L.rho = J.rho;
-            for (int k = 0; k < 3; k++) { rv.R.v[k] = I.v[k] - vframe[k]; rv.L.v[k] = J.v[k] - vframe[k]; }
-            riemann_solver(rv, ro, n, T(1.4) * ptl, gc, stop);
-            if ((ro.P_M < T(0)) || Real<T>::isnan_(ro.P_M)) {
+        // Up to three attempts (hydro_core_meshless_functions.h:350-427): the
+        // reconstructed faces; then the cell-centred states at 1.4 x the
+        // pressure limit; then the same at zero velocity at 2 x. The same calls
+        // in the same order as the reference, through one call site: a single
+        // inlined copy of the solver keeps the kernel's code (and its
+        // instruction-cache misses) smaller.
+        for (int attempt = 0; attempt < 3; attempt++) {
+            T lim = ptl;
+            if (attempt > 0) {
                 rv.R.p = Pressure_i; rv.L.p = Pressure_j;
                 rv.R.rho = I.rho; rv.L.rho = J.rho;
-                for (int k = 0; k < 3; k++) { rv.R.v[k] = T(0); rv.L.v[k] = T(0); }
-                riemann_solver(rv, ro, n, T(2.0) * ptl, gc, stop);
-                if ((ro.P_M < T(0)) || Real<T>::isnan_(ro.P_M)) stop = 1234;
+                for (int k = 0; k < 3; k++) {
+                    rv.R.v[k] = attempt == 1 ? I.v[k] - vframe[k] : T(0);
+                    rv.L.v[k] = attempt == 1 ? J.v[k] - vframe[k] : T(0);
+                }
+                lim = attempt == 1 ? T(1.4) * ptl : T(2.0) * ptl;
             }
+            riemann_solver(rv, ro, n, lim, gc, stop);
+            bool retry = (ro.P_M < T(0)) || Real<T>::isnan_(ro.P_M);
+            if (attempt == 0) retry = retry || (ro.P_M > T(1.4) * ptl);
+            if (!retry) break;
+            if (attempt == 2) stop = 1234;
         }
         if (!((ro.P_M > T(0)) && (!Real<T>::isnan_(ro.P_M)))) { Fl = Crv<T>{}; break; }
         ro.F.p += dot3(vframe, ro.F.v);  // de-boost, hydro_core_meshless_functions.h:459-468
@@ -880,7 +897,7 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         for (int k = 0; k < 3; k++) Fl.v[k] = ro.F.v[k] * FAN;
         if (!mfv) {  // MFM face entropic switch, hydro_core_meshless_functions.h:515-574
             const T SM_over_ceff = fabs(ro.S_M) / dmin(I.cs, J.cs);
-            if ((SM_over_ceff < eps_big) || (leak_vs_tol > T(1))) {
+            if ((SM_over_ceff < eps_big) || (leak_vs_tol > 1.0)) {
                 int use = 1;
                 const T facenorm_pm = ro.P_M * FAN;
                 const T PdV_fac = ro.P_M * vdotr2_phys / T(1.0);
@@ -888,15 +905,14 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
                 const T PdV_j = dwk_j * V_j * V_j * J.drk * PdV_fac;
                 const T du_old = facenorm_pm * (ro.S_M + face_area_dot_vel);
                 const T du_new = T(0.5) * (PdV_i - PdV_j + facenorm_pm * (face_vel_i + face_vel_j));
-                const T cnum2 = J.cond * J.cond;
-                const T ratio = T(1.001);
-                const T to_i = Pressure_i / I.rho, to_j = Pressure_j / J.rho;
+                const double ratio = 1.001;
+                const double to_i = I.prd, to_j = J.prd;
                 if (use && SM_over_ceff > eps_small && cnum2 < cnumcrit2) {
-                    if (to_i > ratio * to_j) {
+                    if (to_i > cr::mul(ratio, to_j)) {
                         const T dtoj = -du_old + facenorm_pm * face_vel_j;
                         if (dtoj > T(0)) use = 0;
                         else { if (dtoj < T(0)) { if (dtoj > -du_new + facenorm_pm * face_vel_j) use = 0; } }
-                    } else if (ratio * to_i < to_j) {
+                    } else if (cr::mul(ratio, to_i) < to_j) {
                         const T dtoi = +du_old - facenorm_pm * face_vel_i;
                         if (dtoi > T(0)) use = 0;
                         else { if (dtoi < T(0)) { if (dtoi > +du_new - facenorm_pm * face_vel_i) use = 0; } }
