@@ -57,6 +57,8 @@ struct gz_context {
     // density work: rows are [d_beg[t], d_end[t]) in d_nbr; d_used entries are taken
     DevBuf acc, h_built, scratch, keep, regrow, todo_a, todo_b, grow, d_beg, d_end, flag, counts, d_off, d_nbr, n_sel;
     long long d_nbr_cap = 0, d_used = 0;
+    bool dens_all = false;           // the density rows cover every particle (last pass had no active list)
+    DevBuf s_acnt, s_bcnt, s_tmp;    // symmetric rows derived from the density rows
     // symmetric rows (shared by gradients and force)
     DevBuf s_off, s_nbr, s_counts;
     long long s_nbr_cap = 0;
@@ -171,7 +173,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->work, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -475,14 +477,55 @@ int refresh_hmax(gz_context *c)
     return 0;
 }
 
-int build_sym_rows(gz_context *c, int rows)
+// Symmetric rows of all particles from the density rows of a pass over all
+// particles: A_i (the converged one-way row) plus B_i (the pairs reached only
+// from j's side), sorted -- the walk's rows, without a second walk.
+int sym_rows_from_density(gz_context *c)
 {
-    if (refresh_hmax(c)) return c->err;
-    long long total = 0;
-    if (build_rows(c, ptr<double>(c->h), 1, ptr<int>(c->targets), rows, c->s_counts, c->s_off, c->s_nbr, c->s_nbr_cap,
-                   &total))
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)std::max(n, 1);
+    if (ensure(c, c->s_acnt, sizeof(int) * N) || ensure(c, c->s_bcnt, sizeof(int) * N) ||
+        ensure(c, c->s_counts, sizeof(long long) * N))
         return c->err;
+    GZ_CUDA(c, cudaMemsetAsync(c->s_bcnt.p, 0, sizeof(int) * N, s));
+    sym_split(n, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), ptr<double>(c->h), c->prm.box_size,
+              ptr<long long>(c->d_beg), ptr<long long>(c->d_end), ptr<int>(c->d_nbr), ptr<int>(c->s_acnt),
+              ptr<int>(c->s_bcnt), s);
+    sym_counts(n, ptr<int>(c->s_acnt), ptr<int>(c->s_bcnt), ptr<long long>(c->s_counts), s);
+    c->launches += 2;
+    GZ_CUDA(c, cudaGetLastError());
+    c->dens_all = false;  // the density rows are compacted in place: consumed
+    long long total = 0;
+    if (exclusive_scan_counts(c, n, c->s_counts, c->s_off, &total)) return c->err;
+    if (total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
+    if (ensure(c, c->s_tmp, sizeof(int) * (size_t)std::max(total, 1ll))) return c->err;
+    if (total > c->s_nbr_cap || !c->s_nbr.p) {
+        if (ensure(c, c->s_nbr, sizeof(int) * (size_t)std::max(total, 1ll))) return c->err;
+        c->s_nbr_cap = (long long)(c->s_nbr.bytes / sizeof(int));
+    }
+    GZ_CUDA(c, cudaMemsetAsync(c->s_bcnt.p, 0, sizeof(int) * N, s));  // reused as the B cursors
+    sym_scatter(n, ptr<long long>(c->d_beg), ptr<int>(c->d_nbr), ptr<int>(c->s_acnt), ptr<long long>(c->s_off),
+                ptr<int>(c->s_bcnt), ptr<int>(c->s_tmp), s);
+    sym_sort(n, ptr<long long>(c->s_off), ptr<int>(c->s_tmp), ptr<int>(c->s_nbr), s);
+    c->launches += 2;
+    GZ_CUDA(c, cudaGetLastError());
     c->pairs_symmetric = total;
+    return 0;
+}
+
+int build_sym_rows(gz_context *c, int rows, bool all)
+{
+    if (all && c->dens_all && rows == c->n && c->n > 0) {
+        if (sym_rows_from_density(c)) return c->err;
+    } else {
+        if (refresh_hmax(c)) return c->err;
+        long long total = 0;
+        if (build_rows(c, ptr<double>(c->h), 1, ptr<int>(c->targets), rows, c->s_counts, c->s_off, c->s_nbr,
+                       c->s_nbr_cap, &total))
+            return c->err;
+        c->pairs_symmetric = total;
+    }
     c->sym_rows = rows;
     c->sym_valid = true;
     return 0;
@@ -579,6 +622,7 @@ static int stage_inputs(gz_context *c)
     c->grid_valid = true;
     c->have_density = c->have_gradients = false;
     c->sym_valid = false;
+    c->dens_all = false;
     return 0;
 }
 
@@ -637,6 +681,7 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
     if (!c) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "density before upload");
+    c->dens_all = false;  // set again only when this pass completes over every particle
     cudaStream_t s = c->stream;
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
@@ -736,6 +781,7 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
     if (n_todo > 0) return fail(c, GZ_ERR_DENSITY_MAXITER, "density did not converge in MAXITER iterations");
     c->have_density = true;
     c->sym_valid = false;
+    c->dens_all = (active == nullptr);
     return GZ_OK;
 }
 
@@ -746,7 +792,7 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     if (!c->have_density) return fail(c, GZ_ERR_ORDER, "gradients before density");
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
-    if (build_sym_rows(c, na)) return c->err;
+    if (build_sym_rows(c, na, active == nullptr)) return c->err;
     c->sym_all = (active == nullptr);
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
@@ -774,7 +820,7 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
                        (active != nullptr && !c->sym_all && c->sym_active.size() == (size_t)n_active &&
                         std::equal(c->sym_active.begin(), c->sym_active.end(), active)));
     if (!same) {
-        if (build_sym_rows(c, na)) return c->err;
+        if (build_sym_rows(c, na, active == nullptr)) return c->err;
         c->sym_all = (active == nullptr);
         c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     }
@@ -906,6 +952,7 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     if (!c || !acc) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "density sums before upload");
+    c->dens_all = false;  // the density rows are about to be replaced
     cudaStream_t s = c->stream;
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;

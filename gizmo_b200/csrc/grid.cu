@@ -400,6 +400,121 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
     }
 }
 
+// ------------------------------------------------ symmetric rows from density rows
+// When the density pass covered every particle, each particle's density row
+// holds every j with r < (row radius) >= its converged h, so the symmetric
+// rows follow without another tree walk:
+//   S_i = A_i u B_i,  A_i = {j : 0 < r2 < h_i^2},  B_i = {j : i in A_j, r2 >= h_i^2}
+// (r2 is bitwise symmetric: the minimum image of -d is the negation of that of
+// d), which is exactly the walk's predicate 0 < r2 and !(r2 >= h_i^2 and
+// r2 >= h_j^2). The rows are sorted at the end, so they equal the walk's.
+
+// Compacts density row i in place to A_i (order kept), marks an entry whose
+// pair is one-sided (r2 >= h_j^2: i belongs in B_j) by storing ~j, and counts
+// |A_i| and |B_j|.
+template <int TPT>
+__global__ void __launch_bounds__(256) k_sym_split(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                                   const double *__restrict__ z, const double *__restrict__ h,
+                                                   double box, const long long *__restrict__ beg,
+                                                   const long long *__restrict__ end, int *nbr, int *acnt, int *bcnt)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gtid / TPT, lane = gtid % TPT;
+    if (i >= n) return;
+    const int gshift = (threadIdx.x & 31) & ~(TPT - 1);
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << gshift);
+    const double half = 0.5 * box;
+    const double xi = x[i], yi = y[i], zi = z[i], hi = h[i];
+    const double hi2 = __dmul_rn(hi, hi);
+    const long long b0 = beg[i], b1 = end[i];
+    long long wpos = b0;
+    for (long long e0 = b0; e0 < b1; e0 += TPT) {
+        const long long e = e0 + lane;
+        int j = 0;
+        bool in_a = false, one_sided = false;
+        if (e < b1) {
+            j = nbr[e];
+            double dx, dy, dz;
+            const double r2 = sep2(xi, yi, zi, x[j], y[j], z[j], box, half, dx, dy, dz);
+            in_a = (r2 > 0) && (r2 < hi2);
+            if (in_a) {
+                const double hj = h[j];
+                one_sided = !(r2 < __dmul_rn(hj, hj));
+                if (one_sided) atomicAdd(bcnt + j, 1);
+            }
+        }
+        const unsigned gb = (__ballot_sync(mask, in_a) >> gshift) & (TPT == 32 ? 0xffffffffu : ((1u << TPT) - 1u));
+        __syncwarp(mask);  // every lane has read its entry before any is overwritten
+        if (in_a) nbr[wpos + __popc(gb & ((1u << lane) - 1u))] = one_sided ? ~j : j;
+        wpos += __popc(gb);
+    }
+    if (lane == 0) acnt[i] = (int)(wpos - b0);
+}
+
+__global__ void k_sym_counts(int n, const int *__restrict__ acnt, const int *__restrict__ bcnt, long long *cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cnt[i] = (long long)acnt[i] + bcnt[i];
+}
+
+// A_i into row i; each marked entry also puts i into row j's B part
+template <int TPT>
+__global__ void __launch_bounds__(256) k_sym_scatter(int n, const long long *__restrict__ beg,
+                                                     const int *__restrict__ nbr, const int *__restrict__ acnt,
+                                                     const long long *__restrict__ s_off, int *bcur, int *rows)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gtid / TPT, lane = gtid % TPT;
+    if (i >= n) return;
+    const long long b0 = beg[i], o = s_off[i];
+    const int a = acnt[i];
+    for (int k = lane; k < a; k += TPT) {
+        const int v = nbr[b0 + k];
+        const int j = v < 0 ? ~v : v;
+        rows[o + k] = j;
+        if (v < 0) rows[s_off[j] + acnt[j] + atomicAdd(bcur + j, 1)] = i;
+    }
+}
+
+// Each row sorted ascending by rank (its entries are distinct), one warp per row.
+__global__ void __launch_bounds__(256) k_sym_sort(int n, const long long *__restrict__ s_off,
+                                                  const int *__restrict__ rows, int *out)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const long long b0 = s_off[i], b1 = s_off[i + 1];
+    const int len = (int)(b1 - b0);
+    for (int k = lane; k < len; k += 32) {
+        const int v = rows[b0 + k];
+        int rank = 0;
+        for (int m = 0; m < len; m++) rank += rows[b0 + m] < v;
+        out[b0 + rank] = v;
+    }
+}
+
+void sym_split(int n, const double *x, const double *y, const double *z, const double *h, double box,
+               const long long *beg, const long long *end, int *nbr, int *acnt, int *bcnt, cudaStream_t s)
+{
+    if (n > 0) k_sym_split<16><<<(unsigned)(((long long)n * 16 + 255) / 256), 256, 0, s>>>(n, x, y, z, h, box, beg, end, nbr, acnt, bcnt);
+}
+
+void sym_counts(int n, const int *acnt, const int *bcnt, long long *cnt, cudaStream_t s)
+{
+    if (n > 0) k_sym_counts<<<(n + 255) / 256, 256, 0, s>>>(n, acnt, bcnt, cnt);
+}
+
+void sym_scatter(int n, const long long *beg, const int *nbr, const int *acnt, const long long *s_off, int *bcur,
+                 int *rows, cudaStream_t s)
+{
+    if (n > 0) k_sym_scatter<16><<<(unsigned)(((long long)n * 16 + 255) / 256), 256, 0, s>>>(n, beg, nbr, acnt, s_off, bcur, rows);
+}
+
+void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStream_t s)
+{
+    if (n > 0) k_sym_sort<<<(unsigned)(((long long)n * 32 + 255) / 256), 256, 0, s>>>(n, s_off, rows, out);
+}
+
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s)
 {
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
@@ -450,9 +565,11 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
                const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s)
 {
     if (n_targets <= 0) return;
-    // a target list much sparser than the particle set has its targets far
-    // apart: one warp per target; otherwise 32 consecutive targets per warp
-    const bool solo = (long long)n_targets * 8 < (long long)t.n_particles;
+    // Group mode (32 targets per warp) for every list: with the transposed
+    // leaf test it serves sparse lists as well, and its traversal tests 32
+    // targets per ballot where the one-target mode tests one. The one-target
+    // mode stays available for lists of a single target.
+    const bool solo = n_targets == 1;
 #define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st, next_group, s)
     if (symmetric) {
         if (solo) { if (nbr) GZ_WALK(true, true, true); else GZ_WALK(true, false, true); }

@@ -19,6 +19,14 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
                const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s);
 
+// symmetric rows derived from the density rows of a pass over all particles
+void sym_split(int n, const double *x, const double *y, const double *z, const double *h, double box,
+               const long long *beg, const long long *end, int *nbr, int *acnt, int *bcnt, cudaStream_t s);
+void sym_counts(int n, const int *acnt, const int *bcnt, long long *cnt, cudaStream_t s);
+void sym_scatter(int n, const long long *beg, const int *nbr, const int *acnt, const long long *s_off, int *bcur,
+                 int *rows, cudaStream_t s);
+void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStream_t s);
+
 // Work description of the density iteration.
 struct DensityWork {
     const int *todo;        // sorted indices still iterating

@@ -113,12 +113,14 @@ void launch_density_sums(const PassParams &p, const Particles &ps, const Density
 }
 
 // -------------------------------------------------------------- gradients
-// What a gradient row reads of each neighbour: FP64 position, h, mass and
-// density (membership and the j filters), pressure and velocity as pair
-// operands (64 bytes in FP32, 80 in FP64).
+// What a gradient row reads of each neighbour: position, h, mass, density,
+// pressure and velocity, all FP64 (80 bytes). The pair takes the differences
+// q_j - q_i in FP64 and only then rounds them to the pair type: in a smooth
+// field q_j and q_i agree to many digits, and rounding them to FP32 first
+// would keep only the few that differ.
 template <typename T> struct __align__(16) GradRec {
     double x, y, z, h, m, rho;
-    T P, vx, vy, vz;
+    double P, vx, vy, vz;
 };
 
 template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *rec)
@@ -127,7 +129,7 @@ template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *
     if (i >= ps.n) return;
     GradRec<T> r;
     r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
-    r.P = T(ps.pressure[i]); r.vx = T(ps.vx[i]); r.vy = T(ps.vy[i]); r.vz = T(ps.vz[i]);
+    r.P = ps.pressure[i]; r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i];
     rec[i] = r;
 }
 
@@ -151,8 +153,7 @@ __global__ void __launch_bounds__(128) k_gradients(PassParams p, Particles ps, c
     const T hi = T(hid);
     T hinv, hinv3, hinv4;
     k_hinv(hi, hinv, hinv3, hinv4);
-    const T rho_i = T(rhoi), P_i = T(Pi);
-    const T vi[3] = {T(ps.vx[i]), T(ps.vy[i]), T(ps.vz[i])};
+    const double vi[3] = {ps.vx[i], ps.vy[i], ps.vz[i]};
     double gr[15];  // [k][q]: q = rho, P, v0, v1, v2
     // the extrema and MaxDistance only ever hold values of type T (differences
     // and distances computed in T), so they are kept in T
@@ -174,15 +175,15 @@ __global__ void __launch_bounds__(128) k_gradients(PassParams p, Particles ps, c
             if ((r2 >= hi2) && (r2 >= hjd * hjd)) continue;
             const T r = Real<T>::sqrt_(T(r2));
             T wk_i = T(0), dwk_i = T(0);
-            const bool in_i = Real<T>::inside(r, r2, hi, hid);
+            const bool in_i = Real<T>::inside(Real<T>::support_r(r, r2), r2, hi, hid);
             if (in_i) k_main(p.kernel, Real<T>::below_one(r * hinv), hinv3, hinv4, wk_i, dwk_i);
             if (r > maxdist) maxdist = r;
             T d[5];
-            d[0] = T(rhoj) - rho_i;
-            d[1] = rj.P - P_i;
-            d[2] = rj.vx - vi[0];
-            d[3] = rj.vy - vi[1];
-            d[4] = rj.vz - vi[2];
+            d[0] = T(rhoj - rhoi);  // differences in FP64, then rounded once
+            d[1] = T(rj.P - Pi);
+            d[2] = T(rj.vx - vi[0]);
+            d[3] = T(rj.vy - vi[1]);
+            d[4] = T(rj.vz - vi[2]);
 #pragma unroll
             for (int q = 0; q < 5; q++) {
                 if (d[q] < mn[q]) mn[q] = d[q]; else if (d[q] > mx[q]) mx[q] = d[q];

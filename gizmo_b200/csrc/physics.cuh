@@ -25,6 +25,7 @@ template <> struct Real<double> {
     static GZ_HD double hllc_tol(double s) { return 1.e-12 * (s + 1e-56); }
     // kernel support as the reference decides it: on r = sqrt(r2) < h
     static GZ_HD bool inside(double r, double /*r2d*/, double h, double /*hd*/) { return r < h; }
+    static GZ_HD double support_r(double r, double /*r2d*/) { return r; }
     static GZ_HD double below_one(double u) { return u; }
 };
 template <> struct Real<float> {
@@ -36,10 +37,12 @@ template <> struct Real<float> {
     // same tolerance, floored at the smallest normal so the all-zero vacuum
     // state (S_L = S_M = S_R = 0) is still trapped instead of dividing 0 by 0
     static GZ_HD float hllc_tol(float s) { return fmaxf(1.e-12f * s, 1e-37f); }
-    // kernel support decided on the exact FP64 r2 < h^2 (the same pairs as the
-    // FP64 form); FP32 rounding of r may reach h there, so u is kept below 1
-    // and a pair inside the support never has both kernel weights zero
-    static GZ_HD bool inside(float, double r2d, float, double hd) { return r2d < hd * hd; }
+    // kernel support decided exactly as the FP64 form decides it, on the FP64
+    // r = sqrt(r2) < h (support_r gives that r once per pair); FP32 rounding of
+    // r may reach h there, so u is kept below 1 and a pair inside the support
+    // never has both kernel weights zero
+    static GZ_HD bool inside(double rd, double /*r2d*/, float, double hd) { return rd < hd; }
+    static GZ_HD double support_r(float, double r2d) { return sqrt(r2d); }
     static GZ_HD float below_one(float u) { return u < 1.0f ? u : 0.99999994f; }
 };
 
@@ -782,10 +785,11 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
     T vsig = I.cs + J.cs;
     T hinv_i, hinv3_i, hinv4_i, hinv_j, hinv3_j, hinv4_j;
     T wk_i = T(0), dwk_i = T(0), wk_j = T(0), dwk_j = T(0);
+    const double r_sup = Real<T>::support_r(r, r2d);
     k_hinv(I.h, hinv_i, hinv3_i, hinv4_i);
-    if (Real<T>::inside(r, r2d, I.h, hi_d)) k_main(kf, Real<T>::below_one(r * hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
+    if (Real<T>::inside(r_sup, r2d, I.h, hi_d)) k_main(kf, Real<T>::below_one(r * hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
     k_hinv(J.h, hinv_j, hinv3_j, hinv4_j);
-    if (Real<T>::inside(r, r2d, J.h, hj_d)) k_main(kf, Real<T>::below_one(r * hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
+    if (Real<T>::inside(r_sup, r2d, J.h, hj_d)) k_main(kf, Real<T>::below_one(r * hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
     // explicitly rounded FP64 (no contraction in either build)
     const double cnumcrit2 = cr::sub(cr::mul(kCnDanger, kCnDanger), cr::mul(I.condd, I.condd));
     const double cnum2 = cr::mul(J.condd, J.condd);
