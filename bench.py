@@ -289,11 +289,19 @@ def run_ours(args, world, rank, local):
         else:
             den = rowb
         rel = d / np.maximum(den, 1e-300)
-        acc[f] = {"max": float(rel.max()), "p99": float(np.percentile(rel, 99)),
+        acc[f] = {"max": float(rel.max()), "p99_99": float(np.percentile(rel, 99.99)), "p99": float(np.percentile(rel, 99)),
                   "p50": float(np.median(rel)), "norm": float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300)),
+                  "above_1e-5": int((rel > 1e-5).sum()), "above_1e-3": int((rel > 1e-3).sum()),
                   "denominator": "flux scale" if f in scale else ("|x| floored at 1e-3 max" if f.startswith("grad") else "|x|")}
     acc["iters_equal_frac"] = float(np.mean(om["iters"] == o64["iters"]))
     acc["max_over_fields"] = max(v["max"] for k, v in acc.items() if isinstance(v, dict))
+    acc["particles"] = N
+    acc["particles_above_1e-5_any_field"] = int(np.count_nonzero(np.any(np.stack(
+        [np.linalg.norm((om[f] - o64[f]).reshape(N, -1), axis=1) / np.maximum(
+            scale[f] if f in scale else (np.maximum(np.linalg.norm(o64[f].reshape(N, -1), axis=1),
+                                                    1e-3 * np.linalg.norm(o64[f].reshape(N, -1), axis=1).max())
+                                         if f.startswith("grad") else np.linalg.norm(o64[f].reshape(N, -1), axis=1)),
+            1e-300) > 1e-5 for f in fields]), axis=0)))
     # conservation per pass (both forms)
     cons = {}
     for tag, o in (("mixed", om), ("fp64", o64)):
@@ -386,8 +394,9 @@ def run_reference(args, world, rank):
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded generator, no dataset)", "impl": "reference",
-        "config": {"workload": workload_desc(args.workload, n1), "n_particles": ncpu, "precision": "fp64",
-                   "parallelism": "host threads", "wall_s": round(wall, 1)},
+        "config": {"workload": workload_desc(args.workload, args.n1 or default_n1(args.workload)),
+                   "sample": workload_desc(args.workload, n1), "n_particles_per_sample": ncpu, "precision": "fp64",
+                   "parallelism": f"{cores} host threads", "wall_s": round(wall, 1)},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -926,9 +926,23 @@ static int rows_to_host(gz_context *c, const int *active, int n_active, int na, 
 
 int gz_neighbors(gz_context *c, const int *active, int n_active, int mode, int64_t *offsets, int *nbrs)
 {
-    if (!c || !offsets || (mode != 0 && mode != 1)) return GZ_ERR_ARG;
+    if (!c || !offsets || mode < 0 || mode > 2) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "neighbours before upload");
+    if (mode == 2) {
+        // the rows the last gradient/force pass over all particles used
+        if (!c->sym_valid || !c->sym_all) return fail(c, GZ_ERR_ORDER, "no symmetric rows of a pass over all particles");
+        int na_all = 0;
+        if (sort_targets(c, nullptr, 0, &na_all)) return c->err;
+        std::vector<long long> h_off;
+        std::vector<int> h_nbr, order;
+        const int rc = rows_to_host(c, active, n_active, na_all, c->s_off, c->s_nbr, h_off, h_nbr, order);
+        if (rc) return rc;
+        const size_t rows = order.size();
+        for (size_t r = 0; r <= rows; r++) offsets[r] = (int64_t)h_off[r];
+        if (nbrs && h_off[rows] > 0) memcpy(nbrs, h_nbr.data(), sizeof(int) * (size_t)h_off[rows]);
+        return GZ_OK;
+    }
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
     if (mode == 1 && refresh_hmax(c)) return c->err;

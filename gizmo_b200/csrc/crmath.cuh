@@ -11,9 +11,9 @@
 //  * double-double arithmetic with error-free transformations (Knuth's
 //    TwoSum, FMA-based TwoProduct) following Hida, Li and Bailey, "Library
 //    for double-double and quad-double arithmetic" (2007);
-//  * exp: Cody-Waite reduction x = k ln2 + r with ln2 in double-double,
-//    r scaled by 2^-8, Horner-form Taylor series of expm1 (11 terms), eight
-//    doublings expm1(2a) = expm1(a) (expm1(a) + 2), then 2^k;
+//  * exp: table-driven reduction x = (64 m + j) ln2/64 + r (Tang 1989) with a
+//    64-entry table of 2^(j/64) in double-double and a Taylor series of
+//    expm1(r), then 2^m;
 //  * log: one Newton step y1 = y0 + x exp(-y0) - 1 from the library log,
 //    evaluated in double-double (quadratic convergence: ~2^-100);
 //  * pow: exp(y log x) in double-double; y = 3, 2 and -1 are exact products
@@ -110,32 +110,126 @@ CR_HD dd dd_div_d(dd a, double b)
     return quick_two_sum(q1, q2);
 }
 
-// ln 2 = kLn2Hi + kLn2Lo to ~2^-107
+// ln 2 = kLn2Hi + kLn2Lo to ~2^-107; ln 2 / 64 likewise (exact scalings)
 constexpr double kLn2Hi = 6.93147180559945286226763982995e-01;
 constexpr double kLn2Lo = 2.31904681384629955842818503524e-17;
-constexpr double kInvLn2 = 1.44269504088896338700465094007e+00;
+constexpr double kLn2Hi64 = kLn2Hi / 64.0;
+constexpr double kLn2Lo64 = kLn2Lo / 64.0;
+constexpr double kInv64Ln2 = 92.33248261689366;
 
-// e^a for a double-double argument, as a double-double
+// 2^(j/64), j = 0..63, as double-doubles (hi, lo), from 70-digit arithmetic
+#define GZ_CR_EXP2_TABLE \
+    { \
+    {1.0, 0.0}, \
+    {1.0108892860517005, -1.5234778603368577e-17}, \
+    {1.0218971486541166, 5.109225028973444e-17}, \
+    {1.0330248790212284, 7.600838874027088e-18}, \
+    {1.0442737824274138, 8.551889705537965e-17}, \
+    {1.0556451783605572, 1.759325738772092e-18}, \
+    {1.0671404006768237, -7.899853966841582e-17}, \
+    {1.0787607977571199, -6.656660436056593e-17}, \
+    {1.0905077326652577, -3.046782079812471e-17}, \
+    {1.102382583307841, 5.2660368715706944e-17}, \
+    {1.1143867425958924, 1.0410278456845571e-16}, \
+    {1.1265216186082418, 5.165856758795457e-17}, \
+    {1.1387886347566916, 8.912812676025408e-17}, \
+    {1.1511892299529827, 3.250710218863827e-17}, \
+    {1.1637248587775775, 3.8292048369240935e-17}, \
+    {1.1763969916502812, 5.554203254218079e-17}, \
+    {1.189207115002721, 3.982015231465646e-17}, \
+    {1.202156731452703, 6.644981499252301e-17}, \
+    {1.215247359980469, -7.712630692681488e-17}, \
+    {1.22848053610687, -1.89878163130253e-17}, \
+    {1.241857812073484, 4.658027591836937e-17}, \
+    {1.255380757024691, -6.7113898212968784e-18}, \
+    {1.2690509571917332, 2.667932131342186e-18}, \
+    {1.2828700160787783, 1.713594918243561e-17}, \
+    {1.2968395546510096, 2.5382502794888315e-17}, \
+    {1.3109612115247644, -7.181536135519454e-17}, \
+    {1.3252366431597413, -2.8587312100388614e-17}, \
+    {1.339667524053303, 8.927282594831732e-17}, \
+    {1.3542555469368927, 7.70094837980299e-17}, \
+    {1.3690024229745905, 9.593797919118849e-17}, \
+    {1.383909881963832, -6.770511658794786e-17}, \
+    {1.3989796725383112, -9.614213209051323e-17}, \
+    {1.4142135623730951, -9.667293313452913e-17}, \
+    {1.42961333839197, -1.2031642489053655e-17}, \
+    {1.4451808069770467, -3.0237581349939873e-17}, \
+    {1.460917794180647, -5.600377186075216e-17}, \
+    {1.4768261459394993, -3.483994556892796e-17}, \
+    {1.4929077282912648, 1.4192920154284036e-17}, \
+    {1.5091644275934228, -1.016455327754295e-16}, \
+    {1.5255981507445384, -1.1024941712342561e-16}, \
+    {1.5422108254079407, 7.949834809697621e-17}, \
+    {1.559004400237837, 3.7812070533575275e-17}, \
+    {1.5759808451078865, -1.0136916471278304e-17}, \
+    {1.593142151342267, -1.0094406542311964e-16}, \
+    {1.6104903319492543, 2.4707192569797888e-17}, \
+    {1.6280274218573478, -6.712955084707084e-17}, \
+    {1.645755478153965, -1.0125679913674773e-16}, \
+    {1.6636765803267364, 5.8909926967131e-17}, \
+    {1.681792830507429, 8.199010020581497e-17}, \
+    {1.7001063537185235, -8.0237193703977e-18}, \
+    {1.718619298122478, -1.851380418263111e-17}, \
+    {1.7373338352737062, 3.164389299292957e-17}, \
+    {1.7562521603732995, 2.960140695448873e-17}, \
+    {1.7753764925265212, 6.429731796556572e-17}, \
+    {1.7947090750031072, 1.8227458427912087e-17}, \
+    {1.8142521755003989, -9.969531538920349e-17}, \
+    {1.8340080864093424, 3.283107224245627e-17}, \
+    {1.8539791250833855, 9.761887490727594e-17}, \
+    {1.8741676341103, -6.122763413004143e-17}, \
+    {1.8945759815869656, 3.4034035352165297e-17}, \
+    {1.9152065613971474, -1.0619946056195963e-16}, \
+    {1.9360617934922943, 1.0332385960676326e-16}, \
+    {1.9571441241754002, 8.960767791036668e-17}, \
+    {1.978456026387951, 4.0388753109278167e-17}, \
+    }
+#ifdef __CUDACC__
+static __constant__ double kExp2TableDev[64][2] = GZ_CR_EXP2_TABLE;
+#endif
+static const double kExp2TableHost[64][2] = GZ_CR_EXP2_TABLE;
+
+// e^a for a double-double argument, as a double-double, by table-driven
+// reduction (Tang, "Table-driven implementation of the exponential function
+// in IEEE floating-point arithmetic", 1989): a = (64 m + j) ln2 / 64 + r with
+// |r| <= ln2 / 128, e^a = 2^m 2^(j/64) e^r. expm1(r) is a Taylor series whose
+// first five terms are summed in double-double and whose terms from r^6 on
+// (below 1e-15 relative) in double, Horner form throughout; accuracy ~2^-100.
 CR_HD dd dd_exp(dd a)
 {
     if (a.hi > 709.7) return {INFINITY, 0.0};
     if (a.hi < -745.2) return {0.0, 0.0};
-    const double k = ::rint(mul(a.hi, kInvLn2));
-    dd kl = two_prod(k, kLn2Hi);
-    kl.lo = add(kl.lo, mul(k, kLn2Lo));
-    kl = quick_two_sum(kl.hi, kl.lo);
-    dd r = dd_add(a, dd_neg(kl));
-    r.hi = mul(r.hi, 1.0 / 256.0);  // exact scalings
-    r.lo = mul(r.lo, 1.0 / 256.0);
-    // expm1(r) = r (1 + r/2 (1 + r/3 (... (1 + r/11))))
-    dd s = {1.0, 0.0};
-    for (int i = 11; i >= 2; i--) s = dd_add({1.0, 0.0}, dd_div_d(dd_mul(r, s), (double)i));
-    s = dd_mul(r, s);
-    for (int i = 0; i < 8; i++) s = dd_add(dd_mul_d(s, 2.0), dd_mul(s, s));
-    dd e = dd_add({1.0, 0.0}, s);
-    const int ki = (int)k;
-    e.hi = ::ldexp(e.hi, ki);
-    e.lo = ::ldexp(e.lo, ki);
+    const double N = ::rint(mul(a.hi, kInv64Ln2));
+    dd nl = two_prod(N, kLn2Hi64);
+    nl.lo = add(nl.lo, mul(N, kLn2Lo64));
+    nl = quick_two_sum(nl.hi, nl.lo);
+    const dd r = dd_add(a, dd_neg(nl));
+    const double x = r.hi;
+    // sum_{k>=6} x^(k-6) / k!, to k = 12
+    double q = 2.08767569878680989792e-09;                 // 1/12!
+    q = add(mul(q, x), 2.50521083854417187751e-08);         // 1/11!
+    q = add(mul(q, x), 2.75573192239858906526e-07);         // 1/10!
+    q = add(mul(q, x), 2.75573192239858906526e-06);         // 1/9!
+    q = add(mul(q, x), 2.48015873015873015873e-05);         // 1/8!
+    q = add(mul(q, x), 1.98412698412698412698e-04);         // 1/7!
+    q = add(mul(q, x), 1.38888888888888888889e-03);         // 1/6!
+    dd s = dd_add({0.008333333333333333, 1.1564823173178714e-19}, {mul(q, x), 0.0});   // 1/5! + r q
+    s = dd_add(dd_mul(s, r), {0.041666666666666664, 2.3129646346357427e-18});           // 1/4!
+    s = dd_add(dd_mul(s, r), {0.16666666666666666, 9.25185853854297e-18});              // 1/3!
+    s = dd_add(dd_mul(s, r), {0.5, 0.0});
+    s = dd_add(dd_mul(s, r), {1.0, 0.0});
+    const dd p = dd_mul(s, r);  // expm1(r)
+    const int Ni = (int)N;
+    const int j = Ni & 63, m = (Ni - j) >> 6;
+#ifdef __CUDA_ARCH__
+    const dd t = {kExp2TableDev[j][0], kExp2TableDev[j][1]};
+#else
+    const dd t = {kExp2TableHost[j][0], kExp2TableHost[j][1]};
+#endif
+    dd e = dd_add(t, dd_mul(t, p));
+    e.hi = ::ldexp(e.hi, m);
+    e.lo = ::ldexp(e.lo, m);
     return e;
 }
 

@@ -168,7 +168,10 @@ void *gz_stream(gz_context *ctx);
 
 /* Exact neighbour sets of the last pass, for bit-exact checks against a CPU
  * search. mode 0: one-way r < h_i at the converged h; mode 1: symmetric
- * 0 < r and (r < h_i or r < h_j). Rows follow `active` (NULL = all),
+ * 0 < r and (r < h_i or r < h_j), from a tree walk; mode 2: the symmetric
+ * rows the last gradient/force pass over all particles used (derived from
+ * the density rows when the density pass covered every particle; otherwise
+ * GZ_ERR_ORDER). Rows follow `active` (NULL = all),
  * entries are original indices sorted ascending. Call once with
  * nbrs == NULL to get offsets (n_active + 1 entries); then with nbrs sized
  * offsets[n_active]. */

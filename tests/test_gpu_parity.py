@@ -140,6 +140,9 @@ def test_neighbour_sets_bit_exact(name):
         few = rng.choice(wl.n, size=wl.n // 20, replace=False).astype(np.int32)
         g0f = hp.neighbors(0, few)
         g1f = hp.neighbors(1, few)
+        # the rows the gradient pass used: derived from the density rows of the pass over all particles
+        hp.hydro_gradient_calc()
+        g2 = hp.neighbors(2)
     st = O.new_state(wl.n, wl.inputs())
     st["h"][:] = h
     o0 = O.neighbors(wl.params, st, 0)
@@ -147,7 +150,7 @@ def test_neighbour_sets_bit_exact(name):
     o1s = O.neighbors(wl.params, st, 1, sub)
     o0f = O.neighbors(wl.params, st, 0, few)
     o1f = O.neighbors(wl.params, st, 1, few)
-    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g1s, o1s), (g0f, o0f), (g1f, o1f)]:
+    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g1s, o1s), (g0f, o0f), (g1f, o1f), (g2, o1)]:
         assert np.array_equal(go, oo)
         assert np.array_equal(gn, on)
     assert g0[0][-1] > 20 * wl.n  # rows are populated
