@@ -24,6 +24,7 @@ ERR_CUDA = 2
 ERR_NO_DEVICE = 3
 ERR_ORDER = 4
 ERR_CAPACITY = 5
+ERR_INTERNAL = 6
 ERR_DENSITY_MAXITER = 1155
 ERR_EMPTY_BRACKET = 90001009
 ERR_RIEMANN = 1234

@@ -6,6 +6,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -58,7 +59,9 @@ struct gz_context {
     DevBuf acc, h_built, scratch, keep, regrow, todo_a, todo_b, grow, d_beg, d_end, flag, counts, d_off, d_nbr, n_sel;
     long long d_nbr_cap = 0, d_used = 0;
     bool dens_all = false;           // the density rows cover every particle (last pass had no active list)
+    DevBuf pad_over, pad_list, pad_sum, pad_counts;  // padded single-walk density rows
     DevBuf s_acnt, s_bcnt, s_tmp;    // symmetric rows derived from the density rows
+    DevBuf pflux, ppart;             // force pass evaluating each pair once: fluxes per row entry, partial sums
     // symmetric rows (shared by gradients and force)
     DevBuf s_off, s_nbr, s_counts;
     long long s_nbr_cap = 0;
@@ -109,6 +112,22 @@ int ensure(gz_context *c, DevBuf &b, size_t bytes)
     GZ_CUDA(c, cudaMalloc(&b.p, want));
     b.bytes = want;
     return 0;
+}
+
+// like ensure(), but a failed allocation is not an error of the context
+bool try_ensure(DevBuf &b, size_t bytes)
+{
+    if (b.bytes >= bytes && b.p) return true;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    if (cudaMalloc(&b.p, bytes > 0 ? bytes : 16) != cudaSuccess) {
+        cudaGetLastError();  // clear the allocation failure
+        b.p = nullptr;
+        return false;
+    }
+    b.bytes = bytes > 0 ? bytes : 16;
+    return true;
 }
 
 void release(DevBuf &b)
@@ -173,7 +192,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->work, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->ppart, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -338,6 +357,22 @@ int exclusive_scan_counts(gz_context *c, int rows, DevBuf &counts, DevBuf &off, 
     return 0;
 }
 
+// nbr holds at least `need` ints, its first `keep` kept if it must grow
+int grow_keep(gz_context *c, DevBuf &nbr, long long &cap, long long keep, long long need)
+{
+    if (need <= cap && nbr.p) return 0;
+    cudaStream_t s = c->stream;
+    const long long want = std::max(need, keep > 0 ? cap + cap / 2 : 0ll);
+    DevBuf grown;
+    if (ensure(c, grown, sizeof(int) * (size_t)std::max(want, 1ll))) return c->err;
+    if (keep > 0) GZ_CUDA(c, cudaMemcpyAsync(grown.p, nbr.p, sizeof(int) * (size_t)keep, cudaMemcpyDeviceToDevice, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    release(nbr);
+    nbr = grown;
+    cap = (long long)(nbr.bytes / sizeof(int));
+    return 0;
+}
+
 // Exact neighbour rows of `targets` (count walk, scan, fill walk), written
 // at nbr + base; the first `base` entries of nbr are kept if it must grow.
 int build_rows(gz_context *c, const double *reach, int symmetric, const int *targets, int rows, DevBuf &counts,
@@ -348,26 +383,81 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
     if (ensure(c, counts, sizeof(long long) * (size_t)std::max(rows, 1)) || ensure(c, c->work, sizeof(int)))
         return c->err;
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<long long>(counts), nullptr, nullptr, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
+              rows, ptr<long long>(counts), nullptr, nullptr, 0, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
     if (base + *total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
-    if (base + *total > cap || !nbr.p) {
-        const long long want = std::max(base + *total, base > 0 ? cap + cap / 2 : 0ll);
-        DevBuf grown;
-        if (ensure(c, grown, sizeof(int) * (size_t)std::max(want, 1ll))) return c->err;
-        if (base > 0) GZ_CUDA(c, cudaMemcpyAsync(grown.p, nbr.p, sizeof(int) * (size_t)base, cudaMemcpyDeviceToDevice, s));
-        GZ_CUDA(c, cudaStreamSynchronize(s));
-        release(nbr);
-        nbr = grown;
-        cap = (long long)(nbr.bytes / sizeof(int));
-    }
+    if (grow_keep(c, nbr, cap, base, base + *total)) return c->err;
     walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
-              rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, ptr<DevStatus>(c->status),
+              rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, 0, ptr<DevStatus>(c->status),
               ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// Density rows of `targets` in one walk: cap slots per target at d_nbr + base
+// (rows [beg, end) per particle); a row longer than cap is rebuilt by the
+// two-pass build behind the padded block. Returns the entries now in use and
+// the row entries built.
+int build_rows_padded(gz_context *c, const double *reach, const int *targets, int rows, int cap, long long base,
+                      long long *used, long long *entries)
+{
+    cudaStream_t s = c->stream;
+    const long long need = base + (long long)rows * cap;
+    if (need > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
+    if (grow_keep(c, c->d_nbr, c->d_nbr_cap, base, need)) return c->err;
+    const size_t R = (size_t)std::max(rows, 1);
+    if (ensure(c, c->counts, sizeof(long long) * R) || ensure(c, c->work, sizeof(int)) ||
+        ensure(c, c->pad_over, R) || ensure(c, c->pad_list, sizeof(int) * R) || ensure(c, c->n_sel, sizeof(int) * 2))
+        return c->err;
+    Tree t = tree_view(c);
+    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0, targets, rows,
+              ptr<long long>(c->counts), nullptr, ptr<int>(c->d_nbr) + base, cap, ptr<DevStatus>(c->status),
+              ptr<int>(c->work), s);
+    padded_rows(rows, targets, ptr<long long>(c->counts), cap, base, ptr<long long>(c->d_beg), ptr<long long>(c->d_end),
+                ptr<unsigned char>(c->pad_over), s);
+    c->launches += 2;
+    GZ_CUDA(c, cudaGetLastError());
+    // rows built: sum of the counts; rows over their cap: compacted list
+    size_t t1 = 0, t2 = 0;
+    cub::DeviceReduce::Sum(nullptr, t1, ptr<long long>(c->counts), ptr<long long>(c->pad_sum), rows, s);
+    cub::DeviceSelect::Flagged(nullptr, t2, targets, ptr<unsigned char>(c->pad_over), ptr<int>(c->pad_list),
+                               ptr<int>(c->n_sel), rows, s);
+    if (ensure(c, c->pad_sum, sizeof(long long)) || ensure(c, c->cub_tmp, std::max(t1, t2))) return c->err;
+    cub::DeviceReduce::Sum(c->cub_tmp.p, t1, ptr<long long>(c->counts), ptr<long long>(c->pad_sum), rows, s);
+    long long built = 0;
+    GZ_CUDA(c, cudaMemcpyAsync(&built, c->pad_sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    cub::DeviceSelect::Flagged(c->cub_tmp.p, t2, targets, ptr<unsigned char>(c->pad_over), ptr<int>(c->pad_list),
+                               ptr<int>(c->n_sel), rows, s);
+    int n_over = 0;
+    GZ_CUDA(c, cudaMemcpyAsync(&n_over, c->n_sel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    long long extra = 0;
+    if (n_over > 0) {
+        // the padded walk took every row's full count: the longer rows need the
+        // fill walk only, at offsets from those counts
+        if (ensure(c, c->pad_counts, sizeof(long long) * (size_t)n_over)) return c->err;
+        size_t t3 = 0;
+        cub::DeviceSelect::Flagged(nullptr, t3, ptr<long long>(c->counts), ptr<unsigned char>(c->pad_over),
+                                   ptr<long long>(c->pad_counts), ptr<int>(c->n_sel) + 1, rows, s);
+        if (ensure(c, c->cub_tmp, t3)) return c->err;
+        cub::DeviceSelect::Flagged(c->cub_tmp.p, t3, ptr<long long>(c->counts), ptr<unsigned char>(c->pad_over),
+                                   ptr<long long>(c->pad_counts), ptr<int>(c->n_sel) + 1, rows, s);
+        if (exclusive_scan_counts(c, n_over, c->pad_counts, c->d_off, &extra)) return c->err;
+        if (need + extra > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
+        if (grow_keep(c, c->d_nbr, c->d_nbr_cap, need, need + extra)) return c->err;
+        walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0,
+                  ptr<int>(c->pad_list), n_over, ptr<long long>(c->pad_counts), ptr<long long>(c->d_off),
+                  ptr<int>(c->d_nbr) + need, 0, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
+        k_set_rows<<<(n_over + 255) / 256, 256, 0, s>>>(n_over, ptr<int>(c->pad_list), ptr<long long>(c->d_off), need,
+                                                        ptr<long long>(c->d_beg), ptr<long long>(c->d_end));
+        c->launches += 2;
+        GZ_CUDA(c, cudaGetLastError());
+    }
+    *used = need + extra;
+    *entries = built;
     return 0;
 }
 
@@ -717,15 +807,13 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
                                                                iter == 0 ? kDensityBufferFirst : kDensityBuffer,
                                                                ptr<double>(c->h_built));
             c->launches++;
-            long long total = 0;
-            if (build_rows(c, ptr<double>(c->h_built), 0, grow, n_grow, c->counts, c->d_off, c->d_nbr, c->d_nbr_cap,
-                           &total, base))
-                return c->err;
-            k_set_rows<<<(n_grow + 255) / 256, 256, 0, s>>>(n_grow, grow, ptr<long long>(c->d_off), base,
-                                                             ptr<long long>(c->d_beg), ptr<long long>(c->d_end));
-            c->launches++;
-            base += total;
-            c->pairs_density += total;
+            // slots per padded row: 2.5 x the expected row length, in multiples of 32
+            const double f = iter == 0 ? kDensityBufferFirst : kDensityBuffer;
+            const int cap = std::max(32, std::min(4096, 32 * (int)std::ceil(2.5 * c->prm.des_num_ngb * f * f * f / 32.0)));
+            long long used = 0, entries = 0;
+            if (build_rows_padded(c, ptr<double>(c->h_built), grow, n_grow, cap, base, &used, &entries)) return c->err;
+            base = used;
+            c->pairs_density += entries;
         }
         DensityWork w{};
         w.todo = todo;
@@ -827,10 +915,24 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
     force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
-    if (c->prm.precision == GZ_PRECISION_MIXED)
-        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, c->stream);
-    else force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, c->stream);
-    if (na > 0) c->launches += 2;
+    // every particle a target: each pair evaluated once, its flux kept per row
+    // entry (when that scratch can be had; otherwise each row evaluates all)
+    const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
+    void *flux = nullptr;
+    double *partial = nullptr;
+    if (active == nullptr && na == c->n && c->n > 0 &&
+        try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)) &&
+        try_ensure(c->ppart, sizeof(double) * 13 * (size_t)c->n)) {
+        flux = c->pflux.p;
+        partial = ptr<double>(c->ppart);
+    }
+    if (mixed)
+        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
+                    partial, c->stream);
+    else
+        force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
+                   partial, c->stream);
+    if (na > 0) c->launches += flux ? 3 : 2;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
     return GZ_OK;

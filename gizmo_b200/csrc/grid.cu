@@ -221,7 +221,7 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                                            const double *__restrict__ y, const double *__restrict__ z,
                                            const double *__restrict__ reach, const double *__restrict__ hsym,
                                            const int *__restrict__ targets, int n_targets, long long *counts,
-                                           const long long *__restrict__ off, int *nbr, DevStatus *st,
+                                           const long long *__restrict__ off, int *nbr, int cap, DevStatus *st,
                                            StackNode (*s_stack)[kStack], double4 (*s_c)[32], double4 (*s_lo)[8],
                                            double4 (*s_hi)[8], int4 (*s_nd)[8])
 {
@@ -234,8 +234,11 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
     double xi = 0, yi = 0, zi = 0, ri = 0;
     if (valid) { xi = x[tg]; yi = y[tg]; zi = z[tg]; ri = reach[tg]; }
     const double ri2 = ri * ri;
+    // a row starts at off[slot] (exact counts known), or, with cap > 0, at
+    // slot * cap in a padded layout whose rows keep at most cap entries (the
+    // count is still taken in full: a longer row is rebuilt elsewhere)
     long long base = 0;
-    if (FILL && valid) base = off[slot];
+    if (FILL && valid) base = cap ? (long long)slot * cap : off[slot];
     long long cnt = 0;  // SOLO: the row length so far (uniform); else this lane's
     // does this lane's sphere reach box [l, u] holding h up to l.w?
     auto reaches = [&](const double4 &l, const double4 &u) -> bool {
@@ -281,7 +284,10 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                         }
                     }
                     const unsigned bal = __ballot_sync(full, acc);
-                    if (FILL && acc) nbr[base + cnt + __popc(bal & ((1u << lane) - 1u))] = jl;
+                    if (FILL && acc) {
+                        const long long k = cnt + __popc(bal & ((1u << lane) - 1u));
+                        if (!cap || k < cap) nbr[base + k] = jl;
+                    }
                     cnt += __popc(bal);
                 } else if (__popc(e.lanes) * 7 < min(32, b - c0) * 5) {
                     // few of the warp's targets reached this leaf: the lanes hold
@@ -306,8 +312,10 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                         }
                         const unsigned bal = __ballot_sync(full, acc);
                         if (FILL) {
-                            const long long at = __shfl_sync(full, base + cnt, tl);
-                            if (acc) nbr[at + __popc(bal & ((1u << lane) - 1u))] = jl;
+                            const long long tc = __shfl_sync(full, cnt, tl);
+                            const long long at = __shfl_sync(full, base, tl);
+                            const long long k = tc + __popc(bal & ((1u << lane) - 1u));
+                            if (acc && (!cap || k < cap)) nbr[at + k] = jl;
                         }
                         if (lane == tl) cnt += __popc(bal);
                     }
@@ -325,7 +333,7 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                             if (SYM) acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(cj.w, cj.w)));
                             else acc = r2 < ri2;
                             if (acc) {
-                                if (FILL) nbr[base + cnt] = c0 + k;
+                                if (FILL && (!cap || cnt < cap)) nbr[base + cnt] = c0 + k;
                                 cnt++;
                             }
                         }
@@ -367,7 +375,7 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
         sp += npush;
         __syncwarp();
     }
-    if (!FILL) {
+    if (!FILL || cap) {
         if (SOLO) { if (lane == 0) counts[slot] = cnt; }
         else if (valid) counts[slot] = cnt;
     }
@@ -381,7 +389,7 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
                                               const double *__restrict__ z, const double *__restrict__ reach,
                                               const double *__restrict__ hsym, const int *__restrict__ targets,
                                               int n_targets, long long *counts, const long long *__restrict__ off,
-                                              int *nbr, DevStatus *st, int *next_group)
+                                              int *nbr, int cap, DevStatus *st, int *next_group)
 {
     __shared__ StackNode s_stack[kWarps][kStack];
     __shared__ double4 s_c[kWarps][32];
@@ -394,7 +402,7 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
         if (lane == 0) g = atomicAdd(next_group, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= n_groups) break;
-        walk_group<SYM, FILL, SOLO>(g, t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st, s_stack,
+        walk_group<SYM, FILL, SOLO>(g, t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, s_stack,
                                     s_c, s_lo, s_hi, s_nd);
         __syncwarp();
     }
@@ -515,6 +523,27 @@ void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStre
     if (n > 0) k_sym_sort<<<(unsigned)(((long long)n * 32 + 255) / 256), 256, 0, s>>>(n, s_off, rows, out);
 }
 
+// After a padded fill: a row that fit its cap slots gets [slot*cap, +count);
+// a longer one is flagged for a rebuild.
+__global__ void k_padded_rows(int na, const int *__restrict__ t, const long long *__restrict__ counts, int cap,
+                              long long base, long long *beg, long long *end, unsigned char *over)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= na) return;
+    const long long c = counts[a];
+    over[a] = c > cap;
+    if (c <= cap) {
+        beg[t[a]] = base + (long long)a * cap;
+        end[t[a]] = base + (long long)a * cap + c;
+    }
+}
+
+void padded_rows(int na, const int *t, const long long *counts, int cap, long long base, long long *beg,
+                 long long *end, unsigned char *over, cudaStream_t s)
+{
+    if (na > 0) k_padded_rows<<<(na + 255) / 256, 256, 0, s>>>(na, t, counts, cap, base, beg, end, over);
+}
+
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s)
 {
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
@@ -542,7 +571,7 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
 template <bool SYM, bool FILL, bool SOLO>
 static void launch_walk(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                         const double *hsym, const int *targets, int n_targets, long long *counts, const long long *off,
-                        int *nbr, DevStatus *st, int *next_group, cudaStream_t s)
+                        int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
 {
     static int resident = 0;  // blocks of this instance resident per SM x SMs (device 0-independent enough)
     if (resident == 0) {
@@ -557,12 +586,12 @@ static void launch_walk(const Tree &t, const double *x, const double *y, const d
     const unsigned blocks = (unsigned)(need < resident ? need : resident);
     cudaMemsetAsync(next_group, 0, sizeof(int), s);
     k_walk<SYM, FILL, SOLO><<<blocks, 32 * kWarps, 0, s>>>(t, x, y, z, reach, hsym, targets, n_targets, counts, off,
-                                                            nbr, st, next_group);
+                                                            nbr, cap, st, next_group);
 }
 
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
-               const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s)
+               const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     // Group mode (32 targets per warp) for every list: with the transposed
@@ -570,7 +599,7 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
     // targets per ballot where the one-target mode tests one. The one-target
     // mode stays available for lists of a single target.
     const bool solo = n_targets == 1;
-#define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, st, next_group, s)
+#define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, next_group, s)
     if (symmetric) {
         if (solo) { if (nbr) GZ_WALK(true, true, true); else GZ_WALK(true, false, true); }
         else { if (nbr) GZ_WALK(true, true, false); else GZ_WALK(true, false, false); }

@@ -17,7 +17,10 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
              const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s);
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
-               const long long *off, int *nbr, DevStatus *st, int *next_group, cudaStream_t s);
+               const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s);
+// rows of a padded fill (cap > 0 above): [beg, end) for the rows that fit, over[a] = 1 for the others
+void padded_rows(int na, const int *t, const long long *counts, int cap, long long base, long long *beg,
+                 long long *end, unsigned char *over, cudaStream_t s);
 
 // symmetric rows derived from the density rows of a pass over all particles
 void sym_split(int n, const double *x, const double *y, const double *z, const double *h, double box,
@@ -59,14 +62,17 @@ void density_finalize(const PassParams &p, const Particles &ps, const double *ac
 // record_bytes(pass) bytes, 16-byte aligned.
 size_t gradient_record_bytes(int mixed);
 size_t force_record_bytes(int mixed);
+size_t pair_flux_bytes(int mixed);  // per symmetric row entry, for a force pass evaluating each pair once
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
                     void *rec, cudaStream_t s);
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
                      void *rec, cudaStream_t s);
+// flux / partial: NULL, or (every particle a target, targets[s] = s) scratch
+// for one evaluation per pair: n_entries x pair_flux_bytes and 13 x n doubles
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, cudaStream_t s);
+                DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s);
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, cudaStream_t s);
+                 DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s);
 void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
 
 }  // namespace gz

@@ -312,10 +312,22 @@ template <typename T> __global__ void k_pack_force(Particles ps, double gamma, F
 // hydro_functions.h:419-509, j-side dMass writes hydro_functions.h:511-532,
 // writeback hydro_force_loop.cc:227-391, final operations
 // hydro_toplevel.cc:133-253.
-template <typename T, int TPT>
+//
+// MODE kBoth: row i evaluates all its pairs (as the reference does: each pair
+//   twice, once per row). Used for active subsets.
+// MODE kUpper / kLower: a pass over every particle evaluates each pair once.
+//   kUpper: row i evaluates its pairs with j > i, stores each flux at the pair's
+//   row entry and its partial sums; kLower: row i reads the flux of each pair
+//   with j < i from i's entry in row j (rows are sorted: binary search), adds
+//   the partial sums and finishes. Both rows use the identical flux.
+constexpr int kBoth = 0, kUpper = 1, kLower = 2;
+constexpr int kPartials = 13;  // acc(3) dtE dtm dm gw(3) vs fa(3)
+
+template <typename T, int TPT, int MODE>
 __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const int *__restrict__ targets,
                                                int n_targets, Csr rows, DevStatus *st,
-                                               const ForceRec<T> *__restrict__ rec)
+                                               const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux,
+                                               double *partial)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -341,7 +353,16 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     int stop = 0;
     if (enabled) {
         vs = (double)rip->s.cs;
-        const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
+        long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
+        if (MODE != kBoth) {
+            // rows are sorted: the pairs with j > i are the row's tail
+            long long a = b0, b = b1;
+            while (a < b) {
+                const long long mid = a + ((b - a) >> 1);
+                if (rows.nbr[mid] < i) a = mid + 1; else b = mid;
+            }
+            if (MODE == kUpper) b0 = a; else b1 = a;
+        }
         for (long long e = b0 + lane; e < b1; e += TPT) {
             const int j = rows.nbr[e];
             const ForceRec<T> *rjp = rec + j;
@@ -352,17 +373,34 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
             const double hjd = rjp->h;
             const double dtj = rjp->s.dt;
             const int j_active = rjp->active;
-            PairFlux<T> F;
             // one call site for both orientations: the lower sorted index is the
             // R side, so rows i and j run the identical instruction sequence on
             // identical operands and get bit-identical fluxes
             const bool fwd = i < j;
             const double sign = fwd ? 1.0 : -1.0;
-            const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
-            // both sides are read from the records in place (global memory, L1-resident)
-            const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
-            force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd, fwd ? hjd : hid, F,
-                       stop);
+            PairFlux<T> F;
+            if (MODE == kLower) {
+                // the flux row j computed for this pair: i's entry in row j
+                const long long b_end = rows.off[j + 1];
+                long long a = rows.off[j], b = b_end;
+                while (a < b) {
+                    const long long mid = a + ((b - a) >> 1);
+                    if (rows.nbr[mid] < i) a = mid + 1; else b = mid;
+                }
+                if (a >= b_end || rows.nbr[a] != i) {  // rows not symmetric: cannot happen for rows built here
+                    stop = 6 /* GZ_ERR_INTERNAL */;
+                    continue;
+                }
+                F = flux[a];
+            } else {
+                const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
+                // both sides are read from the records in place (global memory, L1-resident)
+                const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
+                force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd,
+                           fwd ? hjd : hid, F, stop);
+                if (MODE == kUpper) flux[e] = F;
+            }
+            (void)r2;
             if (!F.valid) continue;
             const double frho = sign * (double)F.rho;
             acc[0] += sign * (double)F.v[0];
@@ -404,6 +442,19 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     dm = warp_sum(dm, mask, TPT);
     vs = warp_max(vs, mask, TPT);
     if (lane != 0) return;
+    if (MODE == kUpper) {
+        const double part[kPartials] = {acc[0], acc[1], acc[2], dtE, dtm, dm, gw[0], gw[1], gw[2], vs, fa[0], fa[1], fa[2]};
+#pragma unroll
+        for (int k = 0; k < kPartials; k++) partial[k * n + i] = part[k];
+        return;
+    }
+    if (MODE == kLower) {
+        for (int k = 0; k < 3; k++) { acc[k] += partial[k * n + i]; gw[k] += partial[(6 + k) * n + i]; fa[k] += partial[(10 + k) * n + i]; }
+        dtE += partial[3 * n + i];
+        dtm += partial[4 * n + i];
+        dm += partial[5 * n + i];
+        vs = fmax(vs, partial[9 * n + i]);
+    }
     // writeback: preloop zeros + this row's sums; MaxSignalVel floor
     const double cs_i = (rhoi > 0) ? sqrt(p.gamma * ps.pressure[i] / rhoi) : sqrt(p.gamma * (p.gamma - 1.) * ps.u[i]);
     double vsig = kMinReal;
@@ -436,20 +487,35 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     ps.dmass[i] += dm;
 }
 
+template <typename T, int MODE>
+void launch_force_mode(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
+                       DevStatus *st, const ForceRec<T> *rec, PairFlux<T> *flux, double *partial, cudaStream_t s)
+{
+    const long long threads = (long long)n_targets * tpt;
+    const unsigned blocks = (unsigned)((threads + 127) / 128);
+    switch (tpt) {
+        case 4: k_force<T, 4, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
+        case 8: k_force<T, 8, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
+        case 32: k_force<T, 32, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
+        default: k_force<T, 16, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
+    }
+}
+
+// `flux` (one PairFlux<T> per row entry) and `partial` ([kPartials][n]) given:
+// every particle is a target (targets[s] = s) and each pair is evaluated once;
+// otherwise (NULL) each row evaluates all its pairs.
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, void *recbuf, cudaStream_t s)
+                  DevStatus *st, void *recbuf, void *fluxbuf, double *partial, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     ForceRec<T> *rec = (ForceRec<T> *)recbuf;
     k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec);
-    const long long threads = (long long)n_targets * tpt;
-    const unsigned blocks = (unsigned)((threads + 127) / 128);
-    switch (tpt) {
-        case 4: k_force<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
-        case 8: k_force<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
-        case 32: k_force<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
-        default: k_force<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec); break;
+    if (fluxbuf && partial) {
+        launch_force_mode<T, kUpper>(p, ps, targets, n_targets, rows, tpt, st, rec, (PairFlux<T> *)fluxbuf, partial, s);
+        launch_force_mode<T, kLower>(p, ps, targets, n_targets, rows, tpt, st, rec, (PairFlux<T> *)fluxbuf, partial, s);
+    } else {
+        launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, nullptr, nullptr, s);
     }
 }
 

@@ -7,6 +7,7 @@ namespace gz {
 
 size_t gradient_record_bytes(int mixed) { return mixed ? sizeof(GradRec<float>) : sizeof(GradRec<double>); }
 size_t force_record_bytes(int mixed) { return mixed ? sizeof(ForceRec<float>) : sizeof(ForceRec<double>); }
+size_t pair_flux_bytes(int mixed) { return mixed ? sizeof(PairFlux<float>) : sizeof(PairFlux<double>); }
 
 __global__ void k_pack_density(Particles ps, DensRec *rec)
 {
@@ -35,9 +36,9 @@ void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, cudaStream_t s)
+                DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, s);
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, partial, s);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's

@@ -53,6 +53,7 @@ extern "C" {
 #define GZ_ERR_NO_DEVICE        3
 #define GZ_ERR_ORDER            4       /* pass called before its inputs exist */
 #define GZ_ERR_CAPACITY         5       /* a device work buffer would exceed its limit */
+#define GZ_ERR_INTERNAL         6       /* an internal consistency check failed (a bug: please report) */
 #define GZ_ERR_DENSITY_MAXITER  1155    /* neighbor_loop_runner.cc:7485 endrun(1155) */
 #define GZ_ERR_EMPTY_BRACKET    90001009 /* density_loop.h:891-895 */
 #define GZ_ERR_RIEMANN          1234    /* hydro_core_meshless_functions.h:403-425 */
