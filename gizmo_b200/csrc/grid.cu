@@ -594,11 +594,22 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
                const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
 {
     if (n_targets <= 0) return;
-    // Group mode (32 targets per warp) for every list: with the transposed
-    // leaf test it serves sparse lists as well, and its traversal tests 32
-    // targets per ballot where the one-target mode tests one. The one-target
-    // mode stays available for lists of a single target.
-    const bool solo = n_targets == 1;
+    // Group mode (32 targets per warp) for dense lists and for lists whose
+    // groups fill the warps the GPU holds resident: its traversal tests 32
+    // targets per ballot where the one-target mode tests one. A short sparse
+    // list (the rows rebuilt after an h regrowth, scattered through the box)
+    // gets one warp per target instead: as groups it would run on a few
+    // warps, each walking 32 unrelated regions one after another.
+    static long long group_warps = 0;
+    if (group_warps == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<false, true, false>, 32 * kWarps, 0);
+        group_warps = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarps;
+    }
+    const bool sparse = (long long)n_targets * 4 < (long long)t.n_particles;
+    const bool solo = n_targets == 1 || (sparse && (n_targets + 31) / 32 < group_warps);
 #define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, next_group, s)
     if (symmetric) {
         if (solo) { if (nbr) GZ_WALK(true, true, true); else GZ_WALK(true, false, true); }
