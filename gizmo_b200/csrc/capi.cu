@@ -76,10 +76,23 @@ struct gz_context {
     int last_iters = 0;
     long long pairs_density = 0, pairs_symmetric = 0;
     bool have_density = false, have_gradients = false;
-    int tpt_density = 16, tpt_gradient = 16, tpt_force = 8;
+    int tpt_force = 8;               // lanes per force row (fixed: measured best at every size)
+    int sms = 148;                   // multiprocessors of the device
 };
 
 namespace {
+
+// Lanes per row of the density and gradient row kernels. Fewer lanes per row
+// mean more rows in flight per warp and a shorter cross-lane reduction, but
+// fewer threads: 4 lanes while the rows still give about eight waves of
+// resident threads (2048 per multiprocessor), 8 or 16 for shorter lists.
+int lanes_per_row(const gz_context *c, long long rows)
+{
+    const long long want = (long long)c->sms * 2048 * 8;
+    int tpt = 4;
+    while (tpt < 16 && rows * tpt < want) tpt *= 2;
+    return tpt;
+}
 
 int fail(gz_context *c, int code, const char *what)
 {
@@ -640,6 +653,8 @@ int gz_create(const gz_params *params, int device, gz_context **out)
     c->prm = *params;
     c->pp = make_pass_params(*params);
     c->device = device;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) c->sms = sms;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return GZ_ERR_CUDA; }
     if (ensure(c, c->status, sizeof(DevStatus))) { cudaStreamDestroy(c->stream); delete c; return GZ_ERR_CUDA; }
     cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
@@ -830,8 +845,8 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         w.rebuild = ptr<int>(c->flag);
         w.iter = iter;
         GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
-        if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
-        else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);
+        if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
+        else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
         density_after_iter(c->pp, ps, w, ptr<DevStatus>(c->status), s);
         c->launches += 2;
         GZ_CUDA(c, cudaGetLastError());
@@ -885,8 +900,8 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
-    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->rec.p, c->stream);
-    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_gradient, c->rec.p, c->stream);
+    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na), c->rec.p, c->stream);
+    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na), c->rec.p, c->stream);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -1092,8 +1107,8 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     w.rec = ptr<DensRec>(c->rec);
     density_pack(ps, ptr<DensRec>(c->rec), s);
     w.acc = ptr<double>(c->acc);
-    if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, c->tpt_density, s);
-    else density_sums_fp64(c->pp, ps, w, c->tpt_density, s);
+    if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
+    else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
     GZ_CUDA(c, cudaGetLastError());
     const int n = c->n;
     std::vector<double> a17((size_t)17 * (size_t)std::max(n, 1));

@@ -16,8 +16,10 @@ namespace gz {
 // ---------------------------------------------------------------- density
 // DensitySpec::pair_kernel (density_loop.h:1140-1385), gas i, gas j; the
 // row is a superset (buffered radius) and r2 < h^2 is re-tested exactly.
+constexpr int kDensityBlock = 128;
+
 template <typename T, int TPT>
-__global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps, DensityWork w)
+__global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p, Particles ps, DensityWork w)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -77,18 +79,11 @@ __global__ void __launch_bounds__(256) k_density_sums(PassParams p, Particles ps
             a[3] -= (double)(dwk * (px * dvx + py * dvy + pz * dvz) / r);
         }
     };
-    // two entries per step: both records are in flight before either is used
+    // one record in flight per lane: the register budget goes to resident
+    // warps (six 128-thread blocks per multiprocessor), which hide the
+    // gather latency better than a second record per lane does
     const long long b0 = w.beg[t], b1 = w.end[t];
-    for (long long e = b0 + lane; e < b1; e += 2 * TPT) {
-        const long long e1 = e + TPT;
-        const bool two = e1 < b1;
-        const int j0 = w.nbr[e];
-        const int j1 = two ? w.nbr[e1] : j0;
-        const DensRec r0 = w.rec[j0];
-        const DensRec r1 = w.rec[j1];
-        pair(r0);
-        if (two) pair(r1);
-    }
+    for (long long e = b0 + lane; e < b1; e += TPT) pair(w.rec[w.nbr[e]]);
 #pragma unroll
     for (int k = 0; k < 17; k++) a[k] = warp_sum(a[k], mask, TPT);
     if (lane == 0) {
@@ -103,12 +98,12 @@ void launch_density_sums(const PassParams &p, const Particles &ps, const Density
 {
     if (w.n_todo <= 0) return;
     const long long threads = (long long)w.n_todo * tpt;
-    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    const unsigned blocks = (unsigned)((threads + kDensityBlock - 1) / kDensityBlock);
     switch (tpt) {
-        case 4: k_density_sums<T, 4><<<blocks, 256, 0, s>>>(p, ps, w); break;
-        case 8: k_density_sums<T, 8><<<blocks, 256, 0, s>>>(p, ps, w); break;
-        case 32: k_density_sums<T, 32><<<blocks, 256, 0, s>>>(p, ps, w); break;
-        default: k_density_sums<T, 16><<<blocks, 256, 0, s>>>(p, ps, w); break;
+        case 4: k_density_sums<T, 4><<<blocks, kDensityBlock, 0, s>>>(p, ps, w); break;
+        case 8: k_density_sums<T, 8><<<blocks, kDensityBlock, 0, s>>>(p, ps, w); break;
+        case 32: k_density_sums<T, 32><<<blocks, kDensityBlock, 0, s>>>(p, ps, w); break;
+        default: k_density_sums<T, 16><<<blocks, kDensityBlock, 0, s>>>(p, ps, w); break;
     }
 }
 
@@ -137,7 +132,7 @@ template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *
 // finalize: construct_gradient (gradients_loop.cc:129-136) and
 // local_slopelimiter (gradients_loop.cc:1077-1130).
 template <typename T, int TPT>
-__global__ void __launch_bounds__(128) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
+__global__ void __launch_bounds__(128, 5) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
                                                    int n_targets, Csr rows, const GradRec<T> *__restrict__ rec)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
