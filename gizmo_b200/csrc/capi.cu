@@ -61,7 +61,7 @@ struct gz_context {
     bool dens_all = false;           // the density rows cover every particle (last pass had no active list)
     DevBuf pad_over, pad_list, pad_sum, pad_counts;  // padded single-walk density rows
     DevBuf s_acnt, s_bcnt, s_tmp;    // symmetric rows derived from the density rows
-    DevBuf pflux, ppart;             // force pass evaluating each pair once: fluxes per row entry, partial sums
+    DevBuf pflux;                    // force pass evaluating each pair once: the flux per row entry
     // symmetric rows (shared by gradients and force)
     DevBuf s_off, s_nbr, s_counts;
     long long s_nbr_cap = 0;
@@ -205,7 +205,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->work, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->ppart, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -934,19 +934,15 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     // entry (when that scratch can be had; otherwise each row evaluates all)
     const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
     void *flux = nullptr;
-    double *partial = nullptr;
     if (active == nullptr && na == c->n && c->n > 0 &&
-        try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)) &&
-        try_ensure(c->ppart, sizeof(double) * 13 * (size_t)c->n)) {
+        try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)))
         flux = c->pflux.p;
-        partial = ptr<double>(c->ppart);
-    }
     if (mixed)
         force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                    partial, c->stream);
+                    c->stream);
     else
         force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                   partial, c->stream);
+                   c->stream);
     if (na > 0) c->launches += flux ? 3 : 2;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;

@@ -67,12 +67,12 @@ void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets
                     void *rec, cudaStream_t s);
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
                      void *rec, cudaStream_t s);
-// flux / partial: NULL, or (every particle a target, targets[s] = s) scratch
-// for one evaluation per pair: n_entries x pair_flux_bytes and 13 x n doubles
+// flux: NULL, or (every particle a target, targets[s] = s) scratch for one
+// evaluation per pair: n_entries x pair_flux_bytes
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s);
+                DevStatus *st, void *rec, void *flux, cudaStream_t s);
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s);
+                 DevStatus *st, void *rec, void *flux, cudaStream_t s);
 void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
 
 }  // namespace gz

@@ -310,19 +310,17 @@ template <typename T> __global__ void k_pack_force(Particles ps, double gamma, F
 //
 // MODE kBoth: row i evaluates all its pairs (as the reference does: each pair
 //   twice, once per row). Used for active subsets.
-// MODE kUpper / kLower: a pass over every particle evaluates each pair once.
-//   kUpper: row i evaluates its pairs with j > i, stores each flux at the pair's
-//   row entry and its partial sums; kLower: row i reads the flux of each pair
-//   with j < i from i's entry in row j (rows are sorted: binary search), adds
-//   the partial sums and finishes. Both rows use the identical flux.
-constexpr int kBoth = 0, kUpper = 1, kLower = 2;
-constexpr int kPartials = 13;  // acc(3) dtE dtm dm gw(3) vs fa(3)
+// MODE kGather: a pass over every particle evaluates each pair once, in
+//   k_force_pairs, which stores its flux at both of the pair's row entries;
+//   row i then reads the flux of every entry in place and accumulates it with
+//   i's sign. Both rows use the identical flux.
+constexpr int kBoth = 0, kGather = 1;
 
 template <typename T, int TPT, int MODE>
 __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const int *__restrict__ targets,
                                                int n_targets, Csr rows, DevStatus *st,
-                                               const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux,
-                                               double *partial)
+                                               const ForceRec<T> *__restrict__ rec,
+                                               const PairFlux<T> *__restrict__ flux)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -348,21 +346,19 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     int stop = 0;
     if (enabled) {
         vs = (double)rip->s.cs;
-        long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
-        if (MODE != kBoth) {
-            // rows are sorted: the pairs with j > i are the row's tail
-            long long a = b0, b = b1;
-            while (a < b) {
-                const long long mid = a + ((b - a) >> 1);
-                if (rows.nbr[mid] < i) a = mid + 1; else b = mid;
-            }
-            if (MODE == kUpper) b0 = a; else b1 = a;
-        }
+        const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         for (long long e = b0 + lane; e < b1; e += TPT) {
             const int j = rows.nbr[e];
+            PairFlux<T> F;
+            if (MODE == kGather) {
+                F = flux[e];  // valid only if both particles have mass and density
+                if (!F.valid) continue;
+            }
             const ForceRec<T> *rjp = rec + j;
             const double mj = rjp->m, rhoj = rjp->rho;
-            if (!(mj > 0 && rhoj > 0)) continue;
+            // (a gathered flux is valid only if j has mass and density: the
+            // test is the pair kernel's, and its loads go unused for MFM)
+            if (MODE == kBoth && !(mj > 0 && rhoj > 0)) continue;
             double dx, dy, dz;
             const double r2 = sep2(xi, yi, zi, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
             const double hjd = rjp->h;
@@ -373,27 +369,12 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
             // identical operands and get bit-identical fluxes
             const bool fwd = i < j;
             const double sign = fwd ? 1.0 : -1.0;
-            PairFlux<T> F;
-            if (MODE == kLower) {
-                // the flux row j computed for this pair: i's entry in row j
-                const long long b_end = rows.off[j + 1];
-                long long a = rows.off[j], b = b_end;
-                while (a < b) {
-                    const long long mid = a + ((b - a) >> 1);
-                    if (rows.nbr[mid] < i) a = mid + 1; else b = mid;
-                }
-                if (a >= b_end || rows.nbr[a] != i) {  // rows not symmetric: cannot happen for rows built here
-                    stop = 6 /* GZ_ERR_INTERNAL */;
-                    continue;
-                }
-                F = flux[a];
-            } else {
+            if (MODE == kBoth) {
                 const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
                 // both sides are read from the records in place (global memory, L1-resident)
                 const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
                 force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd,
                            fwd ? hjd : hid, F, stop);
-                if (MODE == kUpper) flux[e] = F;
             }
             (void)r2;
             if (!F.valid) continue;
@@ -437,19 +418,6 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     dm = warp_sum(dm, mask, TPT);
     vs = warp_max(vs, mask, TPT);
     if (lane != 0) return;
-    if (MODE == kUpper) {
-        const double part[kPartials] = {acc[0], acc[1], acc[2], dtE, dtm, dm, gw[0], gw[1], gw[2], vs, fa[0], fa[1], fa[2]};
-#pragma unroll
-        for (int k = 0; k < kPartials; k++) partial[k * n + i] = part[k];
-        return;
-    }
-    if (MODE == kLower) {
-        for (int k = 0; k < 3; k++) { acc[k] += partial[k * n + i]; gw[k] += partial[(6 + k) * n + i]; fa[k] += partial[(10 + k) * n + i]; }
-        dtE += partial[3 * n + i];
-        dtm += partial[4 * n + i];
-        dm += partial[5 * n + i];
-        vs = fmax(vs, partial[9 * n + i]);
-    }
     // writeback: preloop zeros + this row's sums; MaxSignalVel floor
     const double cs_i = (rhoi > 0) ? sqrt(p.gamma * ps.pressure[i] / rhoi) : sqrt(p.gamma * (p.gamma - 1.) * ps.u[i]);
     double vsig = kMinReal;
@@ -482,35 +450,134 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     ps.dmass[i] += dm;
 }
 
+// Each pair of the symmetric rows once, for a pass over every particle
+// (targets[s] = s, rows sorted). A warp takes kPairRows consecutive rows and
+// spreads the pairs j > i of all of them over its lanes, one pair per lane per
+// round, so no lane idles on a short row. The pair is evaluated in the
+// canonical orientation (lower index as the i side), and its flux is stored at
+// the pair's entry in row i and at i's entry in row j (a binary search of the
+// sorted row j); a pair of which either particle has no mass or density stores
+// an invalid flux. k_force<kGather> then accumulates both rows from the stored
+// fluxes.
+constexpr int kPairRows = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps, int n_rows, Csr rows, DevStatus *st,
+                                                     const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux)
+{
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long r0 = warp * kPairRows;
+    if (r0 >= n_rows) return;  // the whole warp leaves together
+    const unsigned full = 0xffffffffu;
+    // lane k: row r0 + k, its first entry with j > i and the number of such entries
+    long long split = 0;
+    int cnt = 0;
+    if (lane < kPairRows && r0 + lane < n_rows) {
+        const int i = (int)(r0 + lane);
+        long long a = rows.off[i], b = rows.off[i + 1];
+        const long long end = b;
+        while (a < b) {
+            const long long mid = a + ((b - a) >> 1);
+            if (rows.nbr[mid] <= i) a = mid + 1; else b = mid;
+        }
+        split = a;
+        cnt = (int)(end - a);
+    }
+    int incl = cnt;  // inclusive scan of the counts over the warp
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(full, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    const int mfv = p.method == 1;
+    GConst<T> gc;
+    {
+        const double G0 = p.gamma;
+        gc.G0 = T(G0); gc.G1 = T((G0 - 1.0) / (2.0 * G0)); gc.G2 = T((G0 + 1.0) / (2.0 * G0));
+        gc.G3 = T((2.0 * G0 / (G0 - 1.0))); gc.G4 = T(2.0 / (G0 - 1.0)); gc.G5 = T(2.0 / (G0 + 1.0));
+        gc.G6 = T((G0 - 1.0) / (G0 + 1.0)); gc.G7 = T(0.5 * (G0 - 1.0)); gc.G8 = T(1.0 / G0); gc.G9 = T(G0 - 1.0);
+        gc.mfv = mfv;
+    }
+    int stop = 0, stop_index = -1;
+    for (int base = 0; base < total; base += 32) {
+        const int f = base + lane;
+        // the row of pair f: the number of rows whose inclusive count is <= f
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int v = __shfl_sync(full, incl, k + step - 1);
+            if (v <= f) k += step;
+        }
+        const int excl_k = __shfl_sync(full, incl - cnt, k);
+        const long long split_k = __shfl_sync(full, split, k);
+        if (f >= total) continue;
+        const int i = (int)(r0 + k);
+        const long long e = split_k + (f - excl_k);
+        const int j = rows.nbr[e];
+        const ForceRec<T> *rip = rec + i, *rjp = rec + j;
+        PairFlux<T> F;
+        F.valid = 0;
+        F.rho = F.p = T(0);
+        F.v[0] = F.v[1] = F.v[2] = T(0);
+        F.vsig_ts = T(0);
+        if (rip->m > 0 && rip->rho > 0 && rjp->m > 0 && rjp->rho > 0) {
+            double dx, dy, dz;
+            const double r2 = sep2(rip->x, rip->y, rip->z, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
+            const T dp[3] = {T(dx), T(dy), T(dz)};
+            int pstop = 0;
+            force_pair(p.kernel, mfv, p.selfgravity_off, gc, rip->s, rjp->s, dp, r2, rip->h, rjp->h, F, pstop);
+            if (pstop && !stop) { stop = pstop; stop_index = i; }
+        }
+        flux[e] = F;
+        // i's entry in row j
+        const long long b_end = rows.off[j + 1];
+        long long a = rows.off[j], b = b_end;
+        while (a < b) {
+            const long long mid = a + ((b - a) >> 1);
+            if (rows.nbr[mid] < i) a = mid + 1; else b = mid;
+        }
+        if (a >= b_end || rows.nbr[a] != i) {  // rows not symmetric: cannot happen for rows built here
+            if (!stop) { stop = 6 /* GZ_ERR_INTERNAL */; stop_index = i; }
+            continue;
+        }
+        flux[a] = F;
+    }
+    if (stop) record_status(st, stop, stop_index);
+}
+
 template <typename T, int MODE>
 void launch_force_mode(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                       DevStatus *st, const ForceRec<T> *rec, PairFlux<T> *flux, double *partial, cudaStream_t s)
+                       DevStatus *st, const ForceRec<T> *rec, const PairFlux<T> *flux, cudaStream_t s)
 {
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);
     switch (tpt) {
-        case 4: k_force<T, 4, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
-        case 8: k_force<T, 8, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
-        case 32: k_force<T, 32, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
-        default: k_force<T, 16, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux, partial); break;
+        case 4: k_force<T, 4, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
+        case 8: k_force<T, 8, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
+        case 32: k_force<T, 32, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
+        default: k_force<T, 16, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
     }
 }
 
-// `flux` (one PairFlux<T> per row entry) and `partial` ([kPartials][n]) given:
-// every particle is a target (targets[s] = s) and each pair is evaluated once;
-// otherwise (NULL) each row evaluates all its pairs.
+// `flux` (one PairFlux<T> per row entry) given: every particle is a target
+// (targets[s] = s) and each pair is evaluated once; otherwise (NULL) each row
+// evaluates all its pairs.
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, void *recbuf, void *fluxbuf, double *partial, cudaStream_t s)
+                  DevStatus *st, void *recbuf, void *fluxbuf, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     ForceRec<T> *rec = (ForceRec<T> *)recbuf;
     k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec);
-    if (fluxbuf && partial) {
-        launch_force_mode<T, kUpper>(p, ps, targets, n_targets, rows, tpt, st, rec, (PairFlux<T> *)fluxbuf, partial, s);
-        launch_force_mode<T, kLower>(p, ps, targets, n_targets, rows, tpt, st, rec, (PairFlux<T> *)fluxbuf, partial, s);
+    if (fluxbuf) {
+        PairFlux<T> *flux = (PairFlux<T> *)fluxbuf;
+        const long long warps = (n_targets + kPairRows - 1) / kPairRows;
+        k_force_pairs<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, n_targets, rows, st, rec, flux);
+        launch_force_mode<T, kGather>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, s);
     } else {
-        launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, nullptr, nullptr, s);
+        launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, nullptr, s);
     }
 }
 

@@ -36,9 +36,9 @@ void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *partial, cudaStream_t s)
+                DevStatus *st, void *rec, void *flux, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, partial, s);
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, s);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's
