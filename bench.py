@@ -270,6 +270,12 @@ def run_ours(args, world, rank, local):
     #  stated against the scale of the terms summed (flux_abs, an FP64 diagnostic).
     fields = ["h", "rho", "pressure", "grad_rho", "grad_p", "grad_v", "accel", "dudt", "dtmass", "vsig"]
     om = hpm.download(fields + ["iters"])
+    # the flux-scale denominators come from one more FP64 pass with the
+    # flux_abs diagnostic on (it is off in the timed passes); the pass's own
+    # outputs are the same with it on or off
+    hp64.set_diagnostics(flux_abs=True)
+    hp64.restage()
+    hp64.full_pass()
     o64 = hp64.download(fields + ["iters", "flux_abs"])
     fa = o64["flux_abs"]
     vmag = np.linalg.norm(wl.vel, axis=1)

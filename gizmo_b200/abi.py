@@ -92,11 +92,12 @@ class GzStatusInfo(C.Structure):
 
 
 EXPORTED_SYMBOLS = [
-    "gz_create", "gz_destroy", "gz_set_params", "gz_upload", "gz_restage", "gz_hydro_density",
+    "gz_create", "gz_destroy", "gz_set_params", "gz_set_diagnostics", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc",
 ]
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
+DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libgizmo_hydro.so")
@@ -119,6 +120,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_create.argtypes = [C.POINTER(GzParams), C.c_int, C.POINTER(vp)]
     lib.gz_destroy.argtypes = [vp]
     lib.gz_set_params.argtypes = [vp, C.POINTER(GzParams)]
+    lib.gz_set_diagnostics.argtypes = [vp, C.c_int]
     lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
     lib.gz_restage.argtypes = [vp]
     for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):

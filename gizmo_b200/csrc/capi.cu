@@ -77,6 +77,8 @@ struct gz_context {
     long long pairs_density = 0, pairs_symmetric = 0;
     bool have_density = false, have_gradients = false;
     int tpt_force = 8;               // lanes per force row (fixed: measured best at every size)
+    int diag = 0;                    // GZ_DIAG_* flags
+    bool fabs_valid = false;         // the last force pass summed flux_abs
     int sms = 148;                   // multiprocessors of the device
 };
 
@@ -679,7 +681,16 @@ int gz_set_params(gz_context *c, const gz_params *params)
     const bool box_changed = params->box_size != c->prm.box_size;
     c->prm = *params;
     c->pp = make_pass_params(*params);
+    c->pp.diag_flux_abs = (c->diag & GZ_DIAG_FLUX_ABS) != 0;
     if (box_changed) c->grid_valid = false;
+    return GZ_OK;
+}
+
+int gz_set_diagnostics(gz_context *c, int flags)
+{
+    if (!c || (flags & ~GZ_DIAG_FLUX_ABS)) return GZ_ERR_ARG;
+    c->diag = flags;
+    c->pp.diag_flux_abs = (flags & GZ_DIAG_FLUX_ABS) != 0;
     return GZ_OK;
 }
 
@@ -692,6 +703,7 @@ static int stage_inputs(gz_context *c)
 {
     const int n = c->n;
     cudaStream_t s = c->stream;
+    c->fabs_valid = false;
     GZ_CUDA(c, cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
     c->err = 0;
     c->err_index = -1;
@@ -930,6 +942,7 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
     force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
+    c->fabs_valid = c->pp.diag_flux_abs != 0;
     // every particle a target: each pair evaluated once, its flux kept per row
     // entry (when that scratch can be had; otherwise each row evaluates all)
     const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
@@ -937,13 +950,15 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     if (active == nullptr && na == c->n && c->n > 0 &&
         try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)))
         flux = c->pflux.p;
+    // the rows' sums before the writeback go to the density accumulators
+    // (17 x n doubles, unused between density passes)
     if (mixed)
         force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                    c->stream);
+                    ptr<double>(c->acc), c->stream);
     else
         force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                   c->stream);
-    if (na > 0) c->launches += flux ? 3 : 2;
+                   ptr<double>(c->acc), c->stream);
+    if (na > 0) c->launches += flux ? 4 : 3;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
     return GZ_OK;
@@ -952,6 +967,8 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
 int gz_download(gz_context *c, const gz_outputs *o)
 {
     if (!c || !o) return GZ_ERR_ARG;
+    if (o->flux_abs && !c->fabs_valid)
+        return fail(c, GZ_ERR_ORDER, "flux_abs: the last force pass ran without GZ_DIAG_FLUX_ABS");
     cudaSetDevice(c->device);
     const int n = c->n;
     if (n == 0) return GZ_OK;

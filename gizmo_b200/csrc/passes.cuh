@@ -289,7 +289,16 @@ template <typename T> struct __align__(16) ForceRec {
     int active;
 };
 
-template <typename T> __global__ void k_pack_force(Particles ps, double gamma, ForceRec<T> *rec)
+// What the gathering force pass reads of each neighbour for the MFV mass
+// bookkeeping and the GravWorkTerm: FP64 position, mass and dt, and whether it
+// is active (48 bytes: three 16-byte loads, in place of four sectors of the
+// neighbour's force record).
+struct __align__(16) GatherRec {
+    double x, y, z, m, dt;
+    int active, pad;
+};
+
+template <typename T> __global__ void k_pack_force(Particles ps, double gamma, ForceRec<T> *rec, GatherRec *grec)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ps.n) return;
@@ -298,6 +307,11 @@ template <typename T> __global__ void k_pack_force(Particles ps, double gamma, F
     load_side(ps, i, gamma, r.s);
     r.active = ps.active[i];
     rec[i] = r;
+    GatherRec g;
+    g.x = r.x; g.y = r.y; g.z = r.z; g.m = r.m; g.dt = ps.dt[i];
+    g.active = r.active;
+    g.pad = 0;
+    grec[i] = g;
 }
 
 // Row i of the symmetric list: every pair is evaluated in one canonical
@@ -315,12 +329,14 @@ template <typename T> __global__ void k_pack_force(Particles ps, double gamma, F
 //   row i then reads the flux of every entry in place and accumulates it with
 //   i's sign. Both rows use the identical flux.
 constexpr int kBoth = 0, kGather = 1;
+constexpr int kRowSums = 13;  // per row: acc(3) dtE dtm dm gw(3) vs, then the flux_abs diagnostic(3)
 
 template <typename T, int TPT, int MODE>
 __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const int *__restrict__ targets,
                                                int n_targets, Csr rows, DevStatus *st,
                                                const ForceRec<T> *__restrict__ rec,
-                                               const PairFlux<T> *__restrict__ flux)
+                                               const GatherRec *__restrict__ grec,
+                                               const PairFlux<T> *__restrict__ flux, double *sums)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = gtid / TPT, lane = gtid % TPT;
@@ -350,43 +366,52 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
         for (long long e = b0 + lane; e < b1; e += TPT) {
             const int j = rows.nbr[e];
             PairFlux<T> F;
+            double mj, dtj, dx, dy, dz;
+            int j_active;
             if (MODE == kGather) {
                 F = flux[e];  // valid only if both particles have mass and density
                 if (!F.valid) continue;
-            }
-            const ForceRec<T> *rjp = rec + j;
-            const double mj = rjp->m, rhoj = rjp->rho;
-            // (a gathered flux is valid only if j has mass and density: the
-            // test is the pair kernel's, and its loads go unused for MFM)
-            if (MODE == kBoth && !(mj > 0 && rhoj > 0)) continue;
-            double dx, dy, dz;
-            const double r2 = sep2(xi, yi, zi, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
-            const double hjd = rjp->h;
-            const double dtj = rjp->s.dt;
-            const int j_active = rjp->active;
-            // one call site for both orientations: the lower sorted index is the
-            // R side, so rows i and j run the identical instruction sequence on
-            // identical operands and get bit-identical fluxes
-            const bool fwd = i < j;
-            const double sign = fwd ? 1.0 : -1.0;
-            if (MODE == kBoth) {
-                const T dp[3] = {T(sign * dx), T(sign * dy), T(sign * dz)};
+                if (mfv) {  // only the MFV bookkeeping reads the neighbour
+                    const GatherRec g = grec[j];
+                    mj = g.m;
+                    dtj = g.dt;
+                    j_active = g.active;
+                    sep2(xi, yi, zi, g.x, g.y, g.z, p.box, p.half, dx, dy, dz);
+                }
+            } else {
+                const ForceRec<T> *rjp = rec + j;
+                mj = rjp->m;
+                const double rhoj = rjp->rho;
+                if (!(mj > 0 && rhoj > 0)) continue;
+                const double r2 = sep2(xi, yi, zi, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
+                const double hjd = rjp->h;
+                dtj = rjp->s.dt;
+                j_active = rjp->active;
+                // one call site for both orientations: the lower sorted index is
+                // the i side of the face, so rows i and j run the identical
+                // instruction sequence on identical operands and get
+                // bit-identical fluxes
+                const bool fwd = i < j;
+                const double sgn = fwd ? 1.0 : -1.0;
+                const T dp[3] = {T(sgn * dx), T(sgn * dy), T(sgn * dz)};
                 // both sides are read from the records in place (global memory, L1-resident)
                 const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
                 force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd,
                            fwd ? hjd : hid, F, stop);
+                if (!F.valid) continue;
             }
-            (void)r2;
-            if (!F.valid) continue;
+            const double sign = (i < j) ? 1.0 : -1.0;
             const double frho = sign * (double)F.rho;
             acc[0] += sign * (double)F.v[0];
             acc[1] += sign * (double)F.v[1];
             acc[2] += sign * (double)F.v[2];
             dtE += sign * (double)F.p;
-            fa[0] += fabs(frho);
-            fa[1] += sqrt((double)F.v[0] * (double)F.v[0] + (double)F.v[1] * (double)F.v[1] +
-                          (double)F.v[2] * (double)F.v[2]);
-            fa[2] += fabs((double)F.p);
+            if (p.diag_flux_abs) {
+                fa[0] += fabs(frho);
+                fa[1] += sqrt((double)F.v[0] * (double)F.v[0] + (double)F.v[1] * (double)F.v[1] +
+                              (double)F.v[2] * (double)F.v[2]);
+                fa[2] += fabs((double)F.p);
+            }
             if ((double)F.vsig_ts > vs) vs = (double)F.vsig_ts;
             if (mfv) {
                 double self_dm, accepted, other_dm;
@@ -418,7 +443,33 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     dm = warp_sum(dm, mask, TPT);
     vs = warp_max(vs, mask, TPT);
     if (lane != 0) return;
-    // writeback: preloop zeros + this row's sums; MaxSignalVel floor
+    const double row[kRowSums] = {acc[0], acc[1], acc[2], dtE, dtm, dm, gw[0], gw[1], gw[2], vs, fa[0], fa[1], fa[2]};
+#pragma unroll
+    for (int k = 0; k < kRowSums - 3; k++) sums[k * n + i] = row[k];
+    if (p.diag_flux_abs)
+#pragma unroll
+        for (int k = kRowSums - 3; k < kRowSums; k++) sums[k * n + i] = row[k];
+}
+
+// The writeback of a force row from its sums, one thread per target: the
+// preloop zeros + the row's sums, the MaxSignalVel floor
+// (hydro_force_loop.cc:227-391) and the final operations
+// (hydro_toplevel.cc:133-253). A separate kernel, because in the row kernel
+// only one lane of each row would run it.
+template <typename T>
+__global__ void __launch_bounds__(256) k_force_finish(PassParams p, Particles ps, const int *__restrict__ targets,
+                                                      int n_targets, const double *__restrict__ sums)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= n_targets) return;
+    const int i = targets[slot];
+    const size_t n = (size_t)ps.n;
+    const int mfv = p.method == 1;
+    const double mi = ps.m[i], rhoi = ps.rho[i], hid = ps.h[i];
+    const double acc[3] = {sums[i], sums[n + i], sums[2 * n + i]};
+    const double dtE = sums[3 * n + i], dtm = sums[4 * n + i], dm = sums[5 * n + i];
+    const double gw[3] = {sums[6 * n + i], sums[7 * n + i], sums[8 * n + i]};
+    const double vs = sums[9 * n + i];
     const double cs_i = (rhoi > 0) ? sqrt(p.gamma * ps.pressure[i] / rhoi) : sqrt(p.gamma * (p.gamma - 1.) * ps.u[i]);
     double vsig = kMinReal;
     const double max_sig = fmax(vs, cs_i);
@@ -443,7 +494,9 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
         if (mfv) for (int k = 0; k < 3; k++) g3[k] *= inv;
         if (hid >= 0.99 * p.max_kernel_radius) du = 0;
     }
-    for (int k = 0; k < 3; k++) { ps.accel[k * n + i] = a3[k]; ps.gw[k * n + i] = g3[k]; ps.fabs[k * n + i] = fa[k]; }
+    for (int k = 0; k < 3; k++) { ps.accel[k * n + i] = a3[k]; ps.gw[k * n + i] = g3[k]; }
+    if (p.diag_flux_abs)
+        for (int k = 0; k < 3; k++) ps.fabs[k * n + i] = sums[(10 + k) * n + i];
     ps.dudt[i] = du;
     ps.vsig[i] = vsig;
     ps.dtmass[i] = dtm;
@@ -549,35 +602,43 @@ __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps,
 
 template <typename T, int MODE>
 void launch_force_mode(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                       DevStatus *st, const ForceRec<T> *rec, const PairFlux<T> *flux, cudaStream_t s)
+                       DevStatus *st, const ForceRec<T> *rec, const GatherRec *grec, const PairFlux<T> *flux,
+                       double *sums, cudaStream_t s)
 {
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);
     switch (tpt) {
-        case 4: k_force<T, 4, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
-        case 8: k_force<T, 8, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
-        case 32: k_force<T, 32, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
-        default: k_force<T, 16, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, flux); break;
+        case 1: k_force<T, 1, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, grec, flux, sums); break;
+        case 4: k_force<T, 4, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, grec, flux, sums); break;
+        case 8: k_force<T, 8, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, grec, flux, sums); break;
+        case 32: k_force<T, 32, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, grec, flux, sums); break;
+        default: k_force<T, 16, MODE><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec, grec, flux, sums); break;
     }
+    k_force_finish<T><<<(unsigned)((n_targets + 255) / 256), 256, 0, s>>>(p, ps, targets, n_targets, sums);
 }
 
 // `flux` (one PairFlux<T> per row entry) given: every particle is a target
 // (targets[s] = s) and each pair is evaluated once; otherwise (NULL) each row
-// evaluates all its pairs.
+// evaluates all its pairs. `sums`: kRowSums x n doubles of scratch.
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, void *recbuf, void *fluxbuf, cudaStream_t s)
+                  DevStatus *st, void *recbuf, void *fluxbuf, double *sums, cudaStream_t s)
 {
     if (n_targets <= 0) return;
+    // the record scratch holds the force records, then the gather records
     ForceRec<T> *rec = (ForceRec<T> *)recbuf;
-    k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec);
+    GatherRec *grec = (GatherRec *)(rec + ps.n);
+    k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec, grec);
     if (fluxbuf) {
         PairFlux<T> *flux = (PairFlux<T> *)fluxbuf;
         const long long warps = (n_targets + kPairRows - 1) / kPairRows;
         k_force_pairs<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, n_targets, rows, st, rec, flux);
-        launch_force_mode<T, kGather>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, s);
+        // one thread per row: the gather's per-entry work is short, and lanes
+        // sharing a row would spend more on the cross-lane reduction and on
+        // idling at the row's end than on the entries themselves
+        launch_force_mode<T, kGather>(p, ps, targets, n_targets, rows, 1, st, rec, grec, flux, sums, s);
     } else {
-        launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, nullptr, s);
+        launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, grec, nullptr, sums, s);
     }
 }
 

@@ -6,7 +6,10 @@
 namespace gz {
 
 size_t gradient_record_bytes(int mixed) { return mixed ? sizeof(GradRec<float>) : sizeof(GradRec<double>); }
-size_t force_record_bytes(int mixed) { return mixed ? sizeof(ForceRec<float>) : sizeof(ForceRec<double>); }
+size_t force_record_bytes(int mixed)
+{
+    return (mixed ? sizeof(ForceRec<float>) : sizeof(ForceRec<double>)) + sizeof(GatherRec);
+}
 size_t pair_flux_bytes(int mixed) { return mixed ? sizeof(PairFlux<float>) : sizeof(PairFlux<double>); }
 
 __global__ void k_pack_density(Particles ps, DensRec *rec)
@@ -36,9 +39,9 @@ void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, cudaStream_t s)
+                DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, s);
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, s);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's

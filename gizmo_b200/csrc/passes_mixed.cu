@@ -23,9 +23,9 @@ void gradients_mixed(const PassParams &p, const Particles &ps, const int *target
 }
 
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, cudaStream_t s)
+                 DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s)
 {
-    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, s);
+    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, s);
 }
 
 }  // namespace gz

@@ -158,6 +158,7 @@ struct DensityScratch {
 struct PassParams {
     int kernel, method, first_step, selfgravity_off;
     double box, half, gamma, des_num_ngb, max_num_ngb_dev, min_kernel_radius, max_kernel_radius;
+    int diag_flux_abs;  // the force pass also sums |pair flux| per row (a diagnostic)
 };
 
 // DensitySpec::after_iter_body for gas (density_loop.h:515-961). acc[14]:

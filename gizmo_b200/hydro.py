@@ -78,6 +78,11 @@ class HydroPass:
         self._check(self.lib.gz_set_params(self._ctx, C.byref(params)))
         self.params = params
 
+    def set_diagnostics(self, flux_abs: bool = False):
+        """Diagnostics of the force pass beyond the reference's outputs (off by
+        default): flux_abs, the per-row sums of |pair flux|."""
+        self._check(self.lib.gz_set_diagnostics(self._ctx, abi.DIAG_FLUX_ABS if flux_abs else 0))
+
     @property
     def stream(self) -> int:
         return int(self.lib.gz_stream(self._ctx) or 0)

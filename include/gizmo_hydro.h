@@ -111,7 +111,7 @@ typedef struct gz_outputs {
     double *dmass;     /* [n]    CellP.dMass (MFV) */
     double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
     int    *iters;     /* [n]    density iterations taken */
-    double *flux_abs;  /* [n][3] diagnostic, no reference counterpart: the sums over the
+    double *flux_abs;  /* [n][3] diagnostic (GZ_DIAG_FLUX_ABS), no reference counterpart: the sums over the
                           force row of |mass flux|, |momentum flux| and |energy flux| of
                           the pairs, the scale against which the cancelling sums dtmass,
                           mass * accel and mass * dudt are accurate */
@@ -136,6 +136,13 @@ int gz_create(const gz_params *params, int device, gz_context **out);
 int gz_destroy(gz_context *ctx);
 /* Replace the run-time configuration (keeps particle data). */
 int gz_set_params(gz_context *ctx, const gz_params *params);
+
+/* Diagnostics the force pass computes besides the reference's outputs (no
+ * reference counterpart). GZ_DIAG_FLUX_ABS: the flux_abs sums of gz_outputs.
+ * Off by default, so that the pass pays for none; gz_download of flux_abs
+ * returns GZ_ERR_ORDER unless the last force pass ran with it on. */
+#define GZ_DIAG_FLUX_ABS 1
+int gz_set_diagnostics(gz_context *ctx, int flags);
 
 /* Copy inputs host -> device, sort the particles by Morton key, build the
  * octree and the sorted particle mirror. Replaces the arena acquire of

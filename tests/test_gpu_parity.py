@@ -283,7 +283,16 @@ def test_flux_scale_bounds_the_rates(precision):
     with HydroPass(wl.params) as hp:
         hp.upload_workload(wl)
         hp.full_pass()
+        with pytest.raises(GizmoHydroError) as e:  # off by default: nothing to download
+            hp.download(["flux_abs"])
+        assert e.value.code == abi.ERR_ORDER
+        plain = hp.download(["accel", "dudt", "dtmass"])
+        hp.set_diagnostics(flux_abs=True)
+        hp.restage()
+        hp.full_pass()
         out = hp.download(["accel", "dudt", "dtmass", "flux_abs"])
+    for k in plain:  # the diagnostic changes none of the pass's outputs
+        assert np.array_equal(plain[k], out[k]), k
     fa = out["flux_abs"]
     assert (fa >= 0).all() and (fa[:, 1] > 0).mean() > 0.99
     slack = 1 + 1e-6
