@@ -86,12 +86,14 @@ namespace {
 
 // Lanes per row of the density and gradient row kernels. Fewer lanes per row
 // mean more rows in flight per warp and a shorter cross-lane reduction, but
-// fewer threads: 4 lanes while the rows still give about eight waves of
-// resident threads (2048 per multiprocessor), 8 or 16 for shorter lists.
-int lanes_per_row(const gz_context *c, long long rows)
+// fewer threads: the fewest lanes (at least `min_lanes`) with which the rows
+// still give about eight waves of resident threads (2048 per multiprocessor),
+// at most 16. The density rows keep at least 4 lanes: their pair work is long
+// and the lanes of a row share its loads.
+int lanes_per_row(const gz_context *c, long long rows, int min_lanes)
 {
     const long long want = (long long)c->sms * 2048 * 8;
-    int tpt = 4;
+    int tpt = min_lanes;
     while (tpt < 16 && rows * tpt < want) tpt *= 2;
     return tpt;
 }
@@ -857,8 +859,8 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         w.rebuild = ptr<int>(c->flag);
         w.iter = iter;
         GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
-        if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
-        else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
+        if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
+        else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
         density_after_iter(c->pp, ps, w, ptr<DevStatus>(c->status), s);
         c->launches += 2;
         GZ_CUDA(c, cudaGetLastError());
@@ -912,8 +914,8 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
-    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na), c->rec.p, c->stream);
-    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na), c->rec.p, c->stream);
+    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, c->stream);
+    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, c->stream);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -1120,8 +1122,8 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     w.rec = ptr<DensRec>(c->rec);
     density_pack(ps, ptr<DensRec>(c->rec), s);
     w.acc = ptr<double>(c->acc);
-    if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
-    else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo), s);
+    if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
+    else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
     GZ_CUDA(c, cudaGetLastError());
     const int n = c->n;
     std::vector<double> a17((size_t)17 * (size_t)std::max(n, 1));

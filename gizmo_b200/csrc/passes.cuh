@@ -244,6 +244,8 @@ void launch_gradients(const PassParams &p, const Particles &ps, const int *targe
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);  // 128-thread blocks: finer register granularity
     switch (tpt) {
+        case 1: k_gradients<T, 1><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
+        case 2: k_gradients<T, 2><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
         case 4: k_gradients<T, 4><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
         case 8: k_gradients<T, 8><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
         case 32: k_gradients<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
