@@ -38,9 +38,18 @@ METRIC = "hydro particle-updates/s @256^3: mixed-prec vs FP64 GPU at <=1e-5 rel 
 UNIT = "particle-updates/s"
 
 # per-pair FLOP constants (FMA = 2, sqrt/div/exp/log = 1 each), counted by hand
-# over the taken MFV/MFM ideal-gas branch of the pair bodies (HLLC solved on the
-# first try): density ~40, gradient ~60, force ~430.
-FLOPS_PER_PAIR = {"density": 40.0, "gradients": 60.0, "force": 430.0}
+# over the taken MFV ideal-gas branch of the pair bodies (HLLC solved on the
+# first try). Density, per accepted pair: separation 8, sqrt 1, u 1, cubic
+# kernel and derivative 10, the 17 sums 52 -> 72. Gradient ~60, force ~430.
+FLOPS_PER_PAIR = {"density": 72.0, "gradients": 60.0, "force": 430.0}
+
+# DRAM bytes per work unit of a kernel from one ncu capture of the 64^3 case
+# (dram__bytes_read.sum + dram__bytes_write.sum over the units of the captured
+# launch), scaled to the units of a launch here: density sums per row
+# (profiles/density_sums_plummer64.md: 140.7 MB over 262,144 rows), the force
+# pair kernel per pair (profiles/force_pairs_plummer64.md: 1108 MB over
+# 7,841,073 pairs).
+DRAM_BYTES_PER_UNIT = {"density_sums": 140.7e6 / 262144, "force": 1108.0e6 / 7841073}
 
 
 def parse_args():
@@ -230,6 +239,8 @@ def run_ours(args, world, rank, local):
         dist_barrier(world)
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if record_clock else None
+        if record_clock:
+            hp.kernel_timing(True)
         l0 = hp.status()["kernel_launches"]
         ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
         for k in range(K):
@@ -247,15 +258,19 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         launches = hp.status()["kernel_launches"] - l0
+        ktimes = None
+        if record_clock:
+            ktimes = hp.kernel_times()
+            hp.kernel_timing(False)
         total = ev[0][0].elapsed_time(ev[K - 1][4]) / 1e3
         parts = {nm: float(np.mean([ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(K)])) / 1e3
                  for i, nm in enumerate(["grid", "density", "gradients", "force"])}
-        return total, parts, clocks, launches
+        return total, parts, clocks, launches, ktimes
 
     K, W = args.steps, args.warmup
-    t_mix, parts_mix, clocks, launches = run_steps(hpm, K, W, record_clock=True)
+    t_mix, parts_mix, clocks, launches, ktimes = run_steps(hpm, K, W, record_clock=True)
     st_mix = hpm.status()
-    t_64, parts_64, _, _ = run_steps(hp64, max(1, min(K, 3)), max(1, min(W, 2)))
+    t_64, parts_64, _, _, _ = run_steps(hp64, max(1, min(K, 3)), max(1, min(W, 2)))
     K64 = max(1, min(K, 3))
     t_mix = dist_max(t_mix, world, "ours")
     t_64 = dist_max(t_64, world, "ours")
@@ -317,10 +332,13 @@ def run_ours(args, world, rank, local):
         cons[tag] = {"momentum": float(np.abs(mom.sum(0)).max() / np.abs(mom).sum()),
                      "mass": float(abs(dtm.sum()) / (np.abs(dtm).sum() + 1e-300))}
 
-    # roofline of the dominant kernel (force): algorithmic FLOPs / event time
+    # Roofline of each timed kernel family (CUDA events around its launches on
+    # the context's stream, over the timed steps of the mixed form): algorithmic
+    # FLOPs / kernel time against the nominal rate of the pipe its arithmetic
+    # runs on. None of these kernels is a contraction (no tensor cores) or
+    # DRAM-bound (the gathers hit L1/L2: see `traffic`); MEASURED_PEAKS.json
+    # holds no FP32/FP64 vector figure, so the peaks are nominal.
     pairs_sym = st_mix["pairs_symmetric"]
-    t_force = parts_mix["force"]
-    achieved = FLOPS_PER_PAIR["force"] * pairs_sym / t_force / 1e12
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -328,6 +346,44 @@ def run_ours(args, world, rank, local):
         pass
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp64_peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+    kernels = {}
+    for name, d in (ktimes or {}).items():
+        if d["launches"] == 0 or d["ms"] <= 0:
+            continue
+        e = {"launches_per_step": d["launches"] / K, "ms_per_step": d["ms"] / K,
+             "ms_per_launch": d["ms"] / d["launches"], "units_per_launch": d["units"] / d["launches"]}
+        flops = None
+        if name == "density_sums":  # FP64; a converged row holds ~DesNumNgb accepted pairs
+            flops, peak, pipe = FLOPS_PER_PAIR["density"] * p.des_num_ngb * d["units"], fp64_peak, "fp64"
+            e["work"] = f"{FLOPS_PER_PAIR['density']:.0f} flop x DesNumNgb ({p.des_num_ngb:.0f}) pairs per row"
+        elif name == "force":  # FP32 pair arithmetic, each pair evaluated once
+            flops, peak, pipe = FLOPS_PER_PAIR["force"] * d["units"], fp32_peak, "fp32"
+            e["work"] = f"{FLOPS_PER_PAIR['force']:.0f} flop per pair evaluation"
+        elif name == "gradients":  # FP32 pair arithmetic over every row entry
+            flops, peak, pipe = FLOPS_PER_PAIR["gradients"] * pairs_sym * d["launches"], fp32_peak, "fp32"
+            e["work"] = f"{FLOPS_PER_PAIR['gradients']:.0f} flop per row entry"
+        if flops is not None:
+            ach = flops / (d["ms"] / 1e3) / 1e12
+            e.update({"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "pipe": pipe})
+        if name in DRAM_BYTES_PER_UNIT:
+            e["traffic_bytes_per_launch"] = DRAM_BYTES_PER_UNIT[name] * e["units_per_launch"]
+        kernels[name] = e
+    dom = max((k for k in kernels if "achieved" in kernels[k]), key=lambda k: kernels[k]["ms_per_step"], default=None)
+    kernel_names = {"density_sums": "k_density_sums<double> (FP64 density sums, all h iterations)",
+                    "force": "k_force_pairs<float> (MFV pair flux, each pair once)",
+                    "gradients": "k_gradients<float> (least-squares gradients)"}
+    roofline = None
+    if dom:
+        d = kernels[dom]
+        roofline = {"kernel": kernel_names[dom], "bound": d["pipe"], "achieved": d["achieved"], "peak": d["peak"],
+                    "unit": "TFLOP/s", "frac": d["frac"], "work": d["work"],
+                    "ms_per_launch": d["ms_per_launch"], "launches_per_step": d["launches_per_step"],
+                    "peak_source": f"nominal {d['pipe'].upper()} pipe: 148 SM x {128 if d['pipe'] == 'fp32' else 64} "
+                                   f"lanes x 2 x {sm_mhz:.0f} MHz (no measured FP32/FP64 figure in "
+                                   "MEASURED_PEAKS.json; the kernels use no tensor cores)",
+                    "traffic": d.get("traffic_bytes_per_launch"),
+                    "traffic_source": "ncu DRAM bytes per unit of the 64^3 capture, scaled to this launch's units"}
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": 1e3 * t_mix / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -341,11 +397,7 @@ def run_ours(args, world, rank, local):
         "accuracy_mixed_vs_fp64": acc, "conservation": cons,
         "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
         "gpu_launches": launches, "clocks": clocks,
-        "roofline": {"kernel": "k_force<float> (MFV pair flux)", "bound": "fp32",
-                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "peak_source": f"nominal FP32 pipe: 148 SM x 128 lanes x 2 x {sm_mhz:.0f} MHz "
-                                    "(no measured FP32 figure in MEASURED_PEAKS.json)",
-                     "flops_per_pair": FLOPS_PER_PAIR["force"], "traffic": None},
+        "roofline": roofline, "kernels": kernels,
     }
 
     # end to end: pinned host buffers in, results out, every step

@@ -93,11 +93,13 @@ class GzStatusInfo(C.Structure):
 
 EXPORTED_SYMBOLS = [
     "gz_create", "gz_destroy", "gz_set_params", "gz_set_diagnostics", "gz_upload", "gz_restage", "gz_hydro_density",
-    "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream",
+    "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream", "gz_kernel_timing",
+    "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc",
 ]
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS
+TIMERS = {"density_sums": 0, "walk": 1, "gradients": 2, "force": 3}  # GZ_TIMER_*
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libgizmo_hydro.so")
@@ -121,6 +123,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_destroy.argtypes = [vp]
     lib.gz_set_params.argtypes = [vp, C.POINTER(GzParams)]
     lib.gz_set_diagnostics.argtypes = [vp, C.c_int]
+    lib.gz_kernel_timing.argtypes = [vp, C.c_int]
+    lib.gz_kernel_time.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
     lib.gz_restage.argtypes = [vp]
     for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):

@@ -78,6 +78,12 @@ struct gz_context {
     bool have_density = false, have_gradients = false;
     int tpt_force = 8;               // lanes per force row (fixed: measured best at every size)
     int diag = 0;                    // GZ_DIAG_* flags
+    bool timing = false;             // gz_kernel_timing on
+    struct Timer {
+        std::vector<EventPair> ev;   // event pairs, one per timed launch since the last read
+        size_t used = 0;
+        long long units = 0;
+    } timers[GZ_TIMERS];
     bool fabs_valid = false;         // the last force pass summed flux_abs
     int sms = 148;                   // multiprocessors of the device
 };
@@ -96,6 +102,37 @@ int lanes_per_row(const gz_context *c, long long rows, int min_lanes)
     int tpt = min_lanes;
     while (tpt < 16 && rows * tpt < want) tpt *= 2;
     return tpt;
+}
+
+// The event pair for one launch of timer `id` (null when timing is off, or
+// when no event could be had: that launch then goes untimed).
+const EventPair *timer_launch(gz_context *c, int id, long long units)
+{
+    if (!c->timing) return nullptr;
+    gz_context::Timer &t = c->timers[id];
+    if (t.used == t.ev.size()) {
+        EventPair e{nullptr, nullptr};
+        if (cudaEventCreate(&e.start) != cudaSuccess) return nullptr;
+        if (cudaEventCreate(&e.stop) != cudaSuccess) { cudaEventDestroy(e.start); return nullptr; }
+        t.ev.push_back(e);
+    }
+    t.units += units;
+    return &t.ev[t.used++];
+}
+
+// record the start / stop of a launch timed from here
+void ev_start(const EventPair *e, cudaStream_t s) { if (e) cudaEventRecord(e->start, s); }
+void ev_stop(const EventPair *e, cudaStream_t s) { if (e) cudaEventRecord(e->stop, s); }
+
+// walk_rows, timed under GZ_TIMER_WALK
+void walk_timed(gz_context *c, const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
+                const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
+{
+    const EventPair *ev = n_targets > 0 ? timer_launch(c, GZ_TIMER_WALK, n_targets) : nullptr;
+    ev_start(ev, s);
+    walk_rows(t, x, y, z, reach, hsym, symmetric, targets, n_targets, counts, off, nbr, cap, st, next_group, s);
+    ev_stop(ev, s);
 }
 
 int fail(gz_context *c, int code, const char *what)
@@ -399,14 +436,14 @@ int build_rows(gz_context *c, const double *reach, int symmetric, const int *tar
     Tree t = tree_view(c);
     if (ensure(c, counts, sizeof(long long) * (size_t)std::max(rows, 1)) || ensure(c, c->work, sizeof(int)))
         return c->err;
-    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+    walk_timed(c, t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
               rows, ptr<long long>(counts), nullptr, nullptr, 0, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (exclusive_scan_counts(c, rows, counts, off, total)) return c->err;
     if (base + *total > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
     if (grow_keep(c, nbr, cap, base, base + *total)) return c->err;
-    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
+    walk_timed(c, t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), symmetric, targets,
               rows, ptr<long long>(counts), ptr<long long>(off), ptr<int>(nbr) + base, 0, ptr<DevStatus>(c->status),
               ptr<int>(c->work), s);
     if (rows > 0) c->launches++;
@@ -430,7 +467,7 @@ int build_rows_padded(gz_context *c, const double *reach, const int *targets, in
         ensure(c, c->pad_over, R) || ensure(c, c->pad_list, sizeof(int) * R) || ensure(c, c->n_sel, sizeof(int) * 2))
         return c->err;
     Tree t = tree_view(c);
-    walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0, targets, rows,
+    walk_timed(c, t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0, targets, rows,
               ptr<long long>(c->counts), nullptr, ptr<int>(c->d_nbr) + base, cap, ptr<DevStatus>(c->status),
               ptr<int>(c->work), s);
     padded_rows(rows, targets, ptr<long long>(c->counts), cap, base, ptr<long long>(c->d_beg), ptr<long long>(c->d_end),
@@ -465,7 +502,7 @@ int build_rows_padded(gz_context *c, const double *reach, const int *targets, in
         if (exclusive_scan_counts(c, n_over, c->pad_counts, c->d_off, &extra)) return c->err;
         if (need + extra > (long long)INT32_MAX * 4) return fail(c, GZ_ERR_CAPACITY, "neighbour rows exceed capacity");
         if (grow_keep(c, c->d_nbr, c->d_nbr_cap, need, need + extra)) return c->err;
-        walk_rows(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0,
+        walk_timed(c, t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), reach, ptr<double>(c->h), 0,
                   ptr<int>(c->pad_list), n_over, ptr<long long>(c->pad_counts), ptr<long long>(c->d_off),
                   ptr<int>(c->d_nbr) + need, 0, ptr<DevStatus>(c->status), ptr<int>(c->work), s);
         k_set_rows<<<(n_over + 255) / 256, 256, 0, s>>>(n_over, ptr<int>(c->pad_list), ptr<long long>(c->d_off), need,
@@ -672,6 +709,8 @@ int gz_destroy(gz_context *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (DevBuf *b : all_buffers(c)) release(*b);
+    for (auto &t : c->timers)
+        for (auto &e : t.ev) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
     cudaStreamDestroy(c->stream);
     delete c;
     return GZ_OK;
@@ -697,6 +736,34 @@ int gz_set_diagnostics(gz_context *c, int flags)
 }
 
 void *gz_stream(gz_context *c) { return c ? (void *)c->stream : nullptr; }
+
+int gz_kernel_timing(gz_context *c, int enable)
+{
+    if (!c) return GZ_ERR_ARG;
+    c->timing = enable != 0;
+    for (auto &t : c->timers) { t.used = 0; t.units = 0; }
+    return GZ_OK;
+}
+
+int gz_kernel_time(gz_context *c, int timer, double *ms, int64_t *launches, int64_t *units)
+{
+    if (!c || timer < 0 || timer >= GZ_TIMERS) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    GZ_CUDA(c, cudaStreamSynchronize(c->stream));
+    gz_context::Timer &t = c->timers[timer];
+    double total = 0;
+    for (size_t k = 0; k < t.used; k++) {
+        float m = 0;
+        GZ_CUDA(c, cudaEventElapsedTime(&m, t.ev[k].start, t.ev[k].stop));
+        total += m;
+    }
+    if (ms) *ms = total;
+    if (launches) *launches = (int64_t)t.used;
+    if (units) *units = t.units;
+    t.used = 0;
+    t.units = 0;
+    return GZ_OK;
+}
 
 // Rebuild the sorted mirror and the octree from the resident inputs (the
 // state a pass starts from): Morton keys, radix sort, gathers, zeroed
@@ -859,8 +926,11 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         w.rebuild = ptr<int>(c->flag);
         w.iter = iter;
         GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
+        const EventPair *ev = timer_launch(c, GZ_TIMER_DENSITY_SUMS, w.n_todo);
+        ev_start(ev, s);
         if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
         else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
+        ev_stop(ev, s);
         density_after_iter(c->pp, ps, w, ptr<DevStatus>(c->status), s);
         c->launches += 2;
         GZ_CUDA(c, cudaGetLastError());
@@ -914,8 +984,11 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
-    if (c->prm.precision == GZ_PRECISION_MIXED) gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, c->stream);
-    else gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, c->stream);
+    const EventPair *ev = na > 0 ? timer_launch(c, GZ_TIMER_GRADIENTS, na) : nullptr;
+    if (c->prm.precision == GZ_PRECISION_MIXED)
+        gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
+    else
+        gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -954,12 +1027,14 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
         flux = c->pflux.p;
     // the rows' sums before the writeback go to the density accumulators
     // (17 x n doubles, unused between density passes)
+    const EventPair *ev = na > 0 ? timer_launch(c, GZ_TIMER_FORCE, flux ? c->pairs_symmetric / 2 : c->pairs_symmetric)
+                                 : nullptr;
     if (mixed)
         force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                    ptr<double>(c->acc), c->stream);
+                    ptr<double>(c->acc), ev, c->stream);
     else
         force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                   ptr<double>(c->acc), c->stream);
+                   ptr<double>(c->acc), ev, c->stream);
     if (na > 0) c->launches += flux ? 4 : 3;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -1122,8 +1197,11 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     w.rec = ptr<DensRec>(c->rec);
     density_pack(ps, ptr<DensRec>(c->rec), s);
     w.acc = ptr<double>(c->acc);
+    const EventPair *ev = timer_launch(c, GZ_TIMER_DENSITY_SUMS, w.n_todo);
+    ev_start(ev, s);
     if (c->prm.precision == GZ_PRECISION_MIXED) density_sums_mixed(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
     else density_sums_fp64(c->pp, ps, w, lanes_per_row(c, w.n_todo, 4), s);
+    ev_stop(ev, s);
     GZ_CUDA(c, cudaGetLastError());
     const int n = c->n;
     std::vector<double> a17((size_t)17 * (size_t)std::max(n, 1));

@@ -64,16 +64,16 @@ size_t gradient_record_bytes(int mixed);
 size_t force_record_bytes(int mixed);  // the force record and the gather record of a particle
 size_t pair_flux_bytes(int mixed);  // per symmetric row entry, for a force pass evaluating each pair once
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                    void *rec, cudaStream_t s);
+                    void *rec, const EventPair *ev, cudaStream_t s);
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     void *rec, cudaStream_t s);
+                     void *rec, const EventPair *ev, cudaStream_t s);
 // flux: NULL, or (every particle a target, targets[s] = s) scratch for one
 // evaluation per pair: n_entries x pair_flux_bytes. sums: 13 x n doubles of
 // scratch (the row sums before the writeback).
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s);
+                DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s);
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s);
+                 DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s);
 void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
 
 }  // namespace gz

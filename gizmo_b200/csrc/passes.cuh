@@ -236,13 +236,14 @@ __global__ void __launch_bounds__(128, 5) k_gradients(PassParams p, Particles ps
 
 template <typename T>
 void launch_gradients(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                      void *recbuf, cudaStream_t s)
+                      void *recbuf, const EventPair *ev, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     GradRec<T> *rec = (GradRec<T> *)recbuf;
     k_pack_gradient<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);  // 128-thread blocks: finer register granularity
+    if (ev) cudaEventRecord(ev->start, s);
     switch (tpt) {
         case 1: k_gradients<T, 1><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
         case 2: k_gradients<T, 2><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
@@ -251,6 +252,7 @@ void launch_gradients(const PassParams &p, const Particles &ps, const int *targe
         case 32: k_gradients<T, 32><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
         default: k_gradients<T, 16><<<blocks, 128, 0, s>>>(p, ps, targets, n_targets, rows, rec); break;
     }
+    if (ev) cudaEventRecord(ev->stop, s);
 }
 
 // ------------------------------------------------------------------ force
@@ -624,7 +626,7 @@ void launch_force_mode(const PassParams &p, const Particles &ps, const int *targ
 // evaluates all its pairs. `sums`: kRowSums x n doubles of scratch.
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, void *recbuf, void *fluxbuf, double *sums, cudaStream_t s)
+                  DevStatus *st, void *recbuf, void *fluxbuf, double *sums, const EventPair *ev, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     // the record scratch holds the force records, then the gather records
@@ -634,13 +636,17 @@ void launch_force(const PassParams &p, const Particles &ps, const int *targets, 
     if (fluxbuf) {
         PairFlux<T> *flux = (PairFlux<T> *)fluxbuf;
         const long long warps = (n_targets + kPairRows - 1) / kPairRows;
+        if (ev) cudaEventRecord(ev->start, s);
         k_force_pairs<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, n_targets, rows, st, rec, flux);
+        if (ev) cudaEventRecord(ev->stop, s);
         // one thread per row: the gather's per-entry work is short, and lanes
         // sharing a row would spend more on the cross-lane reduction and on
         // idling at the row's end than on the entries themselves
         launch_force_mode<T, kGather>(p, ps, targets, n_targets, rows, 1, st, rec, grec, flux, sums, s);
     } else {
+        if (ev) cudaEventRecord(ev->start, s);  // (also spans the writeback kernel)
         launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, grec, nullptr, sums, s);
+        if (ev) cudaEventRecord(ev->stop, s);
     }
 }
 

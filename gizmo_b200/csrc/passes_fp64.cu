@@ -33,15 +33,15 @@ void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWo
 }
 
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                    void *rec, cudaStream_t s)
+                    void *rec, const EventPair *ev, cudaStream_t s)
 {
-    launch_gradients<double>(p, ps, targets, n_targets, rows, tpt, rec, s);
+    launch_gradients<double>(p, ps, targets, n_targets, rows, tpt, rec, ev, s);
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s)
+                DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, s);
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, ev, s);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's

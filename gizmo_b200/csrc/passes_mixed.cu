@@ -17,15 +17,15 @@ void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityW
 }
 
 void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     void *rec, cudaStream_t s)
+                     void *rec, const EventPair *ev, cudaStream_t s)
 {
-    launch_gradients<float>(p, ps, targets, n_targets, rows, tpt, rec, s);
+    launch_gradients<float>(p, ps, targets, n_targets, rows, tpt, rec, ev, s);
 }
 
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, double *sums, cudaStream_t s)
+                 DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s)
 {
-    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, s);
+    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, ev, s);
 }
 
 }  // namespace gz

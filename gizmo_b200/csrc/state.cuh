@@ -58,6 +58,12 @@ struct __align__(16) DensRec {
 };
 
 // Compressed neighbour rows: row r of `slot_of` targets.
+// CUDA events recorded around one kernel of a pass, for the caller's timing
+// (null: not timed).
+struct EventPair {
+    cudaEvent_t start, stop;
+};
+
 struct Csr {
     const long long *off;           // [rows + 1]
     const int *nbr;                 // sorted particle indices

@@ -83,6 +83,20 @@ class HydroPass:
         default): flux_abs, the per-row sums of |pair flux|."""
         self._check(self.lib.gz_set_diagnostics(self._ctx, abi.DIAG_FLUX_ABS if flux_abs else 0))
 
+    def kernel_timing(self, enable: bool = True):
+        """Start (clearing the totals) or stop CUDA-event timing of the main kernels."""
+        self._check(self.lib.gz_kernel_timing(self._ctx, 1 if enable else 0))
+
+    def kernel_times(self) -> dict:
+        """Per timer since the last read: kernel milliseconds, launches and work
+        units (rows, targets or pair evaluations); clears the totals."""
+        out = {}
+        for name, t in abi.TIMERS.items():
+            ms, nl, un = C.c_double(), C.c_int64(), C.c_int64()
+            self._check(self.lib.gz_kernel_time(self._ctx, t, C.byref(ms), C.byref(nl), C.byref(un)))
+            out[name] = {"ms": ms.value, "launches": nl.value, "units": un.value}
+        return out
+
     @property
     def stream(self) -> int:
         return int(self.lib.gz_stream(self._ctx) or 0)

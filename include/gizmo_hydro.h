@@ -122,7 +122,7 @@ typedef struct gz_status_info {
     int      index;             /* original particle index it refers to, -1 if none */
     int      density_iterations;/* iterations of the last density pass */
     int      reserved;
-    int64_t  pairs_density;     /* accepted one-way pairs summed over iterations */
+    int64_t  pairs_density;     /* density-row entries built (candidates within the row radii) */
     int64_t  pairs_symmetric;   /* symmetric pairs (rows of the gradient/force lists) */
     int64_t  device_bytes;      /* device memory held by the context */
     int64_t  kernel_launches;   /* kernels of this library launched by the context so far */
@@ -173,6 +173,22 @@ int gz_status(gz_context *ctx, gz_status_info *info);
 /* CUDA stream of the context (cudaStream_t), for callers that time or
  * order work around the passes. */
 void *gz_stream(gz_context *ctx);
+
+/* CUDA-event timing of the passes' main kernels on the context's stream (no
+ * reference counterpart: a measurement aid). gz_kernel_timing(ctx, 1) starts
+ * recording and clears the totals, 0 stops it. gz_kernel_time synchronises the
+ * stream and returns, for one timer, the summed kernel time in milliseconds,
+ * the launches and the work units since the last clear, then clears them.
+ * Units: GZ_TIMER_DENSITY_SUMS rows summed; GZ_TIMER_WALK targets walked;
+ * GZ_TIMER_GRADIENTS rows; GZ_TIMER_FORCE pair evaluations (each pair once in
+ * a pass over every particle, otherwise every row entry). */
+#define GZ_TIMER_DENSITY_SUMS 0
+#define GZ_TIMER_WALK         1
+#define GZ_TIMER_GRADIENTS    2
+#define GZ_TIMER_FORCE        3
+#define GZ_TIMERS             4
+int gz_kernel_timing(gz_context *ctx, int enable);
+int gz_kernel_time(gz_context *ctx, int timer, double *ms, int64_t *launches, int64_t *units);
 
 /* Exact neighbour sets of the last pass, for bit-exact checks against a CPU
  * search. mode 0: one-way r < h_i at the converged h; mode 1: symmetric
