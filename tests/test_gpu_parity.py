@@ -300,3 +300,24 @@ def test_flux_scale_bounds_the_rates(precision):
     vmag = np.linalg.norm(wl.vel, axis=1)
     net_mom = np.linalg.norm(wl.mass[:, None] * out["accel"] + wl.vel * out["dtmass"][:, None], axis=1)
     assert (net_mom <= fa[:, 1] * slack + 1e-300).all()
+
+
+def test_kernel_timers_count_the_pass():
+    """gz_kernel_timing / gz_kernel_time: every timed family launched in a full
+    pass reports positive time and its work units (the force pass over every
+    particle evaluates each symmetric pair once); reading clears the totals."""
+    wl = CASES["plummer16"](abi.PRECISION_MIXED)
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.kernel_timing(True)
+        hp.full_pass()
+        t = hp.kernel_times()
+        st = hp.status()
+        again = hp.kernel_times()
+        hp.kernel_timing(False)
+    for name in ("density_sums", "walk", "gradients", "force"):
+        assert t[name]["launches"] > 0 and t[name]["ms"] > 0, name
+    assert t["density_sums"]["launches"] == st["density_iterations"]
+    assert t["gradients"]["units"] == wl.n
+    assert t["force"]["units"] == st["pairs_symmetric"] // 2
+    assert all(v["launches"] == 0 and v["units"] == 0 for v in again.values())
