@@ -81,9 +81,18 @@ __global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p,
     };
     // one record in flight per lane: the register budget goes to resident
     // warps (six 128-thread blocks per multiprocessor), which hide the
-    // gather latency better than a second record per lane does
+    // gather latency better than a second record per lane does; the next
+    // entry's index is loaded a step ahead, so the record load does not wait
+    // on it
     const long long b0 = w.beg[t], b1 = w.end[t];
-    for (long long e = b0 + lane; e < b1; e += TPT) pair(w.rec[w.nbr[e]]);
+    long long e = b0 + lane;
+    int j = e < b1 ? w.nbr[e] : 0;
+    for (; e < b1; e += TPT) {
+        const long long en = e + TPT;
+        const int jn = en < b1 ? w.nbr[en] : 0;
+        pair(w.rec[j]);
+        j = jn;
+    }
 #pragma unroll
     for (int k = 0; k < 17; k++) a[k] = warp_sum(a[k], mask, TPT);
     if (lane == 0) {

@@ -754,7 +754,9 @@ template <typename T> struct Side {
 };
 
 // Result of one canonical pair evaluation, i = the "local" (R) side.
-template <typename T> struct PairFlux {
+// (16-byte aligned: 32 bytes in FP32, 64 in FP64, so that a stored flux
+// fills whole sectors)
+template <typename T> struct __align__(16) PairFlux {
     T rho, p, v[3];  // Fluxes.{rho,p,v} after face-area scaling and the MFM switch
     T vsig_ts;       // vsig + |c_i - c_j|, for MaxSignalVel
     int valid;       // inside support (r < max(h_i,h_j), r > 0, j has mass/density)
