@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(256) k_sym_sort(int n, const long long *__rest
 void sym_split(int n, const double *x, const double *y, const double *z, const double *h, double box,
                const long long *beg, const long long *end, int *nbr, int *acnt, int *bcnt, cudaStream_t s)
 {
-    if (n > 0) k_sym_split<16><<<(unsigned)(((long long)n * 16 + 255) / 256), 256, 0, s>>>(n, x, y, z, h, box, beg, end, nbr, acnt, bcnt);
+    if (n > 0) k_sym_split<8><<<(unsigned)(((long long)n * 8 + 255) / 256), 256, 0, s>>>(n, x, y, z, h, box, beg, end, nbr, acnt, bcnt);
 }
 
 void sym_counts(int n, const int *acnt, const int *bcnt, long long *cnt, cudaStream_t s)
@@ -515,7 +515,7 @@ void sym_counts(int n, const int *acnt, const int *bcnt, long long *cnt, cudaStr
 void sym_scatter(int n, const long long *beg, const int *nbr, const int *acnt, const long long *s_off, int *bcur,
                  int *rows, cudaStream_t s)
 {
-    if (n > 0) k_sym_scatter<16><<<(unsigned)(((long long)n * 16 + 255) / 256), 256, 0, s>>>(n, beg, nbr, acnt, s_off, bcur, rows);
+    if (n > 0) k_sym_scatter<8><<<(unsigned)(((long long)n * 8 + 255) / 256), 256, 0, s>>>(n, beg, nbr, acnt, s_off, bcur, rows);
 }
 
 void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStream_t s)
