@@ -17,7 +17,9 @@
 // lane tests its own target), so 32 targets on both sides of a jump of the
 // Morton curve cost two small searches, not one search of their joint
 // bounding box. Leaf particles are staged through shared memory, and every
-// lane whose sphere reached the leaf tests them. Membership uses the
+// lane whose sphere reached the leaf tests them. Box and candidate tests run
+// in FP32 with outward margins that bound the FP32 rounding; only a candidate
+// within that margin of its sphere takes the FP64 test. Membership is thus the
 // reference predicates on FP64 minimum-image separations rounded exactly as
 // the CPU does, so the rows are bit-identical to an exact CPU search:
 //   one-way   r2 < R_i^2                                (density, R = buffered h)
@@ -184,15 +186,22 @@ __global__ void k_tree_up(int n_nodes, const int4 *__restrict__ node, const int 
 }
 
 // Periodic gap between a point and a box [l, u] on one axis (both inside
-// [0, box)), minus an absolute allowance for the rounding of the subtractions.
-GZ_DEV double axis_gap(double x, double l, double u, double box, double eps)
+// [0, box)) in FP32, minus an allowance `eps` that covers the FP32 rounding of
+// the point, the box (rounded outward) and the subtractions: never larger than
+// the FP64 gap.
+GZ_DEV float axis_gap_f(float x, float l, float u, float box, float eps)
 {
-    double g;
-    if (x < l) g = fmin(l - x, x + box - u);
-    else if (x > u) g = fmin(x - u, l + box - x);
-    else return 0.0;
+    float g;
+    if (x < l) g = fminf(l - x, x + box - u);
+    else if (x > u) g = fminf(x - u, l + box - x);
+    else return 0.0f;
     g -= eps;
-    return g > 0 ? g : 0.0;
+    return g > 0.0f ? g : 0.0f;
+}
+
+GZ_DEV float wrap1f(float d, float box, float half)
+{
+    return (d > half) ? d - box : ((d < -half) ? d + box : d);
 }
 
 constexpr int kStack = 160;  // >= 7 x 22 levels + 8
@@ -205,6 +214,22 @@ struct StackNode {
     unsigned lanes;
 };
 
+// FP32 screening of a candidate at FP32 separation r2f from a target whose
+// search radius is R (FP32, rounded up): 0 = outside, 1 = inside, 2 = too close
+// to the boundary to tell (the FP64 test decides). `scr` bounds the difference
+// between an FP32 separation and the FP64 one: positions lie in [0, box), so
+// each rounding to FP32 and each FP32 subtraction is within 2^-24 box, and
+// three axes of three roundings each stay below 6 x 2^-24 box; scr = 8 x
+// 2^-24 box. With `positive` the pair also needs r > 0 (symmetric rows).
+GZ_DEV int screen(float r2f, float R, float scr, bool positive)
+{
+    const float hi = R + scr;
+    if (r2f > hi * hi) return 0;
+    const float lo = R - scr;
+    if (lo > 0.0f && r2f < lo * lo && (!positive || r2f > 4.0f * scr * scr)) return 1;
+    return 2;
+}
+
 // Warp-cooperative tree walk. FILL=false counts rows; FILL=true writes them.
 //   SOLO=false: the warp's 32 lanes hold 32 consecutive targets; a node is
 //     opened if any lane's sphere reaches it and a leaf particle is tested by
@@ -215,25 +240,32 @@ struct StackNode {
 //     one the other mode writes.
 // Opening a node loads its children's records in one coalesced access
 // (children are contiguous) and tests them there, so only reached children
-// are pushed and a pop costs no memory round trip.
+// are pushed and a pop costs no memory round trip. Box tests and candidate
+// tests run in FP32 with outward margins; a candidate within the margin of
+// its sphere is decided by the exact FP64 predicate, so the rows are those of
+// the FP64 predicates alone.
 template <bool SYM, bool FILL, bool SOLO>
 __device__ __forceinline__ void walk_group(const int group, const Tree &t, const double *__restrict__ x,
                                            const double *__restrict__ y, const double *__restrict__ z,
                                            const double *__restrict__ reach, const double *__restrict__ hsym,
                                            const int *__restrict__ targets, int n_targets, long long *counts,
                                            const long long *__restrict__ off, int *nbr, int cap, DevStatus *st,
-                                           StackNode (*s_stack)[kStack], double4 (*s_c)[32], double4 (*s_lo)[8],
-                                           double4 (*s_hi)[8], int4 (*s_nd)[8])
+                                           StackNode (*s_stack)[kStack], double4 (*s_c)[32], float4 (*s_cf)[32],
+                                           float4 (*s_lo)[8], float4 (*s_hi)[8], int4 (*s_nd)[8])
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned full = 0xffffffffu;
     const int slot = SOLO ? group : group * 32 + lane;
     const bool valid = slot < n_targets;
     const int tg = valid ? targets[slot] : -1;
-    const double box = t.box, half = 0.5 * box, eps = 4e-16 * box;
+    const double box = t.box, half = 0.5 * box;
+    const float boxf = (float)box, halff = 0.5f * boxf;
+    const float scr = 4.77e-7f * boxf;  // 8 x 2^-24 box
     double xi = 0, yi = 0, zi = 0, ri = 0;
     if (valid) { xi = x[tg]; yi = y[tg]; zi = z[tg]; ri = reach[tg]; }
     const double ri2 = ri * ri;
+    const float xf = __double2float_rn(xi), yf = __double2float_rn(yi), zf = __double2float_rn(zi);
+    const float rf = __double2float_ru(ri);
     // a row starts at off[slot] (exact counts known), or, with cap > 0, at
     // slot * cap in a padded layout whose rows keep at most cap entries (the
     // count is still taken in full: a longer row is rebuilt elsewhere)
@@ -241,16 +273,21 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
     if (FILL && valid) base = cap ? (long long)slot * cap : off[slot];
     long long cnt = 0;  // SOLO: the row length so far (uniform); else this lane's
     // does this lane's sphere reach box [l, u] holding h up to l.w?
-    auto reaches = [&](const double4 &l, const double4 &u) -> bool {
-        const double R = SYM ? fmax(ri, l.w) : ri;
-        const double gx = axis_gap(xi, l.x, u.x, box, eps);
-        const double gy = axis_gap(yi, l.y, u.y, box, eps);
-        const double gz = axis_gap(zi, l.z, u.z, box, eps);
-        return valid && (gx * gx + gy * gy + gz * gz <= R * R * (1.0 + 1e-9));
+    auto reaches = [&](const float4 &l, const float4 &u) -> bool {
+        const float R = (SYM ? fmaxf(rf, l.w) : rf) + scr;
+        const float gx = axis_gap_f(xf, l.x, u.x, boxf, scr);
+        const float gy = axis_gap_f(yf, l.y, u.y, boxf, scr);
+        const float gz = axis_gap_f(zf, l.z, u.z, boxf, scr);
+        return valid && (gx * gx + gy * gy + gz * gz <= R * R * 1.00001f);
+    };
+    auto outward = [](const double4 &l, const double4 &u, float4 &fl, float4 &fu) {
+        fl = make_float4(__double2float_rd(l.x), __double2float_rd(l.y), __double2float_rd(l.z), __double2float_ru(l.w));
+        fu = make_float4(__double2float_ru(u.x), __double2float_ru(u.y), __double2float_ru(u.z), 0.0f);
     };
     int sp = 0;
     {
-        const double4 l = t.lo[0], u = t.hi[0];
+        float4 l, u;
+        outward(t.lo[0], t.hi[0], l, u);
         const unsigned m = __ballot_sync(full, reaches(l, u));
         if (m) {
             if (lane == 0) {
@@ -272,16 +309,21 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
             for (int c0 = a; c0 < b; c0 += 32) {
                 const int jl = c0 + lane;
                 if (SOLO) {
-                    bool acc = false;
+                    double cx = 0, cy = 0, cz = 0, hj = 0;
+                    int sc = 0;
                     if (jl < b) {
+                        cx = x[jl]; cy = y[jl]; cz = z[jl];
+                        if (SYM) hj = hsym[jl];
+                        const float dx = wrap1f(xf - __double2float_rn(cx), boxf, halff);
+                        const float dy = wrap1f(yf - __double2float_rn(cy), boxf, halff);
+                        const float dz = wrap1f(zf - __double2float_rn(cz), boxf, halff);
+                        sc = screen(dx * dx + dy * dy + dz * dz, SYM ? fmaxf(rf, __double2float_ru(hj)) : rf, scr, SYM);
+                    }
+                    bool acc = sc == 1;
+                    if (sc == 2) {
                         double dx, dy, dz;
-                        const double r2 = sep2(xi, yi, zi, x[jl], y[jl], z[jl], box, half, dx, dy, dz);
-                        if (SYM) {
-                            const double hj = hsym[jl];
-                            acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(hj, hj)));
-                        } else {
-                            acc = r2 < ri2;
-                        }
+                        const double r2 = sep2(xi, yi, zi, cx, cy, cz, box, half, dx, dy, dz);
+                        acc = SYM ? ((r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(hj, hj)))) : (r2 < ri2);
                     }
                     const unsigned bal = __ballot_sync(full, acc);
                     if (FILL && acc) {
@@ -293,22 +335,35 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                     // few of the warp's targets reached this leaf: the lanes hold
                     // the candidates and the warp loops over the reaching targets
                     // (each target's row gets its hits in candidate order, as below)
-                    double cx = 0, cy = 0, cz = 0, ch2 = 0;
+                    double cx = 0, cy = 0, cz = 0, hj = 0;
+                    float cxf = 0, cyf = 0, czf = 0, hjf = 0;
                     if (jl < b) {
                         cx = x[jl]; cy = y[jl]; cz = z[jl];
-                        if (SYM) { const double hj = hsym[jl]; ch2 = __dmul_rn(hj, hj); }
+                        cxf = __double2float_rn(cx); cyf = __double2float_rn(cy); czf = __double2float_rn(cz);
+                        if (SYM) { hj = hsym[jl]; hjf = __double2float_ru(hj); }
                     }
                     unsigned rem = e.lanes;
                     while (rem) {
                         const int tl = __ffs(rem) - 1;
                         rem &= rem - 1u;
-                        const double tx = __shfl_sync(full, xi, tl), ty = __shfl_sync(full, yi, tl);
-                        const double tz = __shfl_sync(full, zi, tl), tr2 = __shfl_sync(full, ri2, tl);
-                        bool acc = false;
+                        const float txf = __shfl_sync(full, xf, tl), tyf = __shfl_sync(full, yf, tl);
+                        const float tzf = __shfl_sync(full, zf, tl), trf = __shfl_sync(full, rf, tl);
+                        int sc = 0;
                         if (jl < b) {
-                            double dx, dy, dz;
-                            const double r2 = sep2(tx, ty, tz, cx, cy, cz, box, half, dx, dy, dz);
-                            acc = SYM ? ((r2 > 0) && !((r2 >= tr2) && (r2 >= ch2))) : (r2 < tr2);
+                            const float dx = wrap1f(txf - cxf, boxf, halff);
+                            const float dy = wrap1f(tyf - cyf, boxf, halff);
+                            const float dz = wrap1f(tzf - czf, boxf, halff);
+                            sc = screen(dx * dx + dy * dy + dz * dz, SYM ? fmaxf(trf, hjf) : trf, scr, SYM);
+                        }
+                        bool acc = sc == 1;
+                        if (__any_sync(full, sc == 2)) {
+                            const double tx = __shfl_sync(full, xi, tl), ty = __shfl_sync(full, yi, tl);
+                            const double tz = __shfl_sync(full, zi, tl), tr2 = __shfl_sync(full, ri2, tl);
+                            if (sc == 2) {
+                                double dx, dy, dz;
+                                const double r2 = sep2(tx, ty, tz, cx, cy, cz, box, half, dx, dy, dz);
+                                acc = SYM ? ((r2 > 0) && !((r2 >= tr2) && (r2 >= __dmul_rn(hj, hj)))) : (r2 < tr2);
+                            }
                         }
                         const unsigned bal = __ballot_sync(full, acc);
                         if (FILL) {
@@ -320,18 +375,30 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
                         if (lane == tl) cnt += __popc(bal);
                     }
                 } else {
-                    if (jl < b) s_c[wib][lane] = make_double4(x[jl], y[jl], z[jl], SYM ? hsym[jl] : 0.0);
+                    if (jl < b) {
+                        const double cx = x[jl], cy = y[jl], cz = z[jl], hj = SYM ? hsym[jl] : 0.0;
+                        s_c[wib][lane] = make_double4(cx, cy, cz, hj);
+                        s_cf[wib][lane] = make_float4(__double2float_rn(cx), __double2float_rn(cy), __double2float_rn(cz),
+                                                      SYM ? __double2float_ru(hj) : 0.0f);
+                    }
                     __syncwarp();
                     const int nk = min(32, b - c0);
                     if (mine) {
 #pragma unroll 4
                         for (int k = 0; k < nk; k++) {
-                            const double4 cj = s_c[wib][k];
-                            double dx, dy, dz;
-                            const double r2 = sep2(xi, yi, zi, cj.x, cj.y, cj.z, box, half, dx, dy, dz);
-                            bool acc;
-                            if (SYM) acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(cj.w, cj.w)));
-                            else acc = r2 < ri2;
+                            const float4 cf = s_cf[wib][k];
+                            const float dx = wrap1f(xf - cf.x, boxf, halff);
+                            const float dy = wrap1f(yf - cf.y, boxf, halff);
+                            const float dz = wrap1f(zf - cf.z, boxf, halff);
+                            const int sc = screen(dx * dx + dy * dy + dz * dz, SYM ? fmaxf(rf, cf.w) : rf, scr, SYM);
+                            bool acc = sc == 1;
+                            if (sc == 2) {
+                                const double4 cj = s_c[wib][k];
+                                double ddx, ddy, ddz;
+                                const double r2 = sep2(xi, yi, zi, cj.x, cj.y, cj.z, box, half, ddx, ddy, ddz);
+                                if (SYM) acc = (r2 > 0) && !((r2 >= ri2) && (r2 >= __dmul_rn(cj.w, cj.w)));
+                                else acc = r2 < ri2;
+                            }
                             if (acc) {
                                 if (FILL && (!cap || cnt < cap)) nbr[base + cnt] = c0 + k;
                                 cnt++;
@@ -347,8 +414,10 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
         const int nc = e.nchild;
         if (lane < nc) {
             s_nd[wib][lane] = t.node[e.child + lane];
-            s_lo[wib][lane] = t.lo[e.child + lane];
-            s_hi[wib][lane] = t.hi[e.child + lane];
+            float4 l, u;
+            outward(t.lo[e.child + lane], t.hi[e.child + lane], l, u);
+            s_lo[wib][lane] = l;
+            s_hi[wib][lane] = u;
         }
         __syncwarp();
         unsigned need[8];
@@ -393,7 +462,8 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
 {
     __shared__ StackNode s_stack[kWarps][kStack];
     __shared__ double4 s_c[kWarps][32];
-    __shared__ double4 s_lo[kWarps][8], s_hi[kWarps][8];
+    __shared__ float4 s_cf[kWarps][32];
+    __shared__ float4 s_lo[kWarps][8], s_hi[kWarps][8];
     __shared__ int4 s_nd[kWarps][8];
     const int lane = threadIdx.x & 31;
     const int n_groups = SOLO ? n_targets : (n_targets + 31) / 32;
@@ -403,7 +473,7 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= n_groups) break;
         walk_group<SYM, FILL, SOLO>(g, t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, s_stack,
-                                    s_c, s_lo, s_hi, s_nd);
+                                    s_c, s_cf, s_lo, s_hi, s_nd);
         __syncwarp();
     }
 }
