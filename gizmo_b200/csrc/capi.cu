@@ -651,7 +651,7 @@ int sym_rows_from_density(gz_context *c)
     GZ_CUDA(c, cudaMemsetAsync(c->s_bcnt.p, 0, sizeof(int) * N, s));  // reused as the B cursors
     sym_scatter(n, ptr<long long>(c->d_beg), ptr<int>(c->d_nbr), ptr<int>(c->s_acnt), ptr<long long>(c->s_off),
                 ptr<int>(c->s_bcnt), ptr<int>(c->s_tmp), s);
-    sym_sort(n, ptr<long long>(c->s_off), ptr<int>(c->s_tmp), ptr<int>(c->s_nbr), s);
+    sym_sort(n, ptr<long long>(c->s_off), ptr<int>(c->s_acnt), ptr<int>(c->s_tmp), ptr<int>(c->s_nbr), s);
     c->launches += 2;
     GZ_CUDA(c, cudaGetLastError());
     c->pairs_symmetric = total;

@@ -554,19 +554,45 @@ __global__ void __launch_bounds__(256) k_sym_scatter(int n, const long long *__r
     }
 }
 
-// Each row sorted ascending by rank (its entries are distinct), one warp per row.
+// Each row sorted ascending (its entries are distinct), TPT lanes per row. A
+// row is A_i (the compacted density row: ascending, as the walk visits leaves
+// and their particles in index order) followed by B_i (unordered, appended by
+// the scatter). An A entry's rank is its index plus the B entries below it; a
+// B entry's rank is the A entries below it (binary search) plus the B entries
+// below it. A row whose A part is not ascending is ranked by comparing every
+// pair.
+template <int TPT>
 __global__ void __launch_bounds__(256) k_sym_sort(int n, const long long *__restrict__ s_off,
-                                                  const int *__restrict__ rows, int *out)
+                                                  const int *__restrict__ acnt, const int *__restrict__ rows, int *out)
 {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= n) return;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gtid / TPT, lane = gtid % TPT;
+    if (i >= n) return;  // the row's lanes leave together
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
     const long long b0 = s_off[i], b1 = s_off[i + 1];
-    const int len = (int)(b1 - b0);
-    for (int k = lane; k < len; k += 32) {
-        const int v = rows[b0 + k];
+    const int len = (int)(b1 - b0), a = acnt[i];
+    const int *r = rows + b0;
+    bool asc = true;
+    for (int k = lane + 1; k < a; k += TPT) asc &= r[k - 1] < r[k];
+    asc = __all_sync(mask, asc);
+    for (int k = lane; k < len; k += TPT) {
+        const int v = r[k];
         int rank = 0;
-        for (int m = 0; m < len; m++) rank += rows[b0 + m] < v;
+        if (asc) {
+            for (int m = a; m < len; m++) rank += r[m] < v;
+            if (k < a) {
+                rank += k;
+            } else {
+                int lo = 0, hi = a;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (r[mid] < v) lo = mid + 1; else hi = mid;
+                }
+                rank += lo;
+            }
+        } else {
+            for (int m = 0; m < len; m++) rank += r[m] < v;
+        }
         out[b0 + rank] = v;
     }
 }
@@ -588,9 +614,9 @@ void sym_scatter(int n, const long long *beg, const int *nbr, const int *acnt, c
     if (n > 0) k_sym_scatter<8><<<(unsigned)(((long long)n * 8 + 255) / 256), 256, 0, s>>>(n, beg, nbr, acnt, s_off, bcur, rows);
 }
 
-void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStream_t s)
+void sym_sort(int n, const long long *s_off, const int *acnt, const int *rows, int *out, cudaStream_t s)
 {
-    if (n > 0) k_sym_sort<<<(unsigned)(((long long)n * 32 + 255) / 256), 256, 0, s>>>(n, s_off, rows, out);
+    if (n > 0) k_sym_sort<8><<<(unsigned)(((long long)n * 8 + 255) / 256), 256, 0, s>>>(n, s_off, acnt, rows, out);
 }
 
 // After a padded fill: a row that fit its cap slots gets [slot*cap, +count);

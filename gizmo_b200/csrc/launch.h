@@ -28,7 +28,7 @@ void sym_split(int n, const double *x, const double *y, const double *z, const d
 void sym_counts(int n, const int *acnt, const int *bcnt, long long *cnt, cudaStream_t s);
 void sym_scatter(int n, const long long *beg, const int *nbr, const int *acnt, const long long *s_off, int *bcur,
                  int *rows, cudaStream_t s);
-void sym_sort(int n, const long long *s_off, const int *rows, int *out, cudaStream_t s);
+void sym_sort(int n, const long long *s_off, const int *acnt, const int *rows, int *out, cudaStream_t s);
 
 // Work description of the density iteration.
 struct DensityWork {
