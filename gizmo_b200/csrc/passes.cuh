@@ -168,8 +168,12 @@ __global__ void __launch_bounds__(128, 5) k_gradients(PassParams p, Particles ps
     for (int k = 0; k < 5; k++) { mx[k] = T(0); mn[k] = T(0); }
     if (enabled) {
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
-        for (long long e = b0 + lane; e < b1; e += TPT) {
-            const GradRec<T> rj = rec[rows.nbr[e]];
+        long long e = b0 + lane;
+        int jn = e < b1 ? rows.nbr[e] : 0;
+        for (; e < b1; e += TPT) {
+            const int jc = jn;
+            jn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;  // the next index is in flight during this pair
+            const GradRec<T> rj = rec[jc];
             const double mj = rj.m, rhoj = rj.rho, hjd = rj.h;
             if (mj <= 0) continue;
             if (rhoj <= 0 || hjd <= 0) continue;
@@ -376,8 +380,11 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     if (enabled) {
         vs = (double)rip->s.cs;
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
-        for (long long e = b0 + lane; e < b1; e += TPT) {
-            const int j = rows.nbr[e];
+        long long e = b0 + lane;
+        int jn = e < b1 ? rows.nbr[e] : 0;
+        for (; e < b1; e += TPT) {
+            const int j = jn;
+            jn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;  // the next index is in flight during this entry
             PairFlux<T> F;
             double mj, dtj, dx, dy, dz;
             int j_active;
