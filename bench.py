@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--cpu-n1", type=int, default=64, help="size of the CPU-baseline instance")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cold", action="store_true")
     return ap.parse_args()
 
 
@@ -176,6 +177,16 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU baseline
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(n1: int, name: str, kind_pref: str = "reference", steps: int = 1):
     """Full CPU pass (density -> gradients -> force) of a smaller instance of the
     same generator on all host threads; returns (rate, seconds, kind, cores, n)."""
@@ -209,6 +220,7 @@ def run_ours(args, world, rank, local):
     wl = make_workload(args.workload, n1, abi.PRECISION_FP64)
     N = wl.n
     t_gen = time.time() - t_gen
+    h_cold = wl.h.copy()  # the generator's seed: octree density estimate
     # steady-state seed: converge once in FP64 from the cold seed
     hp64 = HydroPass(wl.params, device=local)
     hp64.upload_workload(wl)
@@ -332,6 +344,38 @@ def run_ours(args, world, rank, local):
         cons[tag] = {"momentum": float(np.abs(mom.sum(0)).max() / np.abs(mom).sum()),
                      "mass": float(abs(dtm.sum()) / (np.abs(dtm).sum() + 1e-300))}
 
+    # Cold seed: one mixed-form pass from the generator's h seed (octree density
+    # estimate, h0 = (3 DesNumNgb / (4 pi n_local))^(1/3)), timed once after the
+    # steady-state runs. Its density runs in slices of 2,097,152 particles (a
+    # one-way row depends on its own target's h only, so slicing changes no
+    # result and bounds the rows a cold seed can ask for); gradients and force
+    # then build their symmetric rows with a tree walk.
+    cold = None
+    if not args.skip_cold:
+        h_steady = wl.h
+        wl.h = h_cold
+        hpm.upload_workload(wl)
+        stream = torch.cuda.ExternalStream(hpm.stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        iters = 0
+        chunk = 1 << 21
+        for a in range(0, N, chunk):
+            hpm.density(np.arange(a, min(N, a + chunk), dtype=np.int32) if N > chunk else None)
+            iters = max(iters, hpm.status()["density_iterations"])
+        ev[1].record(stream)
+        hpm.hydro_gradient_calc()
+        hpm.hydro_force()
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        t_cold = ev[0].elapsed_time(ev[2]) / 1e3
+        cold = {"value": N / t_cold, "unit": UNIT, "ms_per_pass": 1e3 * t_cold,
+                "density_ms": ev[0].elapsed_time(ev[1]), "density_iterations_max": iters,
+                "seed": "octree density estimate (3 DesNumNgb / (4 pi n_local))^(1/3)",
+                "note": "mixed form; density in slices of 2,097,152 particles; one pass, after the steady-state runs"}
+        wl.h = h_steady  # the end-to-end steps below start from the steady-state seed again
+
     # Roofline of each timed kernel family (CUDA events around its launches on
     # the context's stream, over the timed steps of the mixed form): algorithmic
     # FLOPs / kernel time against the nominal rate of the pipe its arithmetic
@@ -397,7 +441,7 @@ def run_ours(args, world, rank, local):
         "accuracy_mixed_vs_fp64": acc, "conservation": cons,
         "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
         "gpu_launches": launches, "clocks": clocks,
-        "roofline": roofline, "kernels": kernels,
+        "roofline": roofline, "kernels": kernels, "cold_seed": cold,
     }
 
     # end to end: pinned host buffers in, results out, every step
@@ -432,7 +476,7 @@ def run_ours(args, world, rank, local):
 
     if rank == 0 and not args.skip_cpu:
         rate, secs, kind, cores, ncpu = cpu_baseline(args.cpu_n1, args.workload)
-        result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+        result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
                                   "sample": f"one full density->gradients->force pass of a {args.cpu_n1}^3 "
                                             f"({ncpu:,}-particle) instance of the same generator, {secs:.2f} s"}
     return result
@@ -455,7 +499,8 @@ def run_reference(args, world, rank):
         "config": {"workload": workload_desc(args.workload, args.n1 or default_n1(args.workload)),
                    "sample": workload_desc(args.workload, n1), "n_particles_per_sample": ncpu, "precision": "fp64",
                    "parallelism": f"{cores} host threads", "wall_s": round(wall, 1)},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+                         "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

@@ -12,6 +12,14 @@ particle masses, numpy ``default_rng`` with the listed seeds):
                 P(k) ~ k^-3 scaled to sigma_lnrho; solenoidal Gaussian velocity
                 field P(k) ~ k^-4 at rms Mach 2; isothermal u = 1 (gamma 1.0001);
                 MFM, Wendland C2, 64 neighbours.
+  shock_tube    lattice + U(-0.1, 0.1) spacing jitter; a plane through the box
+                centre with a random unit normal splits left and right states,
+                rho_L, rho_R ~ U[0.125, 1] (set through the particle masses),
+                P_L, P_R ~ U[0.1, 1], at rest; MFM, gamma 5/3, cubic, 32
+                neighbours. In the periodic box the plane's image is a second
+                discontinuity.
+  boxes         a batch of independent boxes of log-uniform sizes, each a
+                shock tube or a Sedov blast (E ~ U[0.1, 10]) with equal odds.
   plummer_mix   90% of particles in 1000 Plummer spheres (scale radius
                 log-uniform in [0.002, 0.02], truncated at 20a, velocity
                 dispersion sqrt(M/sqrt(r^2+a^2)) per axis), 10% uniform
@@ -123,7 +131,7 @@ def timestep_bins(h: np.ndarray, cs: np.ndarray, kmin: int = 4, kmax: int = 30) 
     return np.ldexp(1.0, -k.astype(np.int64))
 
 
-def sedov(n1: int = 32, seed: int = 1, precision: int = PRECISION_FP64) -> Workload:
+def sedov(n1: int = 32, seed: int = 1, precision: int = PRECISION_FP64, energy: float = 1.0) -> Workload:
     rng = np.random.default_rng(seed)
     N = n1 ** 3
     s = 1.0 / n1
@@ -140,13 +148,60 @@ def sedov(n1: int = 32, seed: int = 1, precision: int = PRECISION_FP64) -> Workl
     near = order[:32]
     h_inj = r[order[32]]
     w = _cubic_w(r[near] / h_inj)
-    u[near] += 1.0 * w / (mass[near] * w).sum()
+    u[near] += energy * w / (mass[near] * w).sum()
     vel = np.zeros((N, 3))
     params = make_params(KERNEL_CUBIC, METHOD_MFM, 5.0 / 3.0, 32.0, 0.1, precision)
     h = np.full(N, (32.0 / (VOLNORM * N)) ** (1.0 / 3.0)) * (1.0 + rng.uniform(-0.05, 0.05, N))
     cs = np.sqrt(params.gamma * (params.gamma - 1) * u)
     dt = timestep_bins(h, cs)
     return Workload("sedov", params, pos, vel, mass, u, dt, h, np.zeros(N), dict(n1=n1, seed=seed))
+
+
+def _jittered_lattice(n1: int, rng: np.random.Generator) -> np.ndarray:
+    s = 1.0 / n1
+    g = (np.arange(n1) + 0.5) * s
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    pos += rng.uniform(-0.1, 0.1, size=pos.shape) * s
+    return pos % 1.0
+
+
+def shock_tube(n1: int = 16, seed: int = 5, precision: int = PRECISION_FP64) -> Workload:
+    rng = np.random.default_rng(seed)
+    N = n1 ** 3
+    pos = _jittered_lattice(n1, rng)
+    normal = rng.standard_normal(3)
+    normal /= np.linalg.norm(normal)
+    rho_l, rho_r = rng.uniform(0.125, 1.0, 2)
+    p_l, p_r = rng.uniform(0.1, 1.0, 2)
+    left = (pos - 0.5) @ normal < 0
+    rho = np.where(left, rho_l, rho_r)
+    mass = rho / N  # equal volumes per lattice particle: the density follows the mass
+    params = make_params(KERNEL_CUBIC, METHOD_MFM, 5.0 / 3.0, 32.0, 0.1, precision)
+    u = np.where(left, p_l, p_r) / ((params.gamma - 1.0) * rho)
+    vel = np.zeros((N, 3))
+    h = np.full(N, (32.0 / (VOLNORM * N)) ** (1.0 / 3.0)) * (1.0 + rng.uniform(-0.05, 0.05, N))
+    cs = np.sqrt(params.gamma * (params.gamma - 1) * u)
+    dt = timestep_bins(h, cs)
+    return Workload("shock_tube", params, pos, vel, mass, u, dt, h, np.zeros(N),
+                    dict(n1=n1, seed=seed, normal=normal.tolist(), rho=(rho_l, rho_r), p=(p_l, p_r)))
+
+
+def boxes(n_boxes: int, seed: int = 5, n_min: int = 1024, n_max: int = 65536,
+          precision: int = PRECISION_FP64) -> list:
+    """A batch of independent boxes: sizes log-uniform in [n_min, n_max] (rounded
+    to a lattice n1^3), each a shock tube or a Sedov blast with equal odds."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n_boxes):
+        n = np.exp(rng.uniform(np.log(n_min), np.log(n_max)))
+        n1 = max(4, int(round(n ** (1.0 / 3.0))))
+        sub = int(rng.integers(1 << 30))
+        if rng.uniform() < 0.5:
+            out.append(shock_tube(n1, seed=sub, precision=precision))
+        else:
+            out.append(sedov(n1, seed=sub, precision=precision, energy=float(rng.uniform(0.1, 10.0))))
+    return out
 
 
 def _grf(ng: int, slope: float, rng: np.random.Generator) -> np.ndarray:
