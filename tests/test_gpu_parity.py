@@ -156,6 +156,47 @@ def test_neighbour_sets_bit_exact(name):
     assert g0[0][-1] > 20 * wl.n  # rows are populated
 
 
+@pytest.mark.parametrize("box", [3.7, 1e-3])
+def test_neighbour_sets_bit_exact_scaled_box(box):
+    """The walk decides most candidates in FP32 with a margin proportional to
+    the box size: on a box far from unit size, with the clusters shifted across
+    the periodic faces and particles on the faces themselves, the rows are still
+    exactly the FP64 predicates' (all walk modes, and the rows the gradient pass
+    derives)."""
+    wl = CASES["plummer16"]()
+    rng = np.random.default_rng(23)
+    pos = (wl.pos + rng.uniform(0, 1, 3)) % 1.0  # clusters straddle the faces
+    pos = pos * box
+    pos[:8, 0] = 0.0  # on a lower face (distinct points)
+    pos[8:16, 1] = np.nextafter(box, 0.0)  # just below an upper face
+    wl.pos = pos
+    wl.h = wl.h * box
+    wl.params.box_size = box
+    wl.params.max_kernel_radius *= box
+    wl.params.min_kernel_radius *= box
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.density()
+        h = hp.download(["h"])["h"]
+        g0 = hp.neighbors(0)
+        g1 = hp.neighbors(1)
+        few = rng.choice(wl.n, size=wl.n // 20, replace=False).astype(np.int32)
+        g0f = hp.neighbors(0, few)
+        g1f = hp.neighbors(1, few)
+        hp.hydro_gradient_calc()
+        g2 = hp.neighbors(2)
+    st = O.new_state(wl.n, wl.inputs())
+    st["h"][:] = h
+    o0 = O.neighbors(wl.params, st, 0)
+    o1 = O.neighbors(wl.params, st, 1)
+    o0f = O.neighbors(wl.params, st, 0, few)
+    o1f = O.neighbors(wl.params, st, 1, few)
+    for (go, gn), (oo, on) in [(g0, o0), (g1, o1), (g0f, o0f), (g1f, o1f), (g2, o1)]:
+        assert np.array_equal(go, oo)
+        assert np.array_equal(gn, on)
+    assert g0[0][-1] > 20 * wl.n
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_active_subset_matches_oracle(name):
     wl = CASES[name]()
