@@ -13,6 +13,24 @@
 
 namespace gz {
 
+// Stores one record per thread of the block, for the consecutive particles
+// [first, first + count), through shared memory, so that the block writes one
+// contiguous run with 16-byte stores instead of each lane a record-sized stride.
+// Every thread of the block takes part (it synchronises the block).
+template <typename R>
+GZ_DEV void store_block_records(R *dst, const R &r, int first, int count, int4 *smem)
+{
+    static_assert(sizeof(R) % 16 == 0, "records are whole 16-byte words");
+    constexpr int kWords = (int)(sizeof(R) / 16);
+    if ((int)threadIdx.x < count) reinterpret_cast<R *>(smem)[threadIdx.x] = r;
+    __syncthreads();
+    int4 *out = reinterpret_cast<int4 *>(dst + first);
+    for (int k = threadIdx.x; k < count * kWords; k += blockDim.x) out[k] = smem[k];
+    __syncthreads();
+}
+
+constexpr int kPackBlock = 128;
+
 // ---------------------------------------------------------------- density
 // DensitySpec::pair_kernel (density_loop.h:1140-1385), gas i, gas j; the
 // row is a superset (buffered radius) and r2 < h^2 is re-tested exactly.
@@ -127,14 +145,17 @@ template <typename T> struct __align__(16) GradRec {
     double P, vx, vy, vz;
 };
 
-template <typename T> __global__ void k_pack_gradient(Particles ps, GradRec<T> *rec)
+template <typename T> __global__ void __launch_bounds__(kPackBlock) k_pack_gradient(Particles ps, GradRec<T> *rec)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ps.n) return;
-    GradRec<T> r;
-    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
-    r.P = ps.pressure[i]; r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i];
-    rec[i] = r;
+    extern __shared__ int4 s_pack[];
+    const int first = blockIdx.x * blockDim.x;
+    const int i = first + threadIdx.x;
+    GradRec<T> r{};
+    if (i < ps.n) {
+        r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
+        r.P = ps.pressure[i]; r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i];
+    }
+    store_block_records(rec, r, first, min((int)blockDim.x, ps.n - first), s_pack);
 }
 
 // gradient_accumulate_neighbor (gradient_functions.h:304-665) + the
@@ -253,7 +274,7 @@ void launch_gradients(const PassParams &p, const Particles &ps, const int *targe
 {
     if (n_targets <= 0) return;
     GradRec<T> *rec = (GradRec<T> *)recbuf;
-    k_pack_gradient<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
+    k_pack_gradient<T><<<(ps.n + kPackBlock - 1) / kPackBlock, kPackBlock, kPackBlock * sizeof(GradRec<T>), s>>>(ps, rec);
     const long long threads = (long long)n_targets * tpt;
     const unsigned blocks = (unsigned)((threads + 127) / 128);  // 128-thread blocks: finer register granularity
     if (ev) cudaEventRecord(ev->start, s);
@@ -315,20 +336,26 @@ struct __align__(16) GatherRec {
     int active, pad;
 };
 
-template <typename T> __global__ void k_pack_force(Particles ps, double gamma, ForceRec<T> *rec, GatherRec *grec)
+
+template <typename T> __global__ void __launch_bounds__(kPackBlock) k_pack_force(Particles ps, double gamma,
+                                                                                ForceRec<T> *rec, GatherRec *grec)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ps.n) return;
-    ForceRec<T> r;
-    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
-    load_side(ps, i, gamma, r.s);
-    r.active = ps.active[i];
-    rec[i] = r;
-    GatherRec g;
-    g.x = r.x; g.y = r.y; g.z = r.z; g.m = r.m; g.dt = ps.dt[i];
-    g.active = r.active;
-    g.pad = 0;
-    grec[i] = g;
+    extern __shared__ int4 s_pack[];
+    const int first = blockIdx.x * blockDim.x;
+    const int i = first + threadIdx.x;
+    const int count = min((int)blockDim.x, ps.n - first);
+    ForceRec<T> r{};
+    GatherRec g{};
+    if (i < ps.n) {
+        r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.h = ps.h[i]; r.m = ps.m[i]; r.rho = ps.rho[i];
+        load_side(ps, i, gamma, r.s);
+        r.active = ps.active[i];
+        g.x = r.x; g.y = r.y; g.z = r.z; g.m = r.m; g.dt = ps.dt[i];
+        g.active = r.active;
+        g.pad = 0;
+    }
+    store_block_records(rec, r, first, count, s_pack);
+    store_block_records(grec, g, first, count, s_pack);
 }
 
 // Row i of the symmetric list: every pair is evaluated in one canonical
@@ -648,7 +675,8 @@ void launch_force(const PassParams &p, const Particles &ps, const int *targets, 
     // the record scratch holds the force records, then the gather records
     ForceRec<T> *rec = (ForceRec<T> *)recbuf;
     GatherRec *grec = (GatherRec *)(rec + ps.n);
-    k_pack_force<T><<<(ps.n + 255) / 256, 256, 0, s>>>(ps, p.gamma, rec, grec);
+    k_pack_force<T><<<(ps.n + kPackBlock - 1) / kPackBlock, kPackBlock, kPackBlock * sizeof(ForceRec<T>), s>>>(
+        ps, p.gamma, rec, grec);
     if (fluxbuf) {
         PairFlux<T> *flux = (PairFlux<T> *)fluxbuf;
         const long long warps = (n_targets + kPairRows - 1) / kPairRows;

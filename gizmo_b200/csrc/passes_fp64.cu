@@ -12,19 +12,23 @@ size_t force_record_bytes(int mixed)
 }
 size_t pair_flux_bytes(int mixed) { return mixed ? sizeof(PairFlux<float>) : sizeof(PairFlux<double>); }
 
-__global__ void k_pack_density(Particles ps, DensRec *rec)
+__global__ void __launch_bounds__(kPackBlock) k_pack_density(Particles ps, DensRec *rec)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ps.n) return;
-    DensRec r;
-    r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.m = ps.m[i];
-    r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i]; r.pad = 0.0;
-    rec[i] = r;
+    extern __shared__ int4 s_pack[];
+    const int first = blockIdx.x * blockDim.x;
+    const int i = first + threadIdx.x;
+    DensRec r{};
+    if (i < ps.n) {
+        r.x = ps.x[i]; r.y = ps.y[i]; r.z = ps.z[i]; r.m = ps.m[i];
+        r.vx = ps.vx[i]; r.vy = ps.vy[i]; r.vz = ps.vz[i]; r.pad = 0.0;
+    }
+    store_block_records(rec, r, first, min((int)blockDim.x, ps.n - first), s_pack);
 }
 
 void density_pack(const Particles &ps, DensRec *rec, cudaStream_t s)
 {
-    if (ps.n > 0) k_pack_density<<<(ps.n + 255) / 256, 256, 0, s>>>(ps, rec);
+    if (ps.n > 0)
+        k_pack_density<<<(ps.n + kPackBlock - 1) / kPackBlock, kPackBlock, kPackBlock * sizeof(DensRec), s>>>(ps, rec);
 }
 
 void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s)
