@@ -474,7 +474,7 @@ def run_ours(args, world, rank, local):
     hpm.close()
     hp64.close()
 
-    if rank == 0 and not args.skip_cpu:
+    if rank == 0 and world == 1 and not args.skip_cpu:  # the CPU baseline: one GPU's run only
         rate, secs, kind, cores, ncpu = cpu_baseline(args.cpu_n1, args.workload)
         result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
                                   "sample": f"one full density->gradients->force pass of a {args.cpu_n1}^3 "
