@@ -36,10 +36,10 @@ struct Particles {
 // owns the sorted run [first, first + count); an internal node's children
 // are the nodes [child, child + nchild); a leaf (child = -1) has at most
 // kLeafMax particles unless it is at the deepest level (coincident keys).
-// Leaves are tested 32 particles at a time; leaves of up to 128 particles
-// (measured against 8 to 96) cost the walk fewer node openings than the extra
+// Leaves are tested 32 particles at a time; leaves of up to 96 particles
+// (measured against 8 to 128) cost the walk fewer node openings than the extra
 // candidate tests they bring.
-constexpr int kLeafMax = 128;
+constexpr int kLeafMax = 96;
 
 struct Tree {
     double box;
