@@ -26,6 +26,8 @@
 //   symmetric r2 > 0 and !(r2 >= h_i^2 and r2 >= h_j^2) (gradients, force)
 #include <cub/cub.cuh>
 
+#include <atomic>
+
 #include "launch.h"
 
 namespace gz {
@@ -205,6 +207,7 @@ GZ_DEV float wrap1f(float d, float box, float half)
 }
 
 constexpr int kStack = 160;  // >= 7 x 22 levels + 8
+constexpr int kMaxWalkDevices = 64;  // devices whose launch shapes are cached
 constexpr int kWarps = 8;    // warps per block of the walks
 
 // A node waiting on a warp's stack: its run, its children and the lanes whose
@@ -669,13 +672,20 @@ static void launch_walk(const Tree &t, const double *x, const double *y, const d
                         const double *hsym, const int *targets, int n_targets, long long *counts, const long long *off,
                         int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
 {
-    static int resident = 0;  // blocks of this instance resident per SM x SMs (device 0-independent enough)
+    // blocks of this instance resident on the current device (multiprocessors
+    // x blocks per multiprocessor), looked up once per device; concurrent
+    // first calls store the same value
+    static std::atomic<int> resident_of[kMaxWalkDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxWalkDevices) dev = 0;
+    int resident = resident_of[dev].load(std::memory_order_relaxed);
     if (resident == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<SYM, FILL, SOLO>, 32 * kWarps, 0);
         resident = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+        resident_of[dev].store(resident, std::memory_order_relaxed);
     }
     const long long groups = SOLO ? n_targets : (n_targets + 31) / 32;
     const long long need = (groups + kWarps - 1) / kWarps;
@@ -696,13 +706,17 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
     // list (the rows rebuilt after an h regrowth, scattered through the box)
     // gets one warp per target instead: as groups it would run on a few
     // warps, each walking 32 unrelated regions one after another.
-    static long long group_warps = 0;
+    static std::atomic<long long> group_warps_of[kMaxWalkDevices];  // per device, as in launch_walk
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxWalkDevices) dev = 0;
+    long long group_warps = group_warps_of[dev].load(std::memory_order_relaxed);
     if (group_warps == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<false, true, false>, 32 * kWarps, 0);
         group_warps = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarps;
+        group_warps_of[dev].store(group_warps, std::memory_order_relaxed);
     }
     const bool sparse = (long long)n_targets * 4 < (long long)t.n_particles;
     const bool solo = n_targets == 1 || (sparse && (n_targets + 31) / 32 < group_warps);
