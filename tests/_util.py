@@ -29,6 +29,30 @@ def rel_err(a, b, floor_frac: float = 1e-6) -> float:
     return float(np.max(np.abs(a - b) / scale))
 
 
+def row_rel_err(a, b, floor_frac: float = 1e-6) -> float:
+    """max over rows of |a_row - b_row| / max(|b_row|, floor_frac * max |b_row|),
+    with the row the trailing components of a vector or tensor field. The sums
+    behind such a field cancel component by component, and their roundoff in
+    another summation order scales with the row's magnitude, not with the size
+    of one (possibly near-zero) component."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if b.size == 0:
+        return 0.0
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    nb = np.linalg.norm(b, axis=1)
+    top = float(nb.max())
+    if top == 0.0:
+        return float(np.linalg.norm(a, axis=1).max())
+    return float(np.max(np.linalg.norm(a - b, axis=1) / np.maximum(nb, floor_frac * top)))
+
+
+def field_err(name: str, a, b, floor_frac: float = 1e-6) -> float:
+    """rel_err for a scalar field, row_rel_err for a vector or tensor field."""
+    return row_rel_err(a, b, floor_frac) if np.asarray(b).ndim > 1 else rel_err(a, b, floor_frac)
+
+
 def norm_err(a, b) -> float:
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()
