@@ -359,12 +359,13 @@ template <typename T> __global__ void __launch_bounds__(kPackBlock) k_pack_force
 }
 
 // Row i of the symmetric list: every pair is evaluated in one canonical
-// orientation (lower sorted index as the R side) so the flux seen from i and
-// from j are exact negatives -- mass and momentum are conserved to roundoff
-// of the FP64 accumulation. i-side accumulation follows
-// hydro_functions.h:419-509, j-side dMass writes hydro_functions.h:511-532,
-// writeback hydro_force_loop.cc:227-391, final operations
-// hydro_toplevel.cc:133-253.
+// orientation (lower sorted index as the i side of the face) so the flux seen
+// from i and from j are exact negatives -- mass and momentum are conserved to
+// roundoff of the FP64 accumulation. i-side accumulation follows
+// hydro_functions.h:419-509, j-side dMass writes hydro_functions.h:511-532.
+// The row's sums go to `sums`; k_force_finish then does the writeback
+// (hydro_force_loop.cc:227-391) and the final operations
+// (hydro_toplevel.cc:133-253).
 //
 // MODE kBoth: row i evaluates all its pairs (as the reference does: each pair
 //   twice, once per row). Used for active subsets.
