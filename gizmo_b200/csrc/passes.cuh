@@ -36,6 +36,31 @@ constexpr int kPackBlock = 128;
 // row is a superset (buffered radius) and r2 < h^2 is re-tested exactly.
 constexpr int kDensityBlock = 128;
 
+// A record through the read-only data path, in 16-byte pieces.
+template <typename R> GZ_DEV R ldg_record(const R *__restrict__ p)
+{
+    static_assert(sizeof(R) % 16 == 0, "records are whole 16-byte words");
+    R r;
+    int4 *d = reinterpret_cast<int4 *>(&r);
+    const int4 *s = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(R) / 16); k++) d[k] = __ldg(s + k);
+    return r;
+}
+
+// A neighbour's density record through the read-only data path, in 16-byte
+// pieces, without its padding word.
+GZ_DEV DensRec load_dens_rec(const DensRec *__restrict__ rec, int j)
+{
+    const double2 *q = reinterpret_cast<const double2 *>(rec + j);
+    const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    DensRec r;
+    r.x = q0.x; r.y = q0.y; r.z = q1.x; r.m = q1.y; r.vx = q2.x; r.vy = q2.y;
+    r.vz = __ldg(reinterpret_cast<const double *>(q + 3));
+    r.pad = 0.0;
+    return r;
+}
+
 template <typename T, int TPT>
 __global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p, Particles ps, DensityWork w)
 {
@@ -103,12 +128,13 @@ __global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p,
     // entry's index is loaded a step ahead, so the record load does not wait
     // on it
     const long long b0 = w.beg[t], b1 = w.end[t];
+    const int *__restrict__ nbr = w.nbr;
     long long e = b0 + lane;
-    int j = e < b1 ? w.nbr[e] : 0;
+    int j = e < b1 ? __ldg(nbr + e) : 0;
     for (; e < b1; e += TPT) {
         const long long en = e + TPT;
-        const int jn = en < b1 ? w.nbr[en] : 0;
-        pair(w.rec[j]);
+        const int jn = en < b1 ? __ldg(nbr + en) : 0;
+        pair(load_dens_rec(w.rec, j));
         j = jn;
     }
 #pragma unroll
@@ -190,11 +216,11 @@ __global__ void __launch_bounds__(128, 5) k_gradients(PassParams p, Particles ps
     if (enabled) {
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         long long e = b0 + lane;
-        int jn = e < b1 ? rows.nbr[e] : 0;
+        int jn = e < b1 ? __ldg(rows.nbr + e) : 0;
         for (; e < b1; e += TPT) {
             const int jc = jn;
-            jn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;  // the next index is in flight during this pair
-            const GradRec<T> rj = rec[jc];
+            jn = e + TPT < b1 ? __ldg(rows.nbr + e + TPT) : 0;  // the next index is in flight during this pair
+            const GradRec<T> rj = ldg_record(rec + jc);
             const double mj = rj.m, rhoj = rj.rho, hjd = rj.h;
             if (mj <= 0) continue;
             if (rhoj <= 0 || hjd <= 0) continue;
@@ -617,7 +643,9 @@ __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps,
         const int i = (int)(r0 + k);
         const long long e = split_k + (f - excl_k);
         const int j = rows.nbr[e];
-        const ForceRec<T> *rip = rec + i, *rjp = rec + j;
+        const ForceRec<T> *rip = rec + i;  // shared by the lanes of the row: cached
+        const ForceRec<T> rj = ldg_record(rec + j);
+        const ForceRec<T> *rjp = &rj;
         PairFlux<T> F;
         F.valid = 0;
         F.rho = F.p = T(0);
