@@ -81,3 +81,16 @@ def test_bad_arguments_rejected_before_device_use():
     assert lib.gz_create(None, 0, C.byref(ctx)) == abi.ERR_ARG
     assert lib.gz_upload(None, None) == abi.ERR_ARG
     assert lib.gz_hydro_density(None, None, 0) == abi.ERR_ARG
+
+
+def test_header_constants_match_the_python_mirror():
+    src = open(HEADER).read()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define\s+GZ_(\w+)\s+(-?\d+)", src, re.M)}
+    timers = {k[len("TIMER_"):].lower(): v for k, v in defines.items() if k.startswith("TIMER_") and k != "TIMERS"}
+    assert timers == abi.TIMERS
+    assert defines["TIMERS"] == len(abi.TIMERS)
+    for name, value in defines.items():
+        if name.startswith("TIMER"):
+            continue
+        assert hasattr(abi, name), name
+        assert getattr(abi, name) == value, name
