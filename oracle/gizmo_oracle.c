@@ -1451,3 +1451,79 @@ double orc_full_pass_seconds(const gz_params *p, orc_state *s, const int *active
     if (status) *status = st;
     return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
+
+/* -------------------------------------------------------------------- kick */
+/* do_the_kick (core/kicks.cc:284-545) for gas cells of the configuration
+ * above (non-comoving: cf_atime = cf_a2inv = cf_hubble_a = 1; no timestep
+ * dilation, cooling, entropy switch, special boundaries or extra physics):
+ *   MFV conserved-mass update      kicks.cc:290-323
+ *   thermal update                 kicks.cc:331-358, 466-478, with
+ *     internal_energy_positivity_catch (core/proto.h:417-421, no u_floor)
+ *     and enforce_temperature_floor (declarations/cell_data.h:604-611)
+ *   momentum kick                  kicks.cc:480-490
+ *   mass check, predicted reset    kicks.cc:521-543
+ * unit_integertime_in_physical is Timebase_interval (core/timestep_functions.h:43-46)
+ * and the non-comoving gravkick factor is (time1 - time0) * Timebase_interval
+ * (timestep_functions.h:203-206, 253-256). Vec3 updates are per component. */
+int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, double min_egy_spec)
+{
+    const int mfv = p->method == GZ_METHOD_MFV;
+    for (int i = 0; i < k->n; i++) {
+        double mass_old, mass_pred, mass_new;
+        mass_old = mass_pred = mass_new = k->mass[i];
+        const long long span = k->tend[i] - k->tstart[i];
+        if (mfv && k->dmass[i] != 0) {
+            double dm = 0;
+            if (mode != 0) {
+                dm = ((double)span * timebase) * k->dtmass[i];
+                if (dm * k->dmass[i] < 0) dm = 0;
+                if (fabs(dm) > fabs(k->dmass[i])) dm = k->dmass[i];
+                k->dmass[i] -= dm;
+            } else {
+                dm = k->dmass[i];
+            }
+            if (dm < -0.99 * k->mass_true[i]) dm = -0.99 * k->mass_true[i];
+            mass_old = k->mass_true[i];
+            mass_pred = k->mass[i];
+            mass_new = mass_old + dm;
+            k->mass_true[i] = mass_new;
+            if (mode == 0) k->dmass[i] = 0;
+        }
+        if (!k->active[i]) continue;
+
+        const double dt_hydro = (double)span * timebase;
+        const double dt_grav = (double)span * timebase;
+        const double *g = k->grav + 3 * (size_t)i;
+        double dent_grav = 0;
+        if (mfv) {
+            const double *w = k->gravwork + 3 * (size_t)i;
+            dent_grav += (w[0] * g[0] + w[1] * g[1] + w[2] * g[2]) * dt_hydro;
+        }
+        const double du_tot = k->dudt[i] * dt_hydro + dent_grav;
+        const double dent = k->u[i] + du_tot;
+        k->u[i] = (dent < 0.5 * k->u[i]) ? 0.5 * k->u[i] : dent;
+        if (min_egy_spec != 0 && k->u[i] < min_egy_spec) {
+            k->u[i] = min_egy_spec;
+            k->dudt[i] = 0;
+        }
+
+        double dp[3];
+        const double *a = k->accel + 3 * (size_t)i;
+        for (int c = 0; c < 3; c++) {
+            dp[c] = 0;
+            dp[c] += g[c] * (mass_pred * dt_grav);
+            dp[c] += a[c] * (mass_pred * dt_hydro);
+        }
+        const double inv_mass = 1.0 / mass_new;
+        double *v = k->vel + 3 * (size_t)i;
+        for (int c = 0; c < 3; c++) v[c] += dp[c] * inv_mass;
+        if (k->mass[i] <= 0 || !isfinite(k->mass[i])) continue;
+        if (mode == 1) {
+            for (int c = 0; c < 3; c++) k->vel_pred[3 * (size_t)i + c] = v[c];
+            if (mfv) k->mass[i] = k->mass_true[i];
+            k->u_pred[i] = k->u[i];
+        }
+        for (int c = 0; c < 3; c++) k->dp[3 * (size_t)i + c] += dp[c];
+    }
+    return 0;
+}

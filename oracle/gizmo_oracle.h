@@ -94,6 +94,34 @@ int orc_neighbors(const gz_params *p, const orc_state *s, const int *active, int
                   int mode, orc_csr *out, int n_threads);
 void orc_csr_free(orc_csr *c);
 
+/* Half-step kick state (core/kicks.cc:284-545, do_the_kick), original
+ * order, FP64, row-major [n][k]. The MFV fields are ignored under MFM. */
+typedef struct orc_kick_state {
+    int n;
+    double *vel;        /* [n][3] P.Vel                          (in/out) */
+    double *u;          /* [n]    CellP.InternalEnergy           (in/out) */
+    double *mass;       /* [n]    P.Mass (MFV: MassTrue after the second half kick) (in/out) */
+    double *mass_true;  /* [n]    CellP.MassTrue (MFV)           (in/out) */
+    double *dmass;      /* [n]    CellP.dMass (MFV)              (in/out) */
+    double *dtmass;     /* [n]    CellP.DtMass (MFV) */
+    double *accel;      /* [n][3] CellP.HydroAccel */
+    double *dudt;       /* [n]    CellP.DtInternalEnergy (the temperature floor zeroes it) (in/out) */
+    double *grav;       /* [n][3] P.GravAccel */
+    double *gravwork;   /* [n][3] CellP.GravWorkTerm (MFV) */
+    double *vel_pred;   /* [n][3] CellP.VelPred           (out after the second half kick) */
+    double *u_pred;     /* [n]    CellP.InternalEnergyPred (out after the second half kick) */
+    double *dp;         /* [n][3] P.dp, the momentum kick accumulates here (in/out) */
+    long long *tstart;  /* [n]    integer time the half step starts */
+    long long *tend;    /* [n]    integer time it ends */
+    int *active;        /* [n]    TimeBinActive of the particle's bin (0/1) */
+} orc_kick_state;
+
+/* One half-step kick of every particle: mode 0 is the first half kick
+ * (kicks.cc:34-97), 1 the second (kicks.cc:99-182). `timebase` is
+ * All.Timebase_interval (physical time per integer tick), `min_egy_spec`
+ * All.MinEgySpec (0: no floor). Non-comoving, no dilation. Returns 0. */
+int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, double min_egy_spec);
+
 /* One-time timing helper for the CPU baseline: runs density (from the
  * given h seeds) -> gradients -> force on `n_active` targets and returns
  * wall seconds. */

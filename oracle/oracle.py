@@ -39,6 +39,39 @@ class OrcState(C.Structure):
     _fields_ = [("n", C.c_int)] + [(name, _ip if dt == np.int32 else _dp) for name, _, dt in STATE_FIELDS]
 
 
+KICK_FIELDS = [  # (name, components, dtype), the order of orc_kick_state
+    ("vel", 3, np.float64), ("u", 1, np.float64), ("mass", 1, np.float64), ("mass_true", 1, np.float64),
+    ("dmass", 1, np.float64), ("dtmass", 1, np.float64), ("accel", 3, np.float64), ("dudt", 1, np.float64),
+    ("grav", 3, np.float64), ("gravwork", 3, np.float64), ("vel_pred", 3, np.float64), ("u_pred", 1, np.float64),
+    ("dp", 3, np.float64), ("tstart", 1, np.int64), ("tend", 1, np.int64), ("active", 1, np.int32),
+]
+_CTYPE = {np.float64: _dp, np.int64: C.POINTER(C.c_longlong), np.int32: _ip}
+
+
+class OrcKickState(C.Structure):
+    _fields_ = [("n", C.c_int)] + [(name, _CTYPE[dt]) for name, _, dt in KICK_FIELDS]
+
+
+def new_kick_state(n: int, inputs: dict) -> dict:
+    """All kick arrays for n particles, zero except what `inputs` fills."""
+    st = {}
+    for name, k, dt in KICK_FIELDS:
+        st[name] = np.zeros((n,) if k == 1 else (n, k), dtype=dt)
+    for name, arr in inputs.items():
+        st[name][...] = arr
+    return st
+
+
+def _c_kick_state(st: dict) -> OrcKickState:
+    s = OrcKickState()
+    s.n = int(st["u"].shape[0])
+    for name, _, dt in KICK_FIELDS:
+        a = st[name]
+        assert a.flags["C_CONTIGUOUS"] and a.dtype == dt and a.shape[0] == s.n, name
+        setattr(s, name, a.ctypes.data_as(_CTYPE[dt]))
+    return s
+
+
 class OrcCsr(C.Structure):
     _fields_ = [("offsets", C.POINTER(C.c_longlong)), ("nbrs", _ip), ("n_rows", C.c_int)]
 
@@ -79,6 +112,9 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
         f.restype = C.c_int
     f = getattr(lib, f"{prefix}_density_sums")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, _dp, _dp, C.c_int]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_kick")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcKickState), C.c_int, C.c_double, C.c_double]
     f.restype = C.c_int
     f = getattr(lib, f"{prefix}_full_pass_seconds")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
@@ -163,6 +199,12 @@ class Oracle:
         if rc:
             raise RuntimeError(f"density_sums failed: {rc}")
         return acc, pv
+
+    def kick(self, st: dict, mode: int, timebase: float, min_egy_spec: float = 0.0) -> int:
+        """One half-step kick (mode 0 first, 1 second) of the kick state, in place."""
+        cs = _c_kick_state(st)
+        f = getattr(self.lib, f"{self.prefix}_kick")
+        return int(f(C.byref(self.params), C.byref(cs), int(mode), float(timebase), float(min_egy_spec)))
 
     def full_pass_seconds(self, st, active=None):
         a, na = self._act(active)
