@@ -91,11 +91,18 @@ class GzStatusInfo(C.Structure):
     ]
 
 
+class GzKickFields(C.Structure):
+    """gz_kick_fields: device pointers (as integers) of one half-step kick."""
+    _fields_ = [("n", C.c_int64)] + [(name, C.c_void_p) for name in (
+        "vel", "u", "mass", "mass_true", "dmass", "dtmass", "accel", "dudt", "grav", "gravwork", "vel_pred",
+        "u_pred", "dp", "tstart", "tend", "active")]
+
+
 EXPORTED_SYMBOLS = [
     "gz_create", "gz_destroy", "gz_set_params", "gz_set_diagnostics", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream", "gz_kernel_timing",
     "gz_kernel_time",
-    "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc",
+    "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
 ]
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS
@@ -136,6 +143,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_neighbors.argtypes = [vp, _ip, C.c_int, C.c_int, C.POINTER(C.c_int64), _ip]
     lib.gz_density_sums.argtypes = [vp, _ip, C.c_int, _dp, _dp]
     lib.gz_density_sums_noalloc.argtypes = [C.POINTER(GzParams), C.c_int, vp, vp, vp, vp, vp, vp, vp]
+    lib.gz_kick.argtypes = [C.POINTER(GzParams), C.POINTER(GzKickFields), C.c_int, C.c_double, C.c_double, vp]
     for name in EXPORTED_SYMBOLS:
         if name != "gz_stream":
             getattr(lib, name).restype = C.c_int

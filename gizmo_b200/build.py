@@ -29,6 +29,7 @@ UNITS = {
     "passes_fp64.cu": ["-fmad=false"],
     "passes_mixed.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noalloc.cu": ["-fmad=false"],
+    "kick.cu": ["-fmad=false"],
 }
 
 

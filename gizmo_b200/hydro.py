@@ -216,3 +216,40 @@ class HydroPass:
         if rc:
             st = self.status()
             raise GizmoHydroError(int(rc), st.get("message", ""))
+
+
+KICK_DTYPES = {name: "torch.float64" for name in (
+    "vel", "u", "mass", "mass_true", "dmass", "dtmass", "accel", "dudt", "grav", "gravwork", "vel_pred", "u_pred",
+    "dp")}
+KICK_DTYPES.update({"tstart": "torch.int64", "tend": "torch.int64", "active": "torch.int32"})
+KICK_VECTORS = ("vel", "accel", "grav", "gravwork", "vel_pred", "dp")
+
+
+def kick(params: abi.GzParams, fields: dict, mode: int, timebase: float, min_egy_spec: float = 0.0,
+         stream: int | None = None) -> None:
+    """One half-step kick of a particle set held in device memory, in place:
+    do_the_kick (src/core/kicks.cc:284-545) as do_first_halfstep_kick (mode 0)
+    and do_second_halfstep_kick (mode 1) apply it.
+
+    ``fields`` maps the gz_kick_fields names to contiguous CUDA tensors in the
+    caller's order ([n] or [n, 3]; FP64, ``tstart``/``tend`` int64, ``active``
+    int32); ``grav``, ``gravwork`` and ``active`` may be left out, and the MFV
+    fields under MFM. The work is queued on ``stream`` (a cudaStream_t handle,
+    None for the default stream) and this returns without waiting."""
+    n = int(fields["u"].shape[0])
+    f = abi.GzKickFields()
+    f.n = n
+    for name, dtype in KICK_DTYPES.items():
+        t = fields.get(name)
+        if t is None:
+            continue
+        rows = 3 if name in KICK_VECTORS else 1
+        if (not t.is_cuda or not t.is_contiguous() or int(t.shape[0]) != n or t.numel() != rows * n
+                or str(t.dtype) != dtype):
+            raise ValueError(f"kick field {name}: want a contiguous CUDA {dtype} tensor of shape "
+                             f"{(n, 3) if rows == 3 else (n,)}")
+        setattr(f, name, t.data_ptr())
+    rc = abi.load_library().gz_kick(C.byref(params), C.byref(f), int(mode), float(timebase), float(min_egy_spec),
+                                    stream)
+    if rc:
+        raise GizmoHydroError(rc, "gz_kick")

@@ -235,6 +235,42 @@ int gz_density_sums(gz_context *ctx, const int *active, int n_active, double *ac
 int gz_density_sums_noalloc(const gz_params *params, int n, const double *pos, const double *vel,
                             const double *mass, const double *h, double *acc, double *pv, void *stream);
 
+/* One half-step kick, do_the_kick (core/kicks.cc:284-545), for every
+ * particle of a set the caller holds in DEVICE memory (the reference's
+ * particle arena, structure of arrays): the loops of do_first_halfstep_kick
+ * (mode 0, kicks.cc:34-97) and do_second_halfstep_kick (mode 1,
+ * kicks.cc:99-182) over gas cells. Rows follow the caller's order; FP64
+ * row-major [n][k] like gz_particles. */
+typedef struct gz_kick_fields {
+    int64_t n;
+    double        *vel;        /* [n][3] P.Vel                                   in/out */
+    double        *u;          /* [n]    CellP.InternalEnergy                    in/out */
+    double        *mass;       /* [n]    P.Mass (MFV: MassTrue after mode 1)     in/out */
+    double        *mass_true;  /* [n]    CellP.MassTrue (MFV; NULL under MFM)    in/out */
+    double        *dmass;      /* [n]    CellP.dMass (MFV; NULL under MFM)       in/out */
+    const double  *dtmass;     /* [n]    CellP.DtMass (MFV; NULL under MFM) */
+    const double  *accel;      /* [n][3] CellP.HydroAccel */
+    double        *dudt;       /* [n]    CellP.DtInternalEnergy (the temperature floor zeroes it) in/out */
+    const double  *grav;       /* [n][3] P.GravAccel (NULL: zero) */
+    const double  *gravwork;   /* [n][3] CellP.GravWorkTerm (MFV; NULL: zero) */
+    double        *vel_pred;   /* [n][3] CellP.VelPred, written by mode 1 */
+    double        *u_pred;     /* [n]    CellP.InternalEnergyPred, written by mode 1 */
+    double        *dp;         /* [n][3] P.dp, the momentum kick is added    in/out */
+    const int64_t *tstart;     /* [n]    integer time the half step starts (Ti_begstep or its midpoint) */
+    const int64_t *tend;       /* [n]    integer time it ends */
+    const int32_t *active;     /* [n]    TimeBinActive[P.TimeBin] (NULL: all active) */
+} gz_kick_fields;
+
+/* Kicks every particle of `f` by one half step. `timebase` is
+ * All.Timebase_interval (physical time per integer tick, non-comoving, no
+ * timestep dilation) and `min_egy_spec` All.MinEgySpec (0: no floor). Work is
+ * queued on `stream` (a cudaStream_t, NULL for the default stream) and the
+ * call returns without waiting; it needs no gz_context and allocates
+ * nothing. Arithmetic is FP64 without contraction, bit-identical to the
+ * reference's expression order. */
+int gz_kick(const gz_params *params, const gz_kick_fields *f, int mode, double timebase, double min_egy_spec,
+            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,6 +83,24 @@ def test_bad_arguments_rejected_before_device_use():
     assert lib.gz_hydro_density(None, None, 0) == abi.ERR_ARG
 
 
+def test_kick_arguments_checked_before_device_use():
+    lib = abi.load_library()
+    from gizmo_b200 import ics
+    p = ics.sedov(4).params
+    f = abi.GzKickFields()
+    f.n = 0
+    assert lib.gz_kick(C.byref(p), C.byref(f), 0, 1e-12, 0.0, None) == abi.OK  # nothing to kick
+    assert lib.gz_kick(C.byref(p), C.byref(f), 2, 1e-12, 0.0, None) == abi.ERR_ARG  # no such half kick
+    assert lib.gz_kick(None, C.byref(f), 0, 1e-12, 0.0, None) == abi.ERR_ARG
+    assert lib.gz_kick(C.byref(p), C.byref(f), 0, -1.0, 0.0, None) == abi.ERR_ARG
+    f.n = 10
+    assert lib.gz_kick(C.byref(p), C.byref(f), 0, 1e-12, 0.0, None) == abi.ERR_ARG  # required fields missing
+    for name in ("vel", "u", "mass", "accel", "dudt", "vel_pred", "u_pred", "dp", "tstart", "tend"):
+        setattr(f, name, 16)  # never dereferenced: the MFV fields are still missing
+    p.method = abi.METHOD_MFV
+    assert lib.gz_kick(C.byref(p), C.byref(f), 0, 1e-12, 0.0, None) == abi.ERR_ARG
+
+
 def test_header_constants_match_the_python_mirror():
     src = open(HEADER).read()
     defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define\s+GZ_(\w+)\s+(-?\d+)", src, re.M)}
