@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(kKickBlock) k_kick(const KickArgs a)
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += stride) {
         const double mass = f.mass[i];
+        if (!(mass > 0)) continue;  // the kick loops skip these cells (kicks.cc:69, 153)
         const double mass_pred = mass;
         double mass_new = mass;
         const double dt = (double)(f.tend[i] - f.tstart[i]) * a.timebase;

@@ -239,8 +239,8 @@ int gz_density_sums_noalloc(const gz_params *params, int n, const double *pos, c
  * particle of a set the caller holds in DEVICE memory (the reference's
  * particle arena, structure of arrays): the loops of do_first_halfstep_kick
  * (mode 0, kicks.cc:34-97) and do_second_halfstep_kick (mode 1,
- * kicks.cc:99-182) over gas cells. Rows follow the caller's order; FP64
- * row-major [n][k] like gz_particles. */
+ * kicks.cc:99-182) over gas cells, which kick only cells with P.Mass > 0.
+ * Rows follow the caller's order; FP64 row-major [n][k] like gz_particles. */
 typedef struct gz_kick_fields {
     int64_t n;
     double        *vel;        /* [n][3] P.Vel                                   in/out */

@@ -1464,11 +1464,14 @@ double orc_full_pass_seconds(const gz_params *p, orc_state *s, const int *active
  *   mass check, predicted reset    kicks.cc:521-543
  * unit_integertime_in_physical is Timebase_interval (core/timestep_functions.h:43-46)
  * and the non-comoving gravkick factor is (time1 - time0) * Timebase_interval
- * (timestep_functions.h:203-206, 253-256). Vec3 updates are per component. */
+ * (timestep_functions.h:203-206, 253-256). Vec3 updates are per component.
+ * The loops of do_first/second_halfstep_kick (kicks.cc:59-77, 144-162) kick
+ * only particles with P.Mass > 0; so does this. */
 int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, double min_egy_spec)
 {
     const int mfv = p->method == GZ_METHOD_MFV;
     for (int i = 0; i < k->n; i++) {
+        if (!(k->mass[i] > 0)) continue; /* the loops call do_the_kick only then: kicks.cc:69, 153 */
         double mass_old, mass_pred, mass_new;
         mass_old = mass_pred = mass_new = k->mass[i];
         const long long span = k->tend[i] - k->tstart[i];

@@ -116,8 +116,9 @@ typedef struct orc_kick_state {
     int *active;        /* [n]    TimeBinActive of the particle's bin (0/1) */
 } orc_kick_state;
 
-/* One half-step kick of every particle: mode 0 is the first half kick
- * (kicks.cc:34-97), 1 the second (kicks.cc:99-182). `timebase` is
+/* One half-step kick of every particle with P.Mass > 0, as the kick loops
+ * select them: mode 0 is the first half kick (kicks.cc:34-97), 1 the second
+ * (kicks.cc:99-182). `timebase` is
  * All.Timebase_interval (physical time per integer tick), `min_egy_spec`
  * All.MinEgySpec (0: no floor). Non-comoving, no dilation. Returns 0. */
 int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, double min_egy_spec);
