@@ -39,53 +39,55 @@ __global__ void __launch_bounds__(kKickBlock) k_kick(const KickArgs a)
     const gz_kick_fields &f = a.f;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += stride) {
+        // Every input of the particle is loaded before the first branch on loaded data, so that
+        // all of its loads are in flight together; the branches below only choose what is stored.
         const double mass = f.mass[i];
+        const int64_t t0 = f.tstart[i], t1 = f.tend[i];
+        const int active = f.active ? f.active[i] : 1;
+        double mass_true = 0, dmass = 0, dtmass = 0;
+        if (a.mfv) {
+            mass_true = f.mass_true[i];
+            dmass = f.dmass[i];
+            dtmass = f.dtmass[i];
+        }
+        double g[3] = {0, 0, 0}, w[3] = {0, 0, 0}, acc[3], vel[3], dp_old[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (f.grav) g[c] = f.grav[3 * i + c];
+            if (a.mfv && f.gravwork) w[c] = f.gravwork[3 * i + c];
+            acc[c] = f.accel[3 * i + c];
+            vel[c] = f.vel[3 * i + c];
+            dp_old[c] = f.dp[3 * i + c];
+        }
+        const double u_old = f.u[i];
+        const double dudt = f.dudt[i];
+
         if (!(mass > 0)) continue;  // the kick loops skip these cells (kicks.cc:69, 153)
         const double mass_pred = mass;
         double mass_new = mass;
-        const double dt = (double)(f.tend[i] - f.tstart[i]) * a.timebase;
-        double mass_true = 0;
-        if (a.mfv) {
-            mass_true = f.mass_true[i];
-            double dmass = f.dmass[i];
-            if (dmass != 0) {
-                double dm;
-                if (a.mode != 0) {
-                    dm = dt * f.dtmass[i];
-                    if (dm * dmass < 0) dm = 0;
-                    if (fabs(dm) > fabs(dmass)) dm = dmass;
-                    dmass -= dm;
-                } else {
-                    dm = dmass;
-                    dmass = 0;
-                }
-                if (dm < -0.99 * mass_true) dm = -0.99 * mass_true;
-                mass_new = mass_true + dm;
-                mass_true = mass_new;
-                f.mass_true[i] = mass_true;
-                f.dmass[i] = dmass;
+        const double dt = (double)(t1 - t0) * a.timebase;
+        if (a.mfv && dmass != 0) {
+            double dm;
+            if (a.mode != 0) {
+                dm = dt * dtmass;
+                if (dm * dmass < 0) dm = 0;
+                if (fabs(dm) > fabs(dmass)) dm = dmass;
+                dmass -= dm;
+            } else {
+                dm = dmass;
+                dmass = 0;
             }
+            if (dm < -0.99 * mass_true) dm = -0.99 * mass_true;
+            mass_new = mass_true + dm;
+            mass_true = mass_new;
+            f.mass_true[i] = mass_true;
+            f.dmass[i] = dmass;
         }
-        if (f.active && !f.active[i]) continue;
+        if (!active) continue;
 
-        double g[3] = {0, 0, 0};
-        if (f.grav) {
-            g[0] = f.grav[3 * i];
-            g[1] = f.grav[3 * i + 1];
-            g[2] = f.grav[3 * i + 2];
-        }
         double dent_grav = 0;
-        if (a.mfv) {
-            double w[3] = {0, 0, 0};
-            if (f.gravwork) {
-                w[0] = f.gravwork[3 * i];
-                w[1] = f.gravwork[3 * i + 1];
-                w[2] = f.gravwork[3 * i + 2];
-            }
-            dent_grav += (w[0] * g[0] + w[1] * g[1] + w[2] * g[2]) * dt;
-        }
-        const double u_old = f.u[i];
-        const double du_tot = f.dudt[i] * dt + dent_grav;
+        if (a.mfv) dent_grav += (w[0] * g[0] + w[1] * g[1] + w[2] * g[2]) * dt;
+        const double du_tot = dudt * dt + dent_grav;
         const double dent = u_old + du_tot;
         double u = (dent < 0.5 * u_old) ? 0.5 * u_old : dent;
         if (a.min_egy_spec != 0 && u < a.min_egy_spec) {
@@ -100,8 +102,8 @@ __global__ void __launch_bounds__(kKickBlock) k_kick(const KickArgs a)
         for (int c = 0; c < 3; c++) {
             dp[c] = 0;
             dp[c] += g[c] * (mass_pred * dt);
-            dp[c] += f.accel[3 * i + c] * (mass_pred * dt);
-            v[c] = f.vel[3 * i + c] + dp[c] * inv_mass;
+            dp[c] += acc[c] * (mass_pred * dt);
+            v[c] = vel[c] + dp[c] * inv_mass;
             f.vel[3 * i + c] = v[c];
         }
         if (mass <= 0 || !isfinite(mass)) continue;
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(kKickBlock) k_kick(const KickArgs a)
             f.u_pred[i] = u;
         }
 #pragma unroll
-        for (int c = 0; c < 3; c++) f.dp[3 * i + c] += dp[c];
+        for (int c = 0; c < 3; c++) f.dp[3 * i + c] = dp_old[c] + dp[c];
     }
 }
 
