@@ -28,6 +28,7 @@ ERR_INTERNAL = 6
 ERR_DENSITY_MAXITER = 1155
 ERR_EMPTY_BRACKET = 90001009
 ERR_RIEMANN = 1234
+ERR_NO_PAST_DRIFT = 90001004
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

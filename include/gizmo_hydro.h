@@ -57,6 +57,7 @@ extern "C" {
 #define GZ_ERR_DENSITY_MAXITER  1155    /* neighbor_loop_runner.cc:7485 endrun(1155) */
 #define GZ_ERR_EMPTY_BRACKET    90001009 /* density_loop.h:891-895 */
 #define GZ_ERR_RIEMANN          1234    /* hydro_core_meshless_functions.h:403-425 */
+#define GZ_ERR_NO_PAST_DRIFT    90001004 /* drift_particle_functions.h:90-95: a drift into the past */
 
 /* Run-time configuration: the All.* fields and compile-time flags the pass
  * reads. Non-cosmological (cf_atime = 1, ComovingIntegrationOn = 0). */

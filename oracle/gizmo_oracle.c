@@ -1530,3 +1530,65 @@ int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, d
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------- drift */
+/* drift_particle_impl (core/drift_particle_functions.h:86-260) for gas cells
+ * of the configuration above, HYDRO_FIX_MESH_MOTION = 5 (declarations/
+ * precompiler_logic.h:78), no timestep dilation, no special boundaries:
+ *   time checks                         drift_particle_functions.h:90-97
+ *   position step: MFV with ParticleVel (advect_mesh_point_body, core/
+ *     timestep_functions.h:979), MFM with Vel (particle_drift_velocity,
+ *     drift_straight_displacement, timestep_functions.h:649-652)
+ *   capped log change, radius factor    timestep_functions.h:312, 323-335
+ *   VelPred, MFV mass (mfv_drifted_mass, timestep_functions.h:993-996),
+ *   density, InternalEnergyPred with internal_energy_positivity_catch
+ *   (core/proto.h:417-421) and the MinEgySpec floor, kernel radius and its
+ *   clamps                              drift_particle_functions.h:158-233
+ *   ideal-gas pressure (gamma - 1) u rho  eos/eos_functions.h:873 (set_eos_pressure_impl)
+ * The drift factor, the gravkick factor and the hydro kick time are all
+ * (time1 - time0) * Timebase_interval here (timestep_functions.h:43-46, 203-206). */
+int orc_drift(const gz_params *p, orc_drift_state *d, long long time1, double timebase, double min_egy_spec)
+{
+    const int mfv = p->method == GZ_METHOD_MFV;
+    int code = 0;
+    for (int i = 0; i < d->n; i++) {
+        const long long time0 = d->ti_current[i];
+        if (time1 < time0) {
+            if (!code) code = GZ_ERR_NO_PAST_DRIFT;
+            continue;
+        }
+        if (time1 == time0) continue;
+        const double dt_drift = (double)(time1 - time0) * timebase;
+        double *x = d->pos + 3 * (size_t)i;
+        const double *w = mfv ? d->pvel + 3 * (size_t)i : d->vel + 3 * (size_t)i;
+        for (int c = 0; c < 3; c++) x[c] += w[c] * dt_drift;
+
+        double lc = d->divvel[i] * dt_drift;
+        if (lc > 0.3) lc = 0.3;
+        if (lc < -0.3) lc = -0.3;
+        const double h_fac = exp(lc / 3.0);
+
+        if (d->mass[i] > 0) {
+            const double dt_entr = (double)(time1 - time0) * timebase;
+            double *vp = d->vel_pred + 3 * (size_t)i;
+            const double *g = d->grav + 3 * (size_t)i;
+            const double *a = d->accel + 3 * (size_t)i;
+            for (int c = 0; c < 3; c++) vp[c] += g[c] * dt_drift + a[c] * dt_entr;
+            if (mfv) {
+                const double m = d->mass[i] + d->dtmass[i] * dt_entr;
+                const double lo = 0.5 * d->mass_true[i];
+                d->mass[i] = m > lo ? m : lo;
+            }
+            d->rho[i] *= exp(-lc);
+            const double etmp = d->u_pred[i] + d->dudt[i] * dt_entr;
+            d->u_pred[i] = (etmp < 0.5 * d->u_pred[i]) ? 0.5 * d->u_pred[i] : etmp;
+            if (d->u_pred[i] < min_egy_spec) d->u_pred[i] = min_egy_spec;
+            d->h[i] *= h_fac;
+            if (d->h[i] < p->min_kernel_radius) d->h[i] = p->min_kernel_radius;
+            if (d->h[i] > p->max_kernel_radius) d->h[i] = p->max_kernel_radius;
+            d->pressure[i] = (p->gamma - 1) * d->u_pred[i] * d->rho[i];
+        }
+        d->ti_current[i] = time1;
+    }
+    return code;
+}

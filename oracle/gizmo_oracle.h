@@ -123,6 +123,37 @@ typedef struct orc_kick_state {
  * All.MinEgySpec (0: no floor). Non-comoving, no dilation. Returns 0. */
 int orc_kick(const gz_params *p, orc_kick_state *k, int mode, double timebase, double min_egy_spec);
 
+/* Drift state (core/drift_particle_functions.h:86-260, drift_particle_impl),
+ * original order, FP64, row-major [n][k]. The MFV fields are ignored under
+ * MFM, `vel` under MFV. */
+typedef struct orc_drift_state {
+    int n;
+    double *pos;        /* [n][3] P.Pos                                  (in/out) */
+    double *vel;        /* [n][3] P.Vel: an MFM cell moves with it */
+    double *pvel;       /* [n][3] CellP.ParticleVel: an MFV cell moves with it */
+    double *vel_pred;   /* [n][3] CellP.VelPred                          (in/out) */
+    double *grav;       /* [n][3] P.GravAccel */
+    double *accel;      /* [n][3] CellP.HydroAccel */
+    double *divvel;     /* [n]    P.Particle_DivVel */
+    double *mass;       /* [n]    P.Mass (MFV: the drifted mass)         (in/out) */
+    double *dtmass;     /* [n]    CellP.DtMass (MFV) */
+    double *mass_true;  /* [n]    CellP.MassTrue (MFV) */
+    double *rho;        /* [n]    CellP.Density                          (in/out) */
+    double *u_pred;     /* [n]    CellP.InternalEnergyPred               (in/out) */
+    double *dudt;       /* [n]    CellP.DtInternalEnergy */
+    double *h;          /* [n]    P.KernelRadius                         (in/out) */
+    double *pressure;   /* [n]    CellP.Pressure                         (out for drifted cells) */
+    long long *ti_current; /* [n] P.Ti_current, set to time1             (in/out) */
+} orc_drift_state;
+
+/* Drifts every gas cell from its Ti_current to the integer time `time1`
+ * (drift_particle_impl; non-comoving, no dilation, ideal gas). `timebase` is
+ * All.Timebase_interval, `min_egy_spec` All.MinEgySpec; the kernel-radius
+ * bounds and gamma come from p. Returns 0, or 90001004 (the reference's
+ * stop code) when a cell's Ti_current lies after time1; that cell is left
+ * as it was. */
+int orc_drift(const gz_params *p, orc_drift_state *d, long long time1, double timebase, double min_egy_spec);
+
 /* One-time timing helper for the CPU baseline: runs density (from the
  * given h seeds) -> gradients -> force on `n_active` targets and returns
  * wall seconds. */

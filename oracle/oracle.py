@@ -72,6 +72,38 @@ def _c_kick_state(st: dict) -> OrcKickState:
     return s
 
 
+DRIFT_FIELDS = [  # (name, components, dtype), the order of orc_drift_state
+    ("pos", 3, np.float64), ("vel", 3, np.float64), ("pvel", 3, np.float64), ("vel_pred", 3, np.float64),
+    ("grav", 3, np.float64), ("accel", 3, np.float64), ("divvel", 1, np.float64), ("mass", 1, np.float64),
+    ("dtmass", 1, np.float64), ("mass_true", 1, np.float64), ("rho", 1, np.float64), ("u_pred", 1, np.float64),
+    ("dudt", 1, np.float64), ("h", 1, np.float64), ("pressure", 1, np.float64), ("ti_current", 1, np.int64),
+]
+
+
+class OrcDriftState(C.Structure):
+    _fields_ = [("n", C.c_int)] + [(name, _CTYPE[dt]) for name, _, dt in DRIFT_FIELDS]
+
+
+def new_drift_state(n: int, inputs: dict) -> dict:
+    """All drift arrays for n particles, zero except what `inputs` fills."""
+    st = {}
+    for name, k, dt in DRIFT_FIELDS:
+        st[name] = np.zeros((n,) if k == 1 else (n, k), dtype=dt)
+    for name, arr in inputs.items():
+        st[name][...] = arr
+    return st
+
+
+def _c_drift_state(st: dict) -> OrcDriftState:
+    s = OrcDriftState()
+    s.n = int(st["mass"].shape[0])
+    for name, _, dt in DRIFT_FIELDS:
+        a = st[name]
+        assert a.flags["C_CONTIGUOUS"] and a.dtype == dt and a.shape[0] == s.n, name
+        setattr(s, name, a.ctypes.data_as(_CTYPE[dt]))
+    return s
+
+
 class OrcCsr(C.Structure):
     _fields_ = [("offsets", C.POINTER(C.c_longlong)), ("nbrs", _ip), ("n_rows", C.c_int)]
 
@@ -115,6 +147,9 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
     f.restype = C.c_int
     f = getattr(lib, f"{prefix}_kick")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcKickState), C.c_int, C.c_double, C.c_double]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_drift")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcDriftState), C.c_longlong, C.c_double, C.c_double]
     f.restype = C.c_int
     f = getattr(lib, f"{prefix}_full_pass_seconds")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
@@ -205,6 +240,12 @@ class Oracle:
         cs = _c_kick_state(st)
         f = getattr(self.lib, f"{self.prefix}_kick")
         return int(f(C.byref(self.params), C.byref(cs), int(mode), float(timebase), float(min_egy_spec)))
+
+    def drift(self, st: dict, time1: int, timebase: float, min_egy_spec: float = 0.0) -> int:
+        """Drift every cell of the drift state to the integer time `time1`, in place."""
+        cs = _c_drift_state(st)
+        f = getattr(self.lib, f"{self.prefix}_drift")
+        return int(f(C.byref(self.params), C.byref(cs), int(time1), float(timebase), float(min_egy_spec)))
 
     def full_pass_seconds(self, st, active=None):
         a, na = self._act(active)
