@@ -99,11 +99,19 @@ class GzKickFields(C.Structure):
         "u_pred", "dp", "tstart", "tend", "active")]
 
 
+class GzDriftFields(C.Structure):
+    """gz_drift_fields: device pointers (as integers) of one drift."""
+    _fields_ = [("n", C.c_int64)] + [(name, C.c_void_p) for name in (
+        "pos", "vel", "pvel", "vel_pred", "grav", "accel", "divvel", "mass", "dtmass", "mass_true", "rho", "u_pred",
+        "dudt", "h", "pressure", "ti_current", "status")]
+
+
 EXPORTED_SYMBOLS = [
     "gz_create", "gz_destroy", "gz_set_params", "gz_set_diagnostics", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream", "gz_kernel_timing",
     "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
+    "gz_drift",
 ]
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS
@@ -145,6 +153,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_density_sums.argtypes = [vp, _ip, C.c_int, _dp, _dp]
     lib.gz_density_sums_noalloc.argtypes = [C.POINTER(GzParams), C.c_int, vp, vp, vp, vp, vp, vp, vp]
     lib.gz_kick.argtypes = [C.POINTER(GzParams), C.POINTER(GzKickFields), C.c_int, C.c_double, C.c_double, vp]
+    lib.gz_drift.argtypes = [C.POINTER(GzParams), C.POINTER(GzDriftFields), C.c_int64, C.c_double, C.c_double,
+                             vp]
     for name in EXPORTED_SYMBOLS:
         if name != "gz_stream":
             getattr(lib, name).restype = C.c_int

@@ -30,6 +30,7 @@ UNITS = {
     "passes_mixed.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noalloc.cu": ["-fmad=false"],
     "kick.cu": ["-fmad=false"],
+    "drift.cu": ["-fmad=false"],
 }
 
 

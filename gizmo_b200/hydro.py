@@ -253,3 +253,42 @@ def kick(params: abi.GzParams, fields: dict, mode: int, timebase: float, min_egy
                                     stream)
     if rc:
         raise GizmoHydroError(rc, "gz_kick")
+
+
+DRIFT_DTYPES = {name: "torch.float64" for name in (
+    "pos", "vel", "pvel", "vel_pred", "grav", "accel", "divvel", "mass", "dtmass", "mass_true", "rho", "u_pred",
+    "dudt", "h", "pressure")}
+DRIFT_DTYPES.update({"ti_current": "torch.int64", "status": "torch.int32"})
+DRIFT_VECTORS = ("pos", "vel", "pvel", "vel_pred", "grav", "accel")
+
+
+def drift(params: abi.GzParams, fields: dict, time1: int, timebase: float, min_egy_spec: float = 0.0,
+          stream: int | None = None) -> None:
+    """Drift a particle set held in device memory to the integer time
+    ``time1``, in place: drift_particle_impl
+    (src/core/drift_particle_functions.h:86-260) for every gas cell, as
+    move_particles (src/core/predict.cc:171) applies it.
+
+    ``fields`` maps the gz_drift_fields names to contiguous CUDA tensors in the
+    caller's order ([n] or [n, 3]; FP64, ``ti_current`` int64); ``status`` is a
+    one-element int32 CUDA tensor that receives GZ_ERR_NO_PAST_DRIFT (90001004)
+    if a cell's Ti_current lies after ``time1`` (that cell is left as it was).
+    ``grav`` may be left out, the MFV fields under MFM, ``vel`` under MFV and
+    ``pvel`` under MFM. Queued on ``stream`` without waiting."""
+    n = int(fields["mass"].shape[0])
+    f = abi.GzDriftFields()
+    f.n = n
+    for name, dtype in DRIFT_DTYPES.items():
+        t = fields.get(name)
+        if t is None:
+            continue
+        rows = 3 if name in DRIFT_VECTORS else 1
+        want = 1 if name == "status" else rows * n
+        if (not t.is_cuda or not t.is_contiguous() or t.numel() != want or str(t.dtype) != dtype
+                or (name != "status" and int(t.shape[0]) != n)):
+            raise ValueError(f"drift field {name}: want a contiguous CUDA {dtype} tensor of {want} elements")
+        setattr(f, name, t.data_ptr())
+    rc = abi.load_library().gz_drift(C.byref(params), C.byref(f), int(time1), float(timebase), float(min_egy_spec),
+                                     stream)
+    if rc:
+        raise GizmoHydroError(rc, "gz_drift")

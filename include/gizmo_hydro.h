@@ -272,6 +272,44 @@ typedef struct gz_kick_fields {
 int gz_kick(const gz_params *params, const gz_kick_fields *f, int mode, double timebase, double min_egy_spec,
             void *stream);
 
+/* The drift, drift_particle_impl (core/drift_particle_functions.h:86-260),
+ * of every gas cell of a set the caller holds in DEVICE memory, from its
+ * Ti_current to the integer time `time1`, as move_particles
+ * (core/predict.cc:171) drifts them. Rows follow the caller's order; FP64 row-major [n][k]. Positions
+ * are not wrapped into the box, as in the reference. */
+typedef struct gz_drift_fields {
+    int64_t n;
+    double        *pos;        /* [n][3] P.Pos                                          in/out */
+    const double  *vel;        /* [n][3] P.Vel: an MFM cell moves with it (unused under MFV) */
+    const double  *pvel;       /* [n][3] CellP.ParticleVel: an MFV cell moves with it (unused under MFM) */
+    double        *vel_pred;   /* [n][3] CellP.VelPred                                  in/out */
+    const double  *grav;       /* [n][3] P.GravAccel (NULL: zero) */
+    const double  *accel;      /* [n][3] CellP.HydroAccel */
+    const double  *divvel;     /* [n]    P.Particle_DivVel */
+    double        *mass;       /* [n]    P.Mass (MFV: the drifted mass)                 in/out */
+    const double  *dtmass;     /* [n]    CellP.DtMass (MFV; NULL under MFM) */
+    const double  *mass_true;  /* [n]    CellP.MassTrue (MFV; NULL under MFM) */
+    double        *rho;        /* [n]    CellP.Density                                  in/out */
+    double        *u_pred;     /* [n]    CellP.InternalEnergyPred                       in/out */
+    const double  *dudt;       /* [n]    CellP.DtInternalEnergy */
+    double        *h;          /* [n]    P.KernelRadius                                 in/out */
+    double        *pressure;   /* [n]    CellP.Pressure (ideal gas), written for drifted cells */
+    int64_t       *ti_current; /* [n]    P.Ti_current, set to time1                     in/out */
+    int32_t       *status;     /* [1]    device word: a cell whose Ti_current lies after time1 is left as
+                                  it was and GZ_ERR_NO_PAST_DRIFT is written here unless a code
+                                  is already there (the kernel never clears it) */
+} gz_drift_fields;
+
+/* Drifts every cell of `f` to `time1`. `timebase` is All.Timebase_interval
+ * (non-comoving, no timestep dilation), `min_egy_spec` All.MinEgySpec; the
+ * kernel-radius bounds and gamma come from `params`. Queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) without waiting; no context, no
+ * allocation. FP64 without contraction; the two exponentials are correctly
+ * rounded, so results match the reference bit for bit except where its
+ * libm exp misrounds (within one ulp). */
+int gz_drift(const gz_params *params, const gz_drift_fields *f, int64_t time1, double timebase, double min_egy_spec,
+             void *stream);
+
 #ifdef __cplusplus
 }
 #endif

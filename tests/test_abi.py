@@ -101,6 +101,24 @@ def test_kick_arguments_checked_before_device_use():
     assert lib.gz_kick(C.byref(p), C.byref(f), 0, 1e-12, 0.0, None) == abi.ERR_ARG
 
 
+def test_drift_arguments_checked_before_device_use():
+    lib = abi.load_library()
+    from gizmo_b200 import ics
+    p = ics.sedov(4).params
+    f = abi.GzDriftFields()
+    f.n = 0
+    assert lib.gz_drift(C.byref(p), C.byref(f), 10, 1e-12, 0.0, None) == abi.OK  # nothing to drift
+    assert lib.gz_drift(None, C.byref(f), 10, 1e-12, 0.0, None) == abi.ERR_ARG
+    assert lib.gz_drift(C.byref(p), C.byref(f), 10, float("nan"), 0.0, None) == abi.ERR_ARG
+    f.n = 10
+    assert lib.gz_drift(C.byref(p), C.byref(f), 10, 1e-12, 0.0, None) == abi.ERR_ARG  # required fields missing
+    for name in ("pos", "vel", "vel_pred", "accel", "divvel", "mass", "rho", "u_pred", "dudt", "h", "pressure",
+                 "ti_current", "status"):
+        setattr(f, name, 16)  # never dereferenced: what is missing is caught first
+    p.method = abi.METHOD_MFV
+    assert lib.gz_drift(C.byref(p), C.byref(f), 10, 1e-12, 0.0, None) == abi.ERR_ARG  # MFV moves with pvel
+
+
 def test_header_constants_match_the_python_mirror():
     src = open(HEADER).read()
     defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define\s+GZ_(\w+)\s+(-?\d+)", src, re.M)}

@@ -1,0 +1,96 @@
+"""gz_drift, the drift on the device, against the oracle's orc_drift (itself
+pinned bit-exact to the reference's drift_particle_impl). Every field is
+bit-exact except the two that pass through an exponential, the density and
+the kernel radius, and the pressure computed from the density: the device's
+exp is correctly rounded, the oracle's is the C library's, which misrounds
+rare hard cases, so those agree within 1 ulp (pressure, one product more:
+2 ulp). Cases: the constructed ones that reach every cap, clamp and floor, a
+set of 4M cells (many grid-stride rounds), a drift into the past, and the
+optional fields left out."""
+import numpy as np
+import pytest
+
+from gizmo_b200 import abi, hydro, ics
+from gizmo_b200.abi import METHOD_MFM, METHOD_MFV
+from oracle import oracle as O
+from tests.test_oracle_drift import TIMEBASE, _constructed
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+ULP = {"rho": 1, "h": 1, "pressure": 2}  # fields through exp: see the module docstring
+
+
+def _params(method):
+    p = ics.sedov(4, seed=1).params
+    p.method = method
+    p.min_kernel_radius, p.max_kernel_radius = 0.05, 0.5
+    return p
+
+
+def _device_drift(params, ds, time1, floor, drop=()):
+    dev = {k: torch.from_numpy(v.copy()).cuda() for k, v in ds.items() if k not in drop}
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hydro.drift(params, dict(dev, status=status), time1, TIMEBASE, floor)
+    torch.cuda.synchronize()
+    out = {k: v.cpu().numpy() for k, v in dev.items()}
+    for k in drop:
+        out[k] = ds[k].copy()
+    return out, int(status.item())
+
+
+def _oracle_drift(params, ds, time1, floor):
+    s = {k: v.copy() for k, v in ds.items()}
+    code = O.Oracle(params, "port").drift(s, time1, TIMEBASE, floor)
+    return s, code
+
+
+def _assert_close(got, want):
+    for name, _, _ in O.DRIFT_FIELDS:
+        if name in ULP:
+            np.testing.assert_array_max_ulp(got[name], want[name], maxulp=ULP[name])
+        else:
+            np.testing.assert_array_equal(got[name], want[name], err_msg=name)
+
+
+@pytest.mark.parametrize("method", [METHOD_MFM, METHOD_MFV], ids=["mfm", "mfv"])
+@pytest.mark.parametrize("floor", [0.0, 3.0])
+def test_device_drift_constructed_cases(method, floor):
+    params = _params(method)
+    ds, time1 = _constructed(4096, 200 + method, params)
+    got, status = _device_drift(params, ds, time1, floor)
+    want, code = _oracle_drift(params, ds, time1, floor)
+    assert status == code == 0
+    _assert_close(got, want)
+
+
+@pytest.mark.parametrize("method", [METHOD_MFM, METHOD_MFV], ids=["mfm", "mfv"])
+def test_device_drift_large_set(method):
+    params = _params(method)
+    ds, time1 = _constructed((1 << 22) + 5, 31 + method, params)
+    got, status = _device_drift(params, ds, time1, 0.0)
+    want, code = _oracle_drift(params, ds, time1, 0.0)
+    assert status == code == 0
+    _assert_close(got, want)
+
+
+def test_device_drift_into_the_past_sets_the_status():
+    params = _params(METHOD_MFV)
+    ds, time1 = _constructed(1000, 9, params)
+    ds["ti_current"][[5, 700]] = time1 + 3
+    got, status = _device_drift(params, ds, time1, 0.0)
+    want, code = _oracle_drift(params, ds, time1, 0.0)
+    assert status == code == abi.ERR_NO_PAST_DRIFT
+    _assert_close(got, want)
+
+
+def test_device_drift_optional_fields_left_out():
+    """No gravity, and each method without the other's fields: the same as zero gravity."""
+    for method, drop in ((METHOD_MFV, ("grav", "vel")), (METHOD_MFM, ("grav", "pvel", "dtmass", "mass_true"))):
+        params = _params(method)
+        ds, time1 = _constructed(3000, 40 + method, params)
+        ds["grav"][...] = 0.0
+        got, status = _device_drift(params, ds, time1, 0.0, drop=drop)
+        want, code = _oracle_drift(params, ds, time1, 0.0)
+        assert status == code == 0
+        _assert_close(got, want)
