@@ -1,12 +1,14 @@
 """gz_drift, the drift on the device, against the oracle's orc_drift (itself
 pinned bit-exact to the reference's drift_particle_impl). Every field is
-bit-exact except the two that pass through an exponential, the density and
-the kernel radius, and the pressure computed from the density: the device's
-exp is correctly rounded, the oracle's is the C library's, which misrounds
-rare hard cases, so those agree within 1 ulp (pressure, one product more:
-2 ulp). Cases: the constructed ones that reach every cap, clamp and floor, a
-set of 4M cells (many grid-stride rounds), a drift into the past, and the
-optional fields left out."""
+bit-exact except three. The density and the kernel radius are products with
+an exponential. The device's exp is correctly rounded; the oracle's is the C
+library's, which is off by one ulp on ~0.05% of these inputs. A factor one ulp
+off moves the exact product by at most 2^-52 of itself, at most 2 ulp of the
+product, and the two rounded products stay within 2 ulp. The pressure
+multiplies such a density, so a relative gap of up to 2^-51 in its exact
+value: within 4 ulp. Cases: the constructed ones that reach every cap, clamp
+and floor, a set of 4M cells (many grid-stride rounds), a drift into the
+past, and the optional fields left out."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,7 @@ from tests.test_oracle_drift import TIMEBASE, _constructed
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-ULP = {"rho": 1, "h": 1, "pressure": 2}  # fields through exp: see the module docstring
+ULP = {"rho": 2, "h": 2, "pressure": 4}  # fields through exp: bounds derived in the module docstring
 
 
 def _params(method):
