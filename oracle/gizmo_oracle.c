@@ -1592,3 +1592,99 @@ int orc_drift(const gz_params *p, orc_drift_state *d, long long time1, double ti
     }
     return code;
 }
+
+/* ---------------------------------------------------------------- timestep */
+#define ORC_TIMEBINS 60
+#define ORC_TIMEBASE (((long long)1) << ORC_TIMEBINS) /* declarations/typedefs.h:8-9 */
+
+/* get_timestep_bin (core/timestep.cc:1525-1545): the bin whose integer step is ti_step. */
+static int orc_timestep_bin(long long ti_step)
+{
+    if (ti_step == 0) return 0;
+    int bin = -1;
+    while (ti_step) {
+        bin++;
+        ti_step >>= 1;
+    }
+    return bin;
+}
+
+/* get_timestep (core/timestep.cc:357-1416) as it compiles for gas cells of
+ * this configuration: cf_a2inv = cf_atime = cf_hubble_a = 1, no PM, no
+ * dilation, STOP_WHEN_BELOW_MINTIMESTEP, dt_displacement = MaxSizeTimestep
+ * (find_dt_displacement_constraint, timestep.cc:1425-1434, non-comoving):
+ *   acceleration criterion   :421-487 (KERNEL_CORE_SIZE 1/2)
+ *   Courant criterion         :711-729 (Get_Particle_Size, declarations/particle_data.h:461-469)
+ *   divergence criterion      :1093-1098
+ *   caps, floor, integer step :1334-1414
+ * then the per-particle binning of find_timesteps (:176-215, 265-270): a power
+ * of two below the wanted step, a larger bin only where it is synchronised. */
+int orc_timestep(const gz_params *p, const orc_timestep_params *tp, orc_timestep_state *t)
+{
+    (void)p;
+    int code = 0;
+    const double tb = tp->timebase;
+    for (int i = 0; i < t->n; i++) {
+        const double *g = t->grav + 3 * (size_t)i;
+        const double *a = t->accel + 3 * (size_t)i;
+        double ax = 1.0 * g[0], ay = 1.0 * g[1], az = 1.0 * g[2];
+        ax += a[0];
+        ay += a[1];
+        az += a[2];
+        double ac = sqrt(ax * ax + ay * ay + az * az);
+        t->aphys[i] = ac;
+        if (ac == 0) ac = 1.0e-30;
+        double h_acc = (1.0 / 2.0) * t->softening[i];
+        if (h_acc <= 0) h_acc = (1.61199 * t->h[i] / t->num_ngb[i]) * 1.0;
+        double dt = sqrt(2 * tp->err_tol_int_accuracy * 1.0 * h_acc / ac);
+        if (t->mass[i] > 0) {
+            const double csnd = 0.5 * t->vsig[i];
+            const double L = 1.61199 * t->h[i] / t->num_ngb[i];
+            const double dt_courant = tp->courant_fac * (L * 1.0) / csnd;
+            if (dt_courant < dt) dt = dt_courant;
+            const double divv = t->divvel[i];
+            if (divv != 0) {
+                const double dt_divv = 1.5 / fabs(1.0 * divv);
+                if (dt_divv < dt) dt = dt_divv;
+            }
+        }
+        dt *= 1.0;
+        if (dt >= tp->max_size_timestep) dt = tp->max_size_timestep;
+        if (dt >= tp->max_size_timestep) dt = tp->max_size_timestep; /* dt_displacement */
+        if ((dt < tp->min_size_timestep) || !(dt / tb >= 2.0)) {
+            if (t->mass[i] > 0 && !code) code = 888;
+            dt = tp->min_size_timestep;
+        }
+        if (dt > 0.5 * ORC_TIMEBASE * tb) dt = 0.5 * ORC_TIMEBASE * tb;
+        long long ti_step = (long long)(dt / tb);
+        if (ti_step <= 1) ti_step = 2;
+        if (!(ti_step > 0 && ti_step < ORC_TIMEBASE)) ti_step = 2;
+        t->ti_want[i] = ti_step;
+
+        ti_step = (long long)(((double)ti_step) / 1.0);
+        long long ti_min = ORC_TIMEBASE;
+        while (ti_min > ti_step) ti_min >>= 1;
+        ti_step = ti_min;
+        int bin = orc_timestep_bin(ti_step);
+        const int binold = t->bin[i];
+        if (bin > binold) {
+            while (tp->bin_active[bin] == 0 && bin > binold) bin--;
+            ti_step = bin ? ((long long)1 << bin) : 0;
+        }
+        if (tp->ti_current >= ORC_TIMEBASE) {
+            ti_step = 0;
+            bin = 0;
+        }
+        if ((ORC_TIMEBASE - tp->ti_current) < ti_step) {
+            if (!code) code = 90001005;
+            ti_step = ORC_TIMEBASE - tp->ti_current;
+            ti_min = ORC_TIMEBASE;
+            while (ti_min > ti_step) ti_min >>= 1;
+            ti_step = ti_min;
+        }
+        t->bin[i] = bin;
+        t->ti_begstep[i] += t->dt_step[i];
+        t->dt_step[i] = ti_step;
+    }
+    return code;
+}

@@ -154,6 +154,42 @@ typedef struct orc_drift_state {
  * as it was. */
 int orc_drift(const gz_params *p, orc_drift_state *d, long long time1, double timebase, double min_egy_spec);
 
+/* Timestep state of gas cells (core/timestep.cc:357-1416 get_timestep, and
+ * the per-particle binning of find_timesteps, timestep.cc:176-270),
+ * original order. */
+typedef struct orc_timestep_state {
+    int n;
+    double *grav;        /* [n][3] P.GravAccel */
+    double *accel;       /* [n][3] CellP.HydroAccel */
+    double *vsig;        /* [n]    CellP.MaxSignalVel */
+    double *h;           /* [n]    P.KernelRadius */
+    double *num_ngb;     /* [n]    P.NumNgb (after the ^(1/3) transform) */
+    double *divvel;      /* [n]    P.Particle_DivVel */
+    double *mass;        /* [n]    P.Mass */
+    double *softening;   /* [n]    P.ForceSoftening (ForceSoftening_KernelRadius) */
+    double *aphys;       /* [n]    out: the physical acceleration get_timestep returns through aphys */
+    long long *ti_want;  /* [n]    out: get_timestep's integer step, before the binning */
+    int *bin;            /* [n]    P.TimeBin                              (in/out) */
+    long long *ti_begstep; /* [n]  P.Ti_begstep                           (in/out) */
+    long long *dt_step;  /* [n]    P.dt_step                              (in/out) */
+} orc_timestep_state;
+
+typedef struct orc_timestep_params {
+    double err_tol_int_accuracy;  /* All.ErrTolIntAccuracy */
+    double courant_fac;           /* All.CourantFac */
+    double max_size_timestep;     /* All.MaxSizeTimestep */
+    double min_size_timestep;     /* All.MinSizeTimestep */
+    double timebase;              /* All.Timebase_interval */
+    long long ti_current;         /* All.Ti_Current */
+    int bin_active[60];           /* TimeBinActive[TIMEBINS] */
+} orc_timestep_params;
+
+/* New timesteps of every gas cell (all taken as active), non-comoving, no
+ * dilation. Returns 0, or the first stop code: 888 (a step below
+ * MinSizeTimestep, STOP_WHEN_BELOW_MINTIMESTEP), 90001005 (beyond the end of
+ * the timeline). */
+int orc_timestep(const gz_params *p, const orc_timestep_params *tp, orc_timestep_state *t);
+
 /* One-time timing helper for the CPU baseline: runs density (from the
  * given h seeds) -> gradients -> force on `n_active` targets and returns
  * wall seconds. */

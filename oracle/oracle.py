@@ -104,6 +104,45 @@ def _c_drift_state(st: dict) -> OrcDriftState:
     return s
 
 
+TIMESTEP_FIELDS = [  # (name, components, dtype), the order of orc_timestep_state
+    ("grav", 3, np.float64), ("accel", 3, np.float64), ("vsig", 1, np.float64), ("h", 1, np.float64),
+    ("num_ngb", 1, np.float64), ("divvel", 1, np.float64), ("mass", 1, np.float64), ("softening", 1, np.float64),
+    ("aphys", 1, np.float64), ("ti_want", 1, np.int64), ("bin", 1, np.int32), ("ti_begstep", 1, np.int64),
+    ("dt_step", 1, np.int64),
+]
+TIMEBINS = 60  # declarations/typedefs.h:8
+
+
+class OrcTimestepState(C.Structure):
+    _fields_ = [("n", C.c_int)] + [(name, _CTYPE[dt]) for name, _, dt in TIMESTEP_FIELDS]
+
+
+class OrcTimestepParams(C.Structure):
+    _fields_ = [("err_tol_int_accuracy", C.c_double), ("courant_fac", C.c_double),
+                ("max_size_timestep", C.c_double), ("min_size_timestep", C.c_double), ("timebase", C.c_double),
+                ("ti_current", C.c_longlong), ("bin_active", C.c_int * TIMEBINS)]
+
+
+def new_timestep_state(n: int, inputs: dict) -> dict:
+    """All timestep arrays for n cells, zero except what `inputs` fills."""
+    st = {}
+    for name, k, dt in TIMESTEP_FIELDS:
+        st[name] = np.zeros((n,) if k == 1 else (n, k), dtype=dt)
+    for name, arr in inputs.items():
+        st[name][...] = arr
+    return st
+
+
+def _c_timestep_state(st: dict) -> OrcTimestepState:
+    s = OrcTimestepState()
+    s.n = int(st["mass"].shape[0])
+    for name, _, dt in TIMESTEP_FIELDS:
+        a = st[name]
+        assert a.flags["C_CONTIGUOUS"] and a.dtype == dt and a.shape[0] == s.n, name
+        setattr(s, name, a.ctypes.data_as(_CTYPE[dt]))
+    return s
+
+
 class OrcCsr(C.Structure):
     _fields_ = [("offsets", C.POINTER(C.c_longlong)), ("nbrs", _ip), ("n_rows", C.c_int)]
 
@@ -150,6 +189,9 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
     f.restype = C.c_int
     f = getattr(lib, f"{prefix}_drift")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcDriftState), C.c_longlong, C.c_double, C.c_double]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_timestep")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcTimestepParams), C.POINTER(OrcTimestepState)]
     f.restype = C.c_int
     f = getattr(lib, f"{prefix}_full_pass_seconds")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
@@ -246,6 +288,12 @@ class Oracle:
         cs = _c_drift_state(st)
         f = getattr(self.lib, f"{self.prefix}_drift")
         return int(f(C.byref(self.params), C.byref(cs), int(time1), float(timebase), float(min_egy_spec)))
+
+    def timestep(self, st: dict, tp: "OrcTimestepParams") -> int:
+        """New timesteps and bins of every cell of the timestep state, in place."""
+        cs = _c_timestep_state(st)
+        f = getattr(self.lib, f"{self.prefix}_timestep")
+        return int(f(C.byref(self.params), C.byref(tp), C.byref(cs)))
 
     def full_pass_seconds(self, st, active=None):
         a, na = self._act(active)
