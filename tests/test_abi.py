@@ -40,6 +40,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", offsetof(gz_params, box_size), offsetof(gz_particles, cond), offsetof(gz_outputs, iters),
          offsetof(gz_outputs, flux_abs));
   printf("%zu %zu\n", offsetof(gz_status_info, pairs_density), offsetof(gz_status_info, message));
+  printf("%zu %zu %zu %zu\n", sizeof(gz_kick_fields), offsetof(gz_kick_fields, active),
+         sizeof(gz_drift_fields), offsetof(gz_drift_fields, status));
   return 0; }
 ''')
     exe = tmp_path / "layout"
@@ -49,8 +51,25 @@ int main(void) {
     want = [C.sizeof(abi.GzParams), C.sizeof(abi.GzParticles), C.sizeof(abi.GzOutputs), C.sizeof(abi.GzStatusInfo),
             abi.GzParams.box_size.offset, abi.GzParticles.cond.offset, abi.GzOutputs.iters.offset,
             abi.GzOutputs.flux_abs.offset,
-            abi.GzStatusInfo.pairs_density.offset, abi.GzStatusInfo.message.offset]
+            abi.GzStatusInfo.pairs_density.offset, abi.GzStatusInfo.message.offset,
+            C.sizeof(abi.GzKickFields), abi.GzKickFields.active.offset,
+            C.sizeof(abi.GzDriftFields), abi.GzDriftFields.status.offset]
     assert got == want
+
+
+@pytest.mark.parametrize("cname,mirror", [("gz_kick_fields", abi.GzKickFields), ("gz_drift_fields", abi.GzDriftFields)])
+def test_device_field_structs_match_c_field_by_field(tmp_path, cname, mirror):
+    """Every field of the ctypes mirror sits at the C offset of the field of the same name: two
+    pointer fields in swapped order would keep the size and hand the kernel the wrong arrays."""
+    names = [f[0] for f in mirror._fields_]
+    prog = tmp_path / "fields.c"
+    prog.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"gizmo_hydro.h\"\nint main(void) {\n"
+                    + "".join(f'  printf("%zu\\n", offsetof({cname}, {n}));\n' for n in names)
+                    + f'  printf("%zu\\n", sizeof({cname}));\n  return 0; }}\n')
+    exe = tmp_path / "fields"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(prog), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == [getattr(mirror, n).offset for n in names] + [C.sizeof(mirror)]
 
 
 def _has_gpu():
