@@ -214,10 +214,11 @@ class HaloPass:
         own_rank = np.argsort(order[own_local], kind="stable")
         own_rows = own_local[own_rank]  # local row of each own particle, in the caller's order
         result = {k: np.asarray(v)[own_rows].copy() for k, v in out.items()}
-        pos_of = {int(g): i for i, g in enumerate(gid)}
-        for part in returned:
-            for g, dm in part:
-                result["dmass"][pos_of[int(g)]] += dm
+        back_rows = np.concatenate(returned, axis=0) if any(len(r) for r in returned) else np.zeros((0, 2))
+        if len(back_rows):
+            by_gid = np.argsort(gid, kind="stable")
+            at = by_gid[np.searchsorted(gid[by_gid], back_rows[:, 0].astype(np.int64))]
+            np.add.at(result["dmass"], at, back_rows[:, 1])
         self.last_radius = 4.0 * H
         self.last_imported = len(imported)
         return result, h_max
