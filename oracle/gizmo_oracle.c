@@ -1053,9 +1053,10 @@ static inline void load_side(const orc_state *s, int i, double gamma, fside *f)
  * (R state), j the neighbour (L state). Returns the MFV j-side dMass write
  * through *dmass_j (0 when none). */
 static void force_pair(const gz_params *p, const gconst *gc, const fside *I, const fside *J, fout *out, double *dmass_j,
-                       int *stop)
+                       int *stop, double *vsig_pair)
 {
     *dmass_j = 0;
+    *vsig_pair = -1; /* set below for a pair that reaches the wake-up test (hydro_functions.h:534-544) */
     if (J->m <= 0) return;
     if (J->rho <= 0) return;
     const int kf = p->kernel, mfv = gc->mfv;
@@ -1234,6 +1235,7 @@ static void force_pair(const gz_params *p, const gconst *gc, const fside *I, con
     out->dtE += Fl.p;
     const double vsig_ts = vsig + fabs(I->cs - J->cs);
     if (vsig_ts > out->vsig) out->vsig = vsig_ts;
+    *vsig_pair = vsig_ts;
     if (mfv) {
         /* j-side write (hydro_functions.h:511-532) */
         double dmass_holder = Fl.rho * I->dt, lim;
@@ -1262,6 +1264,14 @@ static void make_gconst(const gz_params *p, gconst *gc)
 }
 
 int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads)
+{
+    return orc_force_wakeup(p, s, active, n_active, n_threads, NULL);
+}
+
+#define WAKEUP 4.1 /* declarations/constants.h:11-13 (SLOPE_LIMITER_TOLERANCE > 0, no GR) */
+
+int orc_force_wakeup(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads,
+                     const int *bin_active)
 {
     set_threads(n_threads);
     int *all = NULL;
@@ -1298,11 +1308,20 @@ int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active,
                 const int j = cand[c];
                 if (j == i) continue;
                 load_side(s, j, p->gamma, &J);
-                double dmj;
-                force_pair(p, &gc, &I, &J, o, &dmj, &stop);
+                double dmj, vsig_pair;
+                force_pair(p, &gc, &I, &J, o, &dmj, &stop, &vsig_pair);
                 if (mfv && dmj != 0) {
 #pragma omp atomic
                     s->dmass[j] += dmj;
+                }
+                /* wake-up (hydro_functions.h:534-544): an inactive neighbour whose stored signal
+                 * speed is too slow for this pair is flagged with this target's bin + 1
+                 * (wakeup_flag_from_timebin, core/proto.h:181) */
+                if (bin_active && vsig_pair >= 0 && !bin_active[s->timebin[j]] &&
+                    vsig_pair > WAKEUP * s->vsig[j]) {
+                    const int w = s->timebin[i] + 1;
+#pragma omp critical(orc_wakeup)
+                    { if (s->wakeup[j] < w) s->wakeup[j] = w; }
                 }
             }
             if (stop) {

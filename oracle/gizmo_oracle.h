@@ -63,6 +63,9 @@ typedef struct orc_state {
     double *dtmass;    /* [n]    CellP.DtMass (MFV) */
     double *dmass;     /* [n]    CellP.dMass (MFV) */
     double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
+    /* individual timesteps (read only by orc_force_wakeup) */
+    int    *timebin;   /* [n]    P.TimeBin */
+    int    *wakeup;    /* [n]    P.wakeup (in/out: the largest wake-up flag set) */
 } orc_state;
 
 /* Neighbour sets in CSR form, original indices, each row sorted ascending. */
@@ -79,6 +82,10 @@ typedef struct orc_csr {
 int orc_density(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
 int orc_gradients(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
 int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
+/* orc_force with the wake-up of inactive neighbours (hydro_functions.h:534-544):
+ * bin_active is TimeBinActive[60]; NULL switches the wake-up off, as orc_force does. */
+int orc_force_wakeup(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads,
+                     const int *bin_active);
 
 /* Density sums at a fixed kernel length, no iteration: writes the raw
  * accumulator of density_loop.h:1140-1385 for each active into acc[a][14]:

@@ -32,6 +32,7 @@ STATE_FIELDS = [  # (name, components, dtype)
     ("grad_rho", 3, np.float64), ("grad_p", 3, np.float64), ("grad_v", 9, np.float64),
     ("accel", 3, np.float64), ("dudt", 1, np.float64), ("vsig", 1, np.float64),
     ("dtmass", 1, np.float64), ("dmass", 1, np.float64), ("gravwork", 3, np.float64),
+    ("timebin", 1, np.int32), ("wakeup", 1, np.int32),
 ]
 
 
@@ -181,6 +182,9 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
         f = getattr(lib, f"{prefix}_{name}")
         f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int]
         f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_force_wakeup")
+    f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
+    f.restype = C.c_int
     f = getattr(lib, f"{prefix}_density_sums")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, _dp, _dp, C.c_int]
     f.restype = C.c_int
@@ -263,6 +267,16 @@ class Oracle:
 
     def force(self, st, active=None):
         return self._run("force", st, active)
+
+    def force_wakeup(self, st, bin_active, active=None):
+        """The force pass with the wake-up of inactive neighbours (TimeBinActive = bin_active[60])."""
+        a, na = self._act(active)
+        cs = _c_state(st)
+        bins = np.ascontiguousarray(bin_active, dtype=np.int32)
+        assert bins.shape == (TIMEBINS,)
+        f = getattr(self.lib, f"{self.prefix}_force_wakeup")
+        return int(f(C.byref(self.params), C.byref(cs), a.ctypes.data_as(_ip) if a is not None else None, na,
+                     self.n_threads, bins.ctypes.data_as(_ip)))
 
     def density_sums(self, st, active=None):
         a, na = self._act(active)
