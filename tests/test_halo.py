@@ -1,10 +1,11 @@
-"""The domain-and-halo form of the hydro pass (gizmo_b200/halo.py) on two
-``gloo`` ranks on the CPU, each rank computing its share with the oracle in
+"""The domain-and-halo form of the hydro pass (gizmo_b200/halo.py) on two and
+three ``gloo`` ranks on the CPU, each rank computing its share with the oracle in
 place of its GPU: the outputs of every particle equal those of a one-domain
 pass, bit for bit, except the MFV dMass, whose sum collects the j-side terms
 of other ranks in another order (within 1e-14 of its largest value). One run
 starts from converged kernel lengths, the other from seeds so small that the
-first halo is too thin and the pass is redone deeper."""
+first halo is too thin and the pass is redone deeper; with three ranks a cell
+is imported by both others and its dMass collects j-side terms from both."""
 import os
 import socket
 import sys
@@ -82,8 +83,9 @@ def _run_ranks(h, world=2):
     return got
 
 
-@pytest.mark.parametrize("seed_scale", [None, 0.6], ids=["converged-seeds", "thin-first-halo"])
-def test_two_domains_equal_one_domain(seed_scale):
+@pytest.mark.parametrize("seed_scale,world", [(None, 2), (0.6, 2), (None, 3)],
+                         ids=["converged-seeds", "thin-first-halo", "three-domains"])
+def test_domains_equal_one_domain(seed_scale, world):
     from oracle import oracle as O
     wl = _workload()
     st = O.new_state(wl.n, wl.inputs())
@@ -94,11 +96,12 @@ def test_two_domains_equal_one_domain(seed_scale):
     ref = O.new_state(wl.n, wl.inputs())
     orc = O.Oracle(wl.params, "port", n_threads=1)
     assert orc.density(ref) == 0 and orc.gradients(ref) == 0 and orc.force(ref) == 0
-    got = _run_ranks(wl.h)
+    got = _run_ranks(wl.h, world)
     covered = np.zeros(wl.n, dtype=int)
     for rank, gid, out, radius, imported in got:
         covered[gid] += 1
-        assert imported < wl.n - len(gid)  # the halo left some of the other domain out
+        if world == 2:  # two Morton halves are slabs: the halo leaves part of the other one out
+            assert imported < wl.n - len(gid)
         if seed_scale is not None:  # the first halo (4 x 1.1 x the largest seed) was redone deeper
             assert radius > 4.0 * 1.1 * wl.h.max() * 1.2
         for f in OUT_FIELDS:
