@@ -8,8 +8,10 @@ computation wrote into those copies. Here the exchange happens once per pass,
 before density, instead of once per loop:
 
   * domains are contiguous ranges of Morton keys with equal particle counts,
-    so a domain is spatially compact and its box is tight;
-  * a rank imports every particle within 4H of its own domain box (periodic),
+    so a domain is spatially compact; it is described by the boxes of its
+    particles in each occupied top-level Morton cell (4 x 4 x 4), which stay
+    tight for any number of ranks;
+  * a rank imports every particle within 4H of its own domain boxes (periodic),
     where H bounds every kernel length the pass produces. That is deep enough
     to compute, redundantly, everything its own particles read: density runs on
     own particles and on imports within 2H of the box, gradients on own
@@ -72,6 +74,33 @@ def box_distance(x: np.ndarray, lo: np.ndarray, hi: np.ndarray, box: float) -> n
             best = d if best is None else np.minimum(best, d)
         d2 += best * best
     return np.sqrt(d2)
+
+
+N_DOMAIN_BOXES = 64  # top two Morton levels: a domain is described by up to 64 boxes
+
+
+def domain_boxes(pos: np.ndarray, box: float) -> np.ndarray:
+    """[N_DOMAIN_BOXES, 6] boxes (lo, hi) of the particles in each occupied top-level Morton
+    cell (4 x 4 x 4); unused rows are empty (lo = +inf, hi = -inf). Their union holds
+    every particle, so a distance to it never exceeds the distance to the nearest particle."""
+    out = np.empty((N_DOMAIN_BOXES, 6))
+    out[:, :3], out[:, 3:] = np.inf, -np.inf
+    if not len(pos):
+        return out
+    cell = (morton_keys(pos, box) >> np.uint64(63 - 6)).astype(np.int64)
+    for c in np.unique(cell):
+        sel = pos[cell == c]
+        out[c, :3], out[c, 3:] = sel.min(0), sel.max(0)
+    return out
+
+
+def boxes_distance(x: np.ndarray, boxes: np.ndarray, box: float) -> np.ndarray:
+    """Distance of each point to the union of boxes (rows lo, hi) in a periodic cube."""
+    d = np.full(len(x), np.inf)
+    for b in boxes:
+        if np.isfinite(b[0]):
+            d = np.minimum(d, box_distance(x, b[:3], b[3:], box))
+    return d
 
 
 def pack(inputs: dict, idx: np.ndarray) -> np.ndarray:
@@ -164,18 +193,17 @@ class HaloPass:
         box = float(self.params.box_size)
         pos = np.asarray(inputs["pos"], dtype=np.float64).reshape(-1, 3)
         n_own = len(gid)
-        lo = pos.min(0) if n_own else np.full(3, np.inf)
-        hi = pos.max(0) if n_own else np.full(3, -np.inf)
-        boxes = self.ex.all_gather_rows(np.concatenate([lo, hi]))
+        mine = domain_boxes(pos, box)
+        boxes = self.ex.all_gather_rows(mine.ravel()).reshape(self.ex.world, N_DOMAIN_BOXES, 6)
         H = self.ex.all_max(float(np.max(inputs["h"])) if n_own else 0.0) * self.h_margin
         for _ in range(self.max_tries):
-            out, h_max = self._attempt(gid, inputs, pos, lo, hi, boxes, H, box)
+            out, h_max = self._attempt(gid, inputs, pos, mine, boxes, H, box)
             if self.ex.all_max(h_max) <= H:
                 return out
             H *= self.h_growth
         raise RuntimeError(f"halo pass: kernel lengths still above the halo depth after {self.max_tries} tries")
 
-    def _attempt(self, gid, inputs, pos, lo, hi, boxes, H, box):
+    def _attempt(self, gid, inputs, pos, mine, boxes, H, box):
         ex = self.ex
         # own particles each other rank needs: within 4H of its domain box
         send = []
@@ -183,7 +211,7 @@ class HaloPass:
             if r == ex.rank or not len(gid):
                 send.append(np.zeros((0, N_INPUT + 1)))
                 continue
-            near = np.nonzero(box_distance(pos, boxes[r][:3], boxes[r][3:], box) < 4.0 * H)[0]
+            near = np.nonzero(boxes_distance(pos, boxes[r], box) < 4.0 * H)[0]
             send.append(np.concatenate([gid[near, None].astype(np.float64), pack(inputs, near)], axis=1))
         got = ex.swap(send)
         imported = np.concatenate([g for g in got], axis=0) if any(len(g) for g in got) else np.zeros((0, N_INPUT + 1))
@@ -195,7 +223,7 @@ class HaloPass:
         local = unpack(rows)
         is_own = (order < len(gid))
         owner = np.where(is_own, ex.rank, np.concatenate([np.full(len(gid), ex.rank), src])[order])
-        d = box_distance(local["pos"], lo, hi, box) if len(gid) else np.full(len(order), np.inf)
+        d = boxes_distance(local["pos"], mine, box)
         d = np.where(is_own, 0.0, d)
         dens = np.nonzero(d < 2.0 * H)[0].astype(np.int32)
         grad = np.nonzero(d < H)[0].astype(np.int32)

@@ -100,8 +100,7 @@ def test_domains_equal_one_domain(seed_scale, world):
     covered = np.zeros(wl.n, dtype=int)
     for rank, gid, out, radius, imported in got:
         covered[gid] += 1
-        if world == 2:  # two Morton halves are slabs: the halo leaves part of the other one out
-            assert imported < wl.n - len(gid)
+        assert imported < wl.n - len(gid)  # the halo left part of the other domains out
         if seed_scale is not None:  # the first halo (4 x 1.1 x the largest seed) was redone deeper
             assert radius > 4.0 * 1.1 * wl.h.max() * 1.2
         for f in OUT_FIELDS:
