@@ -1632,7 +1632,7 @@ static int orc_timestep_bin(long long ti_step)
  * this configuration: cf_a2inv = cf_atime = cf_hubble_a = 1, no PM, no
  * dilation, STOP_WHEN_BELOW_MINTIMESTEP, dt_displacement = MaxSizeTimestep
  * (find_dt_displacement_constraint, timestep.cc:1425-1434, non-comoving):
- *   acceleration criterion   :421-487 (KERNEL_CORE_SIZE 1/2)
+ *   acceleration criterion   :421-487 (KERNEL_CORE_SIZE of the kernel)
  *   Courant criterion         :711-729 (Get_Particle_Size, declarations/particle_data.h:461-469)
  *   divergence criterion      :1093-1098
  *   caps, floor, integer step :1334-1414
@@ -1640,7 +1640,8 @@ static int orc_timestep_bin(long long ti_step)
  * of two below the wanted step, a larger bin only where it is synchronised. */
 int orc_timestep(const gz_params *p, const orc_timestep_params *tp, orc_timestep_state *t)
 {
-    (void)p;
+    /* KERNEL_CORE_SIZE: 1/2 for the cubic spline, 2/5 for Wendland C2 (mesh/kernel.h:59, 113) */
+    const double core = p->kernel == GZ_KERNEL_CUBIC ? (1.0 / 2.0) : (2.0 / 5.0);
     int code = 0;
     const double tb = tp->timebase;
     for (int i = 0; i < t->n; i++) {
@@ -1653,7 +1654,7 @@ int orc_timestep(const gz_params *p, const orc_timestep_params *tp, orc_timestep
         double ac = sqrt(ax * ax + ay * ay + az * az);
         t->aphys[i] = ac;
         if (ac == 0) ac = 1.0e-30;
-        double h_acc = (1.0 / 2.0) * t->softening[i];
+        double h_acc = core * t->softening[i];
         if (h_acc <= 0) h_acc = (1.61199 * t->h[i] / t->num_ngb[i]) * 1.0;
         double dt = sqrt(2 * tp->err_tol_int_accuracy * 1.0 * h_acc / ac);
         if (t->mass[i] > 0) {

@@ -98,6 +98,19 @@ def test_drift_constructed_cases(method, floor):
         assert (r["u_pred"][2:] >= floor).all()
 
 
+
+def test_drift_isothermal_wendland_build():
+    """The build of the log-normal workload (MFM, Wendland C2, gamma = 1.0001): the
+    pressure of a drifted cell carries gamma - 1 = 1e-4."""
+    params = ics.lognormal(8, seed_density=2, seed_velocity=3, grid=16).params
+    params.min_kernel_radius, params.max_kernel_radius = 0.05, 0.5
+    if not O.ref_available(params):
+        pytest.skip("reference build not present")
+    ds, time1 = _constructed(2048, 210, params)
+    r, code = _both(params, ds, time1, 3.0)
+    assert code == 0
+
+
 def test_drift_into_the_past_is_refused():
     params = ics.sedov(4, seed=1).params
     if not O.ref_available(params):

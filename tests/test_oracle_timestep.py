@@ -60,11 +60,14 @@ def test_timestep_after_force_pass(method):
     assert ((r["dt_step"] & (r["dt_step"] - 1)) == 0).all() and (r["dt_step"] <= r["ti_want"]).all()
 
 
-def test_timestep_constructed_cases():
+@pytest.mark.parametrize("build", ["mfm_cubic", "mfm_wendland_isothermal"])
+def test_timestep_constructed_cases(build):
     """Each criterion binds somewhere: acceleration (with and without a
     softening), Courant, divergence, MaxSizeTimestep; zero mass (acceleration
-    only); a bin that wants to grow into unsynchronised bins."""
-    params = ics.sedov(4, seed=1).params
+    only); a bin that wants to grow into unsynchronised bins. Against the
+    reference compiled for the Sedov build and for the log-normal one."""
+    params = (ics.sedov(4, seed=1) if build == "mfm_cubic"
+              else ics.lognormal(8, seed_density=2, seed_velocity=3, grid=16)).params
     if not O.ref_available(params):
         pytest.skip("reference build not present")
     n = 4096
