@@ -14,10 +14,13 @@ from oracle import oracle as O
 from tests._util import FORCE_FIELDS
 
 
-@pytest.mark.parametrize("method", [METHOD_MFM, METHOD_MFV], ids=["mfm", "mfv"])
-def test_wakeup_port_equals_reference(method):
-    wl = ics.sedov(12, seed=7)
-    wl.params.method = method
+@pytest.mark.parametrize("build", ["sedov_mfm", "sedov_mfv", "lognormal_mfm_wendland"])
+def test_wakeup_port_equals_reference(build):
+    if build.startswith("sedov"):
+        wl = ics.sedov(12, seed=7)
+        wl.params.method = METHOD_MFV if build.endswith("mfv") else METHOD_MFM
+    else:
+        wl = ics.lognormal(12, seed_density=2, seed_velocity=3, grid=24)
     if not O.ref_available(wl.params):
         pytest.skip("reference build not present")
     base = O.new_state(wl.n, wl.inputs())
