@@ -306,7 +306,8 @@ typedef struct gz_drift_fields {
  * cudaStream_t, NULL for the default stream) without waiting; no context, no
  * allocation. FP64 without contraction; the two exponentials are correctly
  * rounded, so results match the reference bit for bit except where its
- * libm exp misrounds (within one ulp). */
+ * libm exp is one ulp off: then the density and the kernel radius differ by
+ * at most 2 ulp and the pressure by at most 4. */
 int gz_drift(const gz_params *params, const gz_drift_fields *f, int64_t time1, double timebase, double min_egy_spec,
              void *stream);
 
