@@ -64,6 +64,15 @@ def parse_args():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cold", action="store_true")
+    # profiling and kernel timing (no bench line)
+    ap.add_argument("--profile-pass", action="store_true",
+                    help="one steady-state pass inside the NVTX range 'steady_pass', timing nothing (for ncu)")
+    ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed", help="arithmetic form of --profile-pass")
+    ap.add_argument("--kernel", choices=["kick", "drift"], default=None,
+                    help="time the device half-step kick or drift alone and print one JSON line")
+    ap.add_argument("--n", type=int, default=1 << 24, help="particles of --kernel")
+    ap.add_argument("--method", choices=["mfm", "mfv"], default="mfv", help="hydro method of --kernel")
+    ap.add_argument("--reps", type=int, default=20, help="timed launches of --kernel")
     return ap.parse_args()
 
 
@@ -505,8 +514,156 @@ def run_reference(args, world, rank):
     }
 
 
+# ------------------------------------------------- profiling and kernel timing
+def profile_pass(args):
+    """One steady-state pass to profile: the workload's particle set, kernel
+    lengths converged once in FP64 from the cold seed, the steady-state seed
+    (converged h x (1 + U(-0.05, 0.05))), then one restage + density +
+    gradients + force pass of ``--form`` inside the NVTX range "steady_pass". A
+    profiler restricted to that range (ncu --nvtx --nvtx-include "steady_pass/")
+    sees the kernels of a timed bench step and none of the set-up."""
+    import torch
+
+    from gizmo_b200 import abi, ics
+    from gizmo_b200.hydro import HydroPass
+
+    n1 = args.n1 or default_n1(args.workload)
+    wl = make_workload(args.workload, n1, abi.PRECISION_FP64)
+    n = wl.n
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        chunk = 1 << 21
+        for a in range(0, n, chunk):
+            hp.density(np.arange(a, min(n, a + chunk), dtype=np.int32) if n > chunk else None)
+        conv = hp.download(["h", "cond"])
+    wl.h = ics.steady_state_seed(conv["h"], 4)
+    wl.cond = conv["cond"]
+    wl.params.precision = abi.PRECISION_MIXED if args.form == "mixed" else abi.PRECISION_FP64
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("steady_pass")
+        hp.restage()
+        hp.full_pass()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        st = hp.status()
+    print(f"ok: {n} particles, {st['pairs_symmetric']} symmetric row entries, "
+          f"{st['density_iterations']} density iterations")
+
+
+# bytes per particle one second half kick reads and writes (all active, MFV with
+# dMass != 0, no temperature floor reached), and one drift (every cell drifted)
+KICK_READ = {"mass": 8, "tstart": 8, "tend": 8, "mass_true": 8, "dmass": 8, "dtmass": 8, "active": 4, "grav": 24,
+             "gravwork": 24, "u": 8, "dudt": 8, "accel": 24, "vel": 24, "dp": 24}
+KICK_WRITE = {"mass_true": 8, "dmass": 8, "u": 8, "vel": 24, "vel_pred": 24, "mass": 8, "u_pred": 8, "dp": 24}
+KICK_MFM_SKIPS = ("mass_true", "dmass", "dtmass", "gravwork")
+DRIFT_READ = {"pos": 24, "move": 24, "vel_pred": 24, "grav": 24, "accel": 24, "divvel": 8, "mass": 8, "dtmass": 8,
+              "mass_true": 8, "rho": 8, "u_pred": 8, "dudt": 8, "h": 8, "ti_current": 8}
+DRIFT_WRITE = {"pos": 24, "vel_pred": 24, "mass": 8, "rho": 8, "u_pred": 8, "h": 8, "pressure": 8, "ti_current": 8}
+DRIFT_MFV_ONLY = ("dtmass", "mass_true")
+
+
+def kernel_bytes_per_particle(kernel: str, mfv: bool) -> int:
+    if kernel == "kick":
+        skip = () if mfv else KICK_MFM_SKIPS
+        return (sum(v for k, v in KICK_READ.items() if k not in skip) +
+                sum(v for k, v in KICK_WRITE.items() if k not in skip and not (k == "mass" and skip)))
+    return (sum(v for k, v in DRIFT_READ.items() if mfv or k not in DRIFT_MFV_ONLY) +
+            sum(v for k, v in DRIFT_WRITE.items() if mfv or k != "mass"))
+
+
+def time_step_kernel(args):
+    """Times ``--reps`` launches of the device kick (second half kicks) or drift
+    (each one step of 2^20 ticks further, so none is a no-op) over ``--n``
+    seeded particles in device memory, all active, gravity on, with CUDA events
+    on the launching stream; prints one JSON line with the mean duration, the
+    algorithmic bytes (each field read or written once) and the bandwidth.
+    Above ~1M particles the working set exceeds the 126 MB L2, so every launch
+    streams from HBM without a flush."""
+    import torch
+
+    from gizmo_b200 import abi, ics
+    from gizmo_b200.hydro import drift, kick
+
+    mfv = args.method == "mfv"
+    params = ics.sedov(4, seed=1).params
+    params.method = abi.METHOD_MFV if mfv else abi.METHOD_MFM
+    n = args.n
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(11 if args.kernel == "kick" else 12)
+
+    def f64(*shape, lo=-1.0, hi=1.0):
+        return torch.rand(*shape, generator=g, device=dev, dtype=torch.float64) * (hi - lo) + lo
+
+    timebase = 2.0 ** -40
+    stream = torch.cuda.current_stream(dev)
+    if args.kernel == "kick":
+        mass = f64(n, lo=0.5, hi=2.0)
+        f = {"vel": f64(n, 3), "u": f64(n, lo=1, hi=10), "mass": mass, "mass_true": mass.clone(),
+             "dmass": f64(n, lo=1e-6, hi=1e-5), "dtmass": f64(n, lo=1e-9, hi=1e-8), "accel": f64(n, 3),
+             "dudt": f64(n), "grav": f64(n, 3), "gravwork": f64(n, 3),
+             "vel_pred": torch.zeros(n, 3, dtype=torch.float64, device=dev),
+             "u_pred": torch.zeros(n, dtype=torch.float64, device=dev),
+             "dp": torch.zeros(n, 3, dtype=torch.float64, device=dev),
+             "tstart": torch.zeros(n, dtype=torch.int64, device=dev),
+             "tend": torch.randint(1 << 20, 1 << 21, (n,), generator=g, device=dev, dtype=torch.int64),
+             "active": torch.ones(n, dtype=torch.int32, device=dev)}
+        if not mfv:
+            for k in KICK_MFM_SKIPS:
+                del f[k]
+
+        def launch(_k):
+            kick(params, f, 1, timebase, 0.0, stream.cuda_stream)
+    else:
+        params.min_kernel_radius, params.max_kernel_radius = 1e-6, 1e6
+        mass = f64(n, lo=0.5, hi=2.0)
+        f = {"pos": f64(n, 3, lo=0, hi=1), "vel_pred": f64(n, 3), "grav": f64(n, 3), "accel": f64(n, 3),
+             "divvel": f64(n), "mass": mass, "rho": f64(n, lo=0.5, hi=2.0), "u_pred": f64(n, lo=1, hi=10),
+             "dudt": f64(n, lo=-1e-3, hi=1e-3), "h": f64(n, lo=0.01, hi=0.02),
+             "pressure": torch.zeros(n, dtype=torch.float64, device=dev),
+             "ti_current": torch.zeros(n, dtype=torch.int64, device=dev),
+             "status": torch.zeros(1, dtype=torch.int32, device=dev)}
+        if mfv:
+            f.update({"pvel": f64(n, 3), "dtmass": f64(n, lo=-1e-3, hi=1e-3), "mass_true": mass.clone()})
+        else:
+            f["vel"] = f64(n, 3)
+
+        def launch(k):
+            drift(params, f, (k + 1) << 20, timebase, 0.0, stream.cuda_stream)
+    for k in range(args.warmup):
+        launch(k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.warmup, args.warmup + args.reps):
+        launch(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if args.kernel == "drift" and int(f["status"].item()) != 0:
+        raise RuntimeError(f"gz_drift status {int(f['status'].item())}")
+    ms = e0.elapsed_time(e1) / args.reps
+    bpp = kernel_bytes_per_particle(args.kernel, mfv)
+    gbs = bpp * n / (ms * 1e-3) / 1e9
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except Exception:
+        pass
+    print(json.dumps({"kernel": f"k_{args.kernel}", "method": args.method, "n": n, "reps": args.reps,
+                      "ms_per_launch": ms, "bytes_per_particle": bpp, "achieved_gbs": gbs, "peak_gbs": peak,
+                      "frac": (gbs / peak) if peak else None, "particles_per_s": n / (ms * 1e-3)}))
+
+
 def main():
     args = parse_args()
+    if args.profile_pass:
+        profile_pass(args)
+        return
+    if args.kernel:
+        time_step_kernel(args)
+        return
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

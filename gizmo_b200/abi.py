@@ -89,6 +89,7 @@ class GzStatusInfo(C.Structure):
         ("device_bytes", C.c_int64),
         ("kernel_launches", C.c_int64),
         ("message", C.c_char * 256),
+        ("h_iter_max", C.c_double),
     ]
 
 

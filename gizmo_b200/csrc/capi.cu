@@ -57,6 +57,8 @@ struct gz_context {
     bool grid_valid = false;
     // density work: rows are [d_beg[t], d_end[t]) in d_nbr; d_used entries are taken
     DevBuf acc, h_built, scratch, keep, regrow, todo_a, todo_b, grow, d_beg, d_end, flag, counts, d_off, d_nbr, n_sel;
+    DevBuf hmax;                     // largest kernel length the density iteration took sums at (double bits)
+    double h_iter_max = 0;           // ... read back after the pass
     long long d_nbr_cap = 0, d_used = 0;
     bool dens_all = false;           // the density rows cover every particle (last pass had no active list)
     DevBuf pad_over, pad_list, pad_sum, pad_counts;  // padded single-walk density rows
@@ -246,7 +248,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->work, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->hmax, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
 }
 
 Tree tree_view(gz_context *c)
@@ -328,7 +330,8 @@ __global__ void k_set_active(int na, const int *__restrict__ t, unsigned char *f
     if (a < na) flag[t[a]] = 1;
 }
 
-__global__ void k_density_prep(int na, const int *__restrict__ t, double *h, double maxsoft, DensityScratch *sc)
+__global__ void k_density_prep(int na, const int *__restrict__ t, double *h, double maxsoft, DensityScratch *sc,
+                               unsigned long long *hmax)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= na) return;
@@ -336,6 +339,7 @@ __global__ void k_density_prep(int na, const int *__restrict__ t, double *h, dou
     double hv = h[i];
     if ((hv < 0) || !isfinite(hv) || (hv > 0.99 * maxsoft)) hv = 0.99 * maxsoft;  // density_loop.cc:837-840
     h[i] = hv;
+    atomicMax(hmax, (unsigned long long)__double_as_longlong(hv));  // hv >= 0: bits order like values
     DensityScratch z{};
     sc[i] = z;
 }
@@ -877,11 +881,13 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         ensure(c, c->todo_b, sizeof(int) * (size_t)std::max(na, 1)) ||
         ensure(c, c->grow, sizeof(int) * (size_t)std::max(na, 1)) || ensure(c, c->keep, (size_t)std::max(na, 1)) ||
         ensure(c, c->regrow, (size_t)std::max(na, 1)) || ensure(c, c->flag, sizeof(int)) ||
-        ensure(c, c->n_sel, sizeof(int) * 2))
+        ensure(c, c->n_sel, sizeof(int) * 2) || ensure(c, c->hmax, sizeof(unsigned long long)))
         return c->err;
+    GZ_CUDA(c, cudaMemsetAsync(c->hmax.p, 0, sizeof(unsigned long long), s));
     if (na > 0) {
         k_density_prep<<<(na + 255) / 256, 256, 0, s>>>(na, ptr<int>(c->targets), ptr<double>(c->h),
-                                                         c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch));
+                                                         c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch),
+                                                         ptr<unsigned long long>(c->hmax));
         c->launches++;
     }
     GZ_CUDA(c, cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * (size_t)na, cudaMemcpyDeviceToDevice, s));
@@ -924,6 +930,7 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
         w.keep = ptr<unsigned char>(c->keep);
         w.regrow = ptr<unsigned char>(c->regrow);
         w.rebuild = ptr<int>(c->flag);
+        w.h_iter_max = ptr<unsigned long long>(c->hmax);
         w.iter = iter;
         GZ_CUDA(c, cudaMemsetAsync(c->flag.p, 0, sizeof(int), s));
         const EventPair *ev = timer_launch(c, GZ_TIMER_DENSITY_SUMS, w.n_todo);
@@ -964,7 +971,10 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     (void)n;
+    unsigned long long hbits = 0;
+    GZ_CUDA(c, cudaMemcpyAsync(&hbits, c->hmax.p, sizeof(hbits), cudaMemcpyDeviceToHost, s));
     if (read_status(c)) return c->err;
+    memcpy(&c->h_iter_max, &hbits, sizeof(double));
     if (n_todo > 0) return fail(c, GZ_ERR_DENSITY_MAXITER, "density did not converge in MAXITER iterations");
     c->have_density = true;
     c->sym_valid = false;
@@ -1238,6 +1248,7 @@ int gz_status(gz_context *c, gz_status_info *info)
             info->index = orig;
     }
     info->density_iterations = c->last_iters;
+    info->h_iter_max = c->h_iter_max;
     info->kernel_launches = c->launches;
     info->pairs_density = c->pairs_density;
     info->pairs_symmetric = c->pairs_symmetric;

@@ -44,6 +44,7 @@ struct DensityWork {
     unsigned char *keep;    // per todo slot: still iterating
     unsigned char *regrow;  // per todo slot: its radius outgrew its row
     int *rebuild;           // set when any radius outgrows its row
+    unsigned long long *h_iter_max;  // atomic maximum of every radius the iteration moves to (double bits)
     int iter;
 };
 

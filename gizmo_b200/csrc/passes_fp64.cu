@@ -69,6 +69,7 @@ __global__ void k_after_iter(PassParams p, Particles ps, DensityWork w, DevStatu
     int regrow = 0;
     if (!conv) {
         ps.h[t] = nh;
+        if (w.h_iter_max) atomicMax(w.h_iter_max, (unsigned long long)__double_as_longlong(nh));
         regrow = nh > w.h_built[t];
         if (regrow) atomicExch(w.rebuild, 1);
     }

@@ -21,15 +21,17 @@ before density, instead of once per loop:
     kernel-length iteration: a density-active particle sees every particle
     within 2H of it, so an intermediate kernel length may reach twice the
     converged bound. The iteration can grow h by up to exp(1.631) per step
-    from a seed far too small (density_loop.h:864-947), so the result equals a
-    one-domain pass when the seeds are within a factor of about two of the
-    converged lengths, as the seeds of any step after the first are;
+    from a seed far too small (density_loop.h:864-947), so the engine reports
+    the largest kernel length at which the density iteration took sums, and a
+    pass in which it exceeded 2H is redone deeper (below): no sum is ever taken
+    over a halo that was too thin;
   * after the pass, the j-side dMass that own force targets wrote into
     imported copies (the MFV mass flux, hydro_functions.h:513-544) goes back to
     the owners, who add it to their own;
-  * if a kernel length came out above H, the pass is redone with a larger H
-    (the same on every rank), so the result never depends on a halo that was
-    too thin.
+  * if a converged kernel length came out above H, or an intermediate one of
+    the density iteration above 2H, the pass is redone with a larger H (the
+    same on every rank), so the result never depends on a halo that was too
+    thin.
 
 Each rank keeps its own and imported particles in global-index order, so every
 neighbour row, and with it every sum, has the order of a one-domain run.
@@ -172,8 +174,9 @@ class HaloPass:
 
     ``engine(params, local_inputs, density_active, gradient_active, force_active)``
     computes the pass on one rank's own and imported particles and returns the
-    output fields (``HydroPass`` names) for all of them; ``hydro_pass_engine``
-    below is the one that runs on the GPU. ``__call__`` takes this rank's own
+    output fields (``HydroPass`` names) for all of them, plus ``h_iter_max``:
+    the largest kernel length at which its density iteration took sums;
+    ``hydro_pass_engine`` below is the one that runs on the GPU. ``__call__`` takes this rank's own
     particles (their global indices and input fields) and returns the outputs of
     those particles, equal to what a one-domain pass gives them.
     """
@@ -188,6 +191,7 @@ class HaloPass:
         self.max_tries = max_tries
         self.last_radius = None
         self.last_imported = None
+        self.last_h_iter_max = None
 
     def __call__(self, gid: np.ndarray, inputs: dict) -> dict:
         box = float(self.params.box_size)
@@ -197,8 +201,11 @@ class HaloPass:
         boxes = self.ex.all_gather_rows(mine.ravel()).reshape(self.ex.world, N_DOMAIN_BOXES, 6)
         H = self.ex.all_max(float(np.max(inputs["h"])) if n_own else 0.0) * self.h_margin
         for _ in range(self.max_tries):
-            out, h_max = self._attempt(gid, inputs, pos, mine, boxes, H, box)
-            if self.ex.all_max(h_max) <= H:
+            out, h_max, h_iter_max = self._attempt(gid, inputs, pos, mine, boxes, H, box)
+            # every rank takes both reductions, in the same order
+            h_max, h_iter_max = self.ex.all_max(h_max), self.ex.all_max(h_iter_max)
+            self.last_h_iter_max = h_iter_max
+            if h_max <= H and h_iter_max <= 2.0 * H:
                 return out
             H *= self.h_growth
         raise RuntimeError(f"halo pass: kernel lengths still above the halo depth after {self.max_tries} tries")
@@ -228,7 +235,8 @@ class HaloPass:
         dens = np.nonzero(d < 2.0 * H)[0].astype(np.int32)
         grad = np.nonzero(d < H)[0].astype(np.int32)
         force = np.nonzero(is_own)[0].astype(np.int32)
-        out = self.engine(self.params, local, dens, grad, force)
+        out = dict(self.engine(self.params, local, dens, grad, force))
+        h_iter_max = float(out.pop("h_iter_max"))
         h_max = float(np.max(out["h"][dens])) if len(dens) else 0.0
         # reverse writeback: the j-side dMass own targets wrote into imported copies
         back = []
@@ -249,7 +257,7 @@ class HaloPass:
             np.add.at(result["dmass"], at, back_rows[:, 1])
         self.last_radius = 4.0 * H
         self.last_imported = len(imported)
-        return result, h_max
+        return result, h_max, h_iter_max
 
 
 def hydro_pass_engine(device: int = 0):
@@ -260,7 +268,10 @@ def hydro_pass_engine(device: int = 0):
         with HydroPass(params, device=device) as hp:
             hp.upload(local["pos"], local["vel"], local["mass"], local["u"], local["dt"], local["h"], local["cond"])
             hp.density(dens)
+            h_iter_max = hp.status()["h_iter_max"]
             hp.hydro_gradient_calc(grad)
             hp.hydro_force(force)
-            return hp.download()
+            out = hp.download()
+            out["h_iter_max"] = h_iter_max
+            return out
     return run

@@ -210,7 +210,8 @@ class HydroPass:
         self.lib.gz_status(self._ctx, C.byref(s))
         return dict(code=s.code, index=s.index, density_iterations=s.density_iterations,
                     pairs_density=s.pairs_density, pairs_symmetric=s.pairs_symmetric,
-                    device_bytes=s.device_bytes, kernel_launches=s.kernel_launches, message=s.message.decode(errors="replace"))
+                    device_bytes=s.device_bytes, kernel_launches=s.kernel_launches,
+                    message=s.message.decode(errors="replace"), h_iter_max=s.h_iter_max)
 
     def _check(self, rc: int):
         if rc:

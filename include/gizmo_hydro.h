@@ -128,6 +128,9 @@ typedef struct gz_status_info {
     int64_t  device_bytes;      /* device memory held by the context */
     int64_t  kernel_launches;   /* kernels of this library launched by the context so far */
     char     message[256];
+    double   h_iter_max;        /* the largest kernel length at which the last density pass took
+                                   sums: its seeds (after the clamp of density_loop.cc:837-840) and
+                                   every radius its iteration moved to */
 } gz_status_info;
 
 typedef struct gz_context gz_context;
@@ -227,7 +230,12 @@ int gz_density_sums(gz_context *ctx, const int *active, int n_active, double *ac
  *     before reading acc;
  *   - the first call on each device looks up that array's device address
  *     (a one-time set-up on the current device): make that first call before
- *     any stream capture;
+ *     any stream capture. Under CUDA's lazy module loading (the default since
+ *     CUDA 12.2) that first call is also where the library's device code is
+ *     loaded on the device and the 4 MiB array is reserved, so it must come
+ *     before the caller's memory pool reserves the device; setting
+ *     CUDA_MODULE_LOADING=EAGER reserves it when the process first creates
+ *     its CUDA context instead. A failed set-up returns GZ_ERR_CUDA;
  *   - every call on a device uses the same array and rewrites it; two calls
  *     whose work overlaps on the GPU (different streams, no ordering between
  *     them) race on it and their results are undefined.

@@ -408,6 +408,12 @@ int orc_density_sums(const gz_params *p, const orc_state *s, const int *active, 
     return 0;
 }
 
+/* Largest kernel length at which the last orc_density took sums (seeds after
+ * the pre-iteration clamp and every radius the iteration moved to). */
+static double g_density_h_iter_max = 0;
+
+double orc_density_h_iter_max(void) { return g_density_h_iter_max; }
+
 int orc_density(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads)
 {
     set_threads(n_threads);
@@ -427,7 +433,8 @@ int orc_density(const gz_params *p, orc_state *s, const int *active, int n_activ
     double *final_acc = (double *)malloc(sizeof(double) * 14 * (size_t)(n_active > 0 ? n_active : 1));
     double *final_pv = (double *)malloc(sizeof(double) * 3 * (size_t)(n_active > 0 ? n_active : 1));
     double *final_h = (double *)malloc(sizeof(double) * (size_t)(n_active > 0 ? n_active : 1));
-#pragma omp parallel
+    double h_iter_max = 0;
+#pragma omp parallel reduction(max : h_iter_max)
     {
         int *cand = NULL, cap = 0;
 #pragma omp for schedule(dynamic, 16)
@@ -438,6 +445,7 @@ int orc_density(const gz_params *p, orc_state *s, const int *active, int n_activ
             double h = s->h[i], acc[14], pv[3];
             int it = 0, conv = 0, stop = 0;
             for (it = 0; it < MAXITER; it++) {
+                if (h > h_iter_max) h_iter_max = h;
                 memset(acc, 0, sizeof(acc));
                 memset(pv, 0, sizeof(pv));
                 const int nc = orc_grid_candidates(&g, xi, h, 0, &cand, &cap);
@@ -466,6 +474,7 @@ int orc_density(const gz_params *p, orc_state *s, const int *active, int n_activ
         }
         free(cand);
     }
+    g_density_h_iter_max = h_iter_max;
     for (int a = 0; a < n_active; a++) density_finalize(p, s, active[a], final_h[a], final_acc + 14 * (size_t)a, final_pv + 3 * (size_t)a);
     free(final_acc); free(final_pv); free(final_h);
     orc_grid_free(&g);

@@ -80,6 +80,8 @@ typedef struct orc_csr {
  * converge, 90001009 empty bracket, 1234 no positive-pressure Riemann
  * solution). n_threads <= 0 uses the OpenMP default. */
 int orc_density(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
+/* The largest kernel length at which the last orc_density evaluated sums. */
+double orc_density_h_iter_max(void);
 int orc_gradients(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
 int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads);
 /* orc_force with the wake-up of inactive neighbours (hydro_functions.h:534-544):

@@ -197,6 +197,10 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
     f = getattr(lib, f"{prefix}_timestep")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcTimestepParams), C.POINTER(OrcTimestepState)]
     f.restype = C.c_int
+    if hasattr(lib, f"{prefix}_density_h_iter_max"):
+        f = getattr(lib, f"{prefix}_density_h_iter_max")
+        f.argtypes = []
+        f.restype = C.c_double
     f = getattr(lib, f"{prefix}_full_pass_seconds")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcState), _ip, C.c_int, C.c_int, _ip]
     f.restype = C.c_double
@@ -261,6 +265,10 @@ class Oracle:
 
     def density(self, st, active=None):
         return self._run("density", st, active)
+
+    def density_h_iter_max(self) -> float:
+        """The largest kernel length at which the last density pass took sums (port only)."""
+        return float(getattr(self.lib, f"{self.prefix}_density_h_iter_max")())
 
     def gradients(self, st, active=None):
         return self._run("gradients", st, active)

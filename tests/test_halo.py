@@ -39,12 +39,31 @@ def _oracle_engine(params, local, dens, grad, force):
     st = O.new_state(len(local["mass"]), local)
     orc = O.Oracle(params, "port", n_threads=1)
     assert orc.density(st, dens) == 0
+    h_iter_max = orc.density_h_iter_max()
     assert orc.gradients(st, grad) == 0
     assert orc.force(st, force) == 0
-    return {k: st[k] for k in OUT_FIELDS}
+    out = {k: st[k] for k in OUT_FIELDS}
+    out["h_iter_max"] = h_iter_max
+    return out
 
 
-def _rank(rank, world, port, h, q):
+class _FirstIterationTooLong:
+    """The oracle engine, except that its first call reports a density iteration
+    that took sums at ten times the largest seed: beyond twice any halo depth
+    the pass could have used, so that attempt must be thrown away."""
+
+    def __init__(self):
+        self.calls = 0
+
+    def __call__(self, params, local, dens, grad, force):
+        out = _oracle_engine(params, local, dens, grad, force)
+        if self.calls == 0:
+            out["h_iter_max"] = 10.0 * float(np.max(local["h"]))
+        self.calls += 1
+        return out
+
+
+def _rank(rank, world, port, h, q, engine_kind="oracle"):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
@@ -57,19 +76,20 @@ def _rank(rank, world, port, h, q):
         owner = halo.domain_owner(inputs["pos"], wl.params.box_size, world)
         gid = np.nonzero(owner == rank)[0]
         mine = {k: np.asarray(v)[gid] for k, v in inputs.items()}
-        hp = halo.HaloPass(wl.params, halo.Exchange(rank, world), _oracle_engine)
+        engine = _oracle_engine if engine_kind == "oracle" else _FirstIterationTooLong()
+        hp = halo.HaloPass(wl.params, halo.Exchange(rank, world), engine)
         out = hp(gid, mine)
-        q.put((rank, gid, out, hp.last_radius, hp.last_imported))
+        q.put((rank, gid, out, hp.last_radius, hp.last_imported, hp.last_h_iter_max))
     finally:
         dist.destroy_process_group()
 
 
-def _run_ranks(h, world=2):
+def _run_ranks(h, world=2, engine_kind="oracle"):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, h, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, h, q, engine_kind)) for r in range(world)]
     for p in procs:
         p.start()
     got = [q.get(timeout=600) for _ in range(world)]
@@ -98,9 +118,10 @@ def test_domains_equal_one_domain(seed_scale, world):
     assert orc.density(ref) == 0 and orc.gradients(ref) == 0 and orc.force(ref) == 0
     got = _run_ranks(wl.h, world)
     covered = np.zeros(wl.n, dtype=int)
-    for rank, gid, out, radius, imported in got:
+    for rank, gid, out, radius, imported, h_iter_max in got:
         covered[gid] += 1
         assert imported < wl.n - len(gid)  # the halo left part of the other domains out
+        assert h_iter_max <= radius / 2  # no density sum was taken beyond 2H
         if seed_scale is not None:  # the first halo (4 x 1.1 x the largest seed) was redone deeper
             assert radius > 4.0 * 1.1 * wl.h.max() * 1.2
         for f in OUT_FIELDS:
@@ -110,3 +131,26 @@ def test_domains_equal_one_domain(seed_scale, world):
             else:
                 assert np.array_equal(a, b), (rank, f)
     assert (covered == 1).all()
+
+
+def test_long_intermediate_kernel_length_redoes_the_pass():
+    """A density iteration that took sums beyond twice the halo depth H (here
+    reported by the engine's first call) is thrown away and the pass redone with
+    a deeper halo, although every converged kernel length stayed below H."""
+    from oracle import oracle as O
+    wl = _workload()
+    st = O.new_state(wl.n, wl.inputs())
+    assert O.Oracle(wl.params, "port").density(st) == 0
+    wl.h = st["h"].copy()
+    ref = O.new_state(wl.n, wl.inputs())
+    orc = O.Oracle(wl.params, "port", n_threads=1)
+    assert orc.density(ref) == 0 and orc.gradients(ref) == 0 and orc.force(ref) == 0
+    got = _run_ranks(wl.h, 2, engine_kind="first-too-long")
+    for rank, gid, out, radius, imported, h_iter_max in got:
+        assert radius > 4.0 * 1.1 * wl.h.max() * 1.2  # redone deeper
+        for f in OUT_FIELDS:
+            a, b = np.asarray(out[f]), np.asarray(ref[f])[gid]
+            if f == "dmass":
+                np.testing.assert_allclose(a, b, rtol=0, atol=1e-14 * np.abs(ref[f]).max())
+            else:
+                assert np.array_equal(a, b), (rank, f)
