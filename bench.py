@@ -220,7 +220,7 @@ def cpu_baseline(n1: int, name: str, kind_pref: str = "reference", steps: int = 
 def run_ours(args, world, rank, local):
     import torch
 
-    from gizmo_b200 import abi, ics
+    from gizmo_b200 import abi, accuracy, ics
     from gizmo_b200.hydro import HydroPass
 
     torch.cuda.set_device(local)
@@ -298,52 +298,28 @@ def run_ours(args, world, rank, local):
     value = world * N * K / t_mix
     value64 = world * N * K64 / t_64
 
-    # Accuracy of the mixed form against the FP64 form (same inputs), per particle:
-    #  h, rho, pressure, vsig: |x32 - x64| / |x64|;
-    #  gradients: |g32 - g64| / max(|g64|, 1e-3 max |g64|) (least-squares sums cancel);
-    #  dtmass, accel, dudt: |x32 - x64| / (sum over the row of |pair flux|, in the
-    #  field's units): the rates are sums of fluxes that cancel, so their error is
-    #  stated against the scale of the terms summed (flux_abs, an FP64 diagnostic).
-    fields = ["h", "rho", "pressure", "grad_rho", "grad_p", "grad_v", "accel", "dudt", "dtmass", "vsig"]
+    # Accuracy of the mixed form against the FP64 form (same inputs), per
+    # particle and field (gizmo_b200/accuracy.py): h, rho, pressure, vsig
+    # against |x|; gradients against |g| floored at 1e-6 max |g|; the rates
+    # dtmass, accel, dudt against the pair-flux scale of the particle's force
+    # row (the bar's denominator) and, reported beside it, against |x| floored
+    # at 1e-6 max |x|. The flux scales come from one more FP64 pass with the
+    # flux_abs diagnostic on (off in the timed passes; the outputs are the same).
+    fields = list(accuracy.FIELDS)
     om = hpm.download(fields + ["iters"])
-    # the flux-scale denominators come from one more FP64 pass with the
-    # flux_abs diagnostic on (it is off in the timed passes); the pass's own
-    # outputs are the same with it on or off
+    refined = hpm.status()["pairs_refined"]
     hp64.set_diagnostics(flux_abs=True)
     hp64.restage()
     hp64.full_pass()
     o64 = hp64.download(fields + ["iters", "flux_abs"])
-    fa = o64["flux_abs"]
-    vmag = np.linalg.norm(wl.vel, axis=1)
     mfv = p.method == abi.METHOD_MFV
-    scale = {"dtmass": fa[:, 0],
-             "accel": (fa[:, 1] + (vmag * fa[:, 0] if mfv else 0.0)) / wl.mass,
-             "dudt": (fa[:, 2] + vmag * fa[:, 1] + ((0.5 * vmag ** 2 + wl.u) * fa[:, 0] if mfv else 0.0)) / wl.mass}
-    acc = {}
-    for f in fields:
-        a, b = om[f], o64[f]
-        rowb = np.linalg.norm(b.reshape(N, -1), axis=1)
-        d = np.linalg.norm((a - b).reshape(N, -1), axis=1)
-        if f in scale:
-            den = scale[f]
-        elif f.startswith("grad"):
-            den = np.maximum(rowb, 1e-3 * rowb.max())
-        else:
-            den = rowb
-        rel = d / np.maximum(den, 1e-300)
-        acc[f] = {"max": float(rel.max()), "p99_99": float(np.percentile(rel, 99.99)), "p99": float(np.percentile(rel, 99)),
-                  "p50": float(np.median(rel)), "norm": float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300)),
-                  "above_1e-5": int((rel > 1e-5).sum()), "above_1e-3": int((rel > 1e-3).sum()),
-                  "denominator": "flux scale" if f in scale else ("|x| floored at 1e-3 max" if f.startswith("grad") else "|x|")}
+    scales = accuracy.flux_scales(wl.vel, wl.mass, wl.u, o64["flux_abs"], mfv,
+                                  accuracy.sound_speed(p.gamma, o64["pressure"], o64["rho"]))
+    err = accuracy.per_particle(om, o64, scales)
+    acc = accuracy.summary(err, 1e-5)
     acc["iters_equal_frac"] = float(np.mean(om["iters"] == o64["iters"]))
-    acc["max_over_fields"] = max(v["max"] for k, v in acc.items() if isinstance(v, dict))
     acc["particles"] = N
-    acc["particles_above_1e-5_any_field"] = int(np.count_nonzero(np.any(np.stack(
-        [np.linalg.norm((om[f] - o64[f]).reshape(N, -1), axis=1) / np.maximum(
-            scale[f] if f in scale else (np.maximum(np.linalg.norm(o64[f].reshape(N, -1), axis=1),
-                                                    1e-3 * np.linalg.norm(o64[f].reshape(N, -1), axis=1).max())
-                                         if f.startswith("grad") else np.linalg.norm(o64[f].reshape(N, -1), axis=1)),
-            1e-300) > 1e-5 for f in fields]), axis=0)))
+    acc["pairs_refined_fp64"] = int(refined)
     # conservation per pass (both forms)
     cons = {}
     for tag, o in (("mixed", om), ("fp64", o64)):
@@ -413,8 +389,8 @@ def run_ours(args, world, rank, local):
         elif name == "force":  # FP32 pair arithmetic, each pair evaluated once
             flops, peak, pipe = FLOPS_PER_PAIR["force"] * d["units"], fp32_peak, "fp32"
             e["work"] = f"{FLOPS_PER_PAIR['force']:.0f} flop per pair evaluation"
-        elif name == "gradients":  # FP32 pair arithmetic over every row entry
-            flops, peak, pipe = FLOPS_PER_PAIR["gradients"] * pairs_sym * d["launches"], fp32_peak, "fp32"
+        elif name == "gradients":  # FP64 pair arithmetic (both forms) over every row entry
+            flops, peak, pipe = FLOPS_PER_PAIR["gradients"] * pairs_sym * d["launches"], fp64_peak, "fp64"
             e["work"] = f"{FLOPS_PER_PAIR['gradients']:.0f} flop per row entry"
         if flops is not None:
             ach = flops / (d["ms"] / 1e3) / 1e12
@@ -425,7 +401,7 @@ def run_ours(args, world, rank, local):
     dom = max((k for k in kernels if "achieved" in kernels[k]), key=lambda k: kernels[k]["ms_per_step"], default=None)
     kernel_names = {"density_sums": "k_density_sums<double> (FP64 density sums, all h iterations)",
                     "force": "k_force_pairs<float> (MFV pair flux, each pair once)",
-                    "gradients": "k_gradients<float> (least-squares gradients)"}
+                    "gradients": "k_gradients<double> (least-squares gradients, FP64 in both forms)"}
     roofline = None
     if dom:
         d = kernels[dom]
@@ -446,12 +422,20 @@ def run_ours(args, world, rank, local):
                    "l2": f"inputs larger than L2 (device state {st_mix['device_bytes'] / 1e9:.1f} GB)",
                    "parallelism": f"replicas x{world}", "generate_s": round(t_gen, 1)},
         "fp64_value": value64, "mixed_over_fp64": value / value64,
-        "pass_seconds": {"mixed": parts_mix, "fp64": parts_64},
-        "accuracy_mixed_vs_fp64": acc, "conservation": cons,
-        "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
-        "gpu_launches": launches, "clocks": clocks,
-        "roofline": roofline, "kernels": kernels, "cold_seed": cold,
+        "accuracy_mixed_vs_fp64": {
+            "bar": 1e-5, "particles_above_bar_any_field": acc["particles_above_bar_any_field"],
+            "max_over_fields": acc["max_over_fields"], "pairs_refined_fp64": acc["pairs_refined_fp64"],
+            "max": {f: acc[f]["max"] for f in accuracy.FIELDS},
+            "rates_vs_value_max": {f: acc[f + ":value"]["max"] for f in accuracy.RATE_FIELDS},
+            "denominators": "|x| (h, rho, pressure, vsig); |g| floored at 1e-6 max (gradients); the row's pair-flux "
+                            "scale (rates; gizmo_b200/accuracy.py), and |x| floored at 1e-6 max beside it"},
+        "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
+        "pass_ms": {form: {k: round(1e3 * v, 2) for k, v in parts.items()}
+                    for form, parts in (("mixed", parts_mix), ("fp64", parts_64))},
+        "conservation": cons, "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
     }
+    # the long tables go to stderr (the one stdout line stays short)
+    details = {"accuracy_mixed_vs_fp64": acc, "kernels": kernels, "cold_seed": cold}
 
     # end to end: pinned host buffers in, results out, every step
     if not args.skip_e2e:
@@ -488,6 +472,8 @@ def run_ours(args, world, rank, local):
         result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
                                   "sample": f"one full density->gradients->force pass of a {args.cpu_n1}^3 "
                                             f"({ncpu:,}-particle) instance of the same generator, {secs:.2f} s"}
+    if rank == 0:
+        print(json.dumps(details), file=sys.stderr, flush=True)
     return result
 
 

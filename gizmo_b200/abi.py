@@ -61,6 +61,8 @@ class GzParticles(C.Structure):
         ("dt", _dp),
         ("h", _dp),
         ("cond", _dp),
+        ("timebin", _ip),
+        ("vsig", _dp),
     ]
 
 
@@ -75,7 +77,7 @@ DIAGNOSTIC_FIELDS = [("flux_abs", 3)]
 
 
 class GzOutputs(C.Structure):
-    _fields_ = [(name, _dp) for name, _ in OUTPUT_FIELDS] + [("iters", _ip), ("flux_abs", _dp)]
+    _fields_ = [(name, _dp) for name, _ in OUTPUT_FIELDS] + [("iters", _ip), ("wakeup", _ip), ("flux_abs", _dp)]
 
 
 class GzStatusInfo(C.Structure):
@@ -90,6 +92,7 @@ class GzStatusInfo(C.Structure):
         ("kernel_launches", C.c_int64),
         ("message", C.c_char * 256),
         ("h_iter_max", C.c_double),
+        ("pairs_refined", C.c_int64),
     ]
 
 
@@ -112,8 +115,9 @@ EXPORTED_SYMBOLS = [
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream", "gz_kernel_timing",
     "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
-    "gz_drift",
+    "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins",
 ]
+TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS
 TIMERS = {"density_sums": 0, "walk": 1, "gradients": 2, "force": 3}  # GZ_TIMER_*
@@ -156,6 +160,9 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_kick.argtypes = [C.POINTER(GzParams), C.POINTER(GzKickFields), C.c_int, C.c_double, C.c_double, vp]
     lib.gz_drift.argtypes = [C.POINTER(GzParams), C.POINTER(GzDriftFields), C.c_int64, C.c_double, C.c_double,
                              vp]
+    lib.gz_set_bin_active.argtypes = [vp, _ip]
+    lib.gz_active_list.argtypes = [vp, _ip, _ip, _ip]
+    lib.gz_wakeup_bins.argtypes = [vp, _ip, C.c_int, C.c_int, _ip, _ip]
     for name in EXPORTED_SYMBOLS:
         if name != "gz_stream":
             getattr(lib, name).restype = C.c_int

@@ -2,12 +2,13 @@
 
 Each translation unit is compiled for sm_100a only. The FP64 pair kernels
 (passes_fp64.cu) are compiled with -fmad=false so their products and sums
-round like the reference's CPU build. The FP32 pair kernels of the mixed form
-(passes_mixed.cu) keep FMA and use the approximate FP32 division and square
-root (a few ulp, far inside the form's 1e-5 budget): the face, Riemann and
-limiter arithmetic divides ~25 times per pair, and the IEEE-rounded FP32
-sequences cost several times the approximate ones. Membership, support and
-every FP64 operation are unaffected.
+round like the reference's CPU build; the FP64 re-evaluation of the mixed
+form's fragile force pairs (force_refine) lives there too. The FP32 pair
+kernels of the mixed form (passes_mixed.cu) keep FMA and use the approximate
+FP32 division and square root (a few ulp): the face, Riemann and limiter
+arithmetic divides ~25 times per pair, and the IEEE-rounded FP32 sequences
+cost several times the approximate ones. Those two flags touch FP32
+operations only.
 """
 from __future__ import annotations
 

@@ -47,6 +47,10 @@ struct gz_context {
     DevBuf stage, stage3, perm, inv, keys, keys_sorted, idx, cub_tmp, targets_orig, targets, targets_tmp;
     // resident copies of the uploaded inputs, original order (gz_restage source)
     DevBuf o_vel, o_mass, o_u, o_dt, o_h, o_cond;
+    // individual timesteps: resident inputs (original order), sorted copies, wake-up flags, TimeBinActive
+    DevBuf o_timebin, o_vsig, timebin, vsig_prev, wakeup, binact, sel_flags, sel_out;
+    bool have_bins = false;          // timebin (and vsig) were uploaded
+    bool binact_on = false;          // gz_set_bin_active gave a table
     DevBuf dl;                       // download staging, [9][n] doubles (widest output field)
     DevBuf rec;                      // packed neighbour records of the running pass
     DevBuf work;                     // work counter of the persistent walks
@@ -58,6 +62,8 @@ struct gz_context {
     // density work: rows are [d_beg[t], d_end[t]) in d_nbr; d_used entries are taken
     DevBuf acc, h_built, scratch, keep, regrow, todo_a, todo_b, grow, d_beg, d_end, flag, counts, d_off, d_nbr, n_sel;
     DevBuf hmax;                     // largest kernel length the density iteration took sums at (double bits)
+    DevBuf refined, rq;              // mixed form: count and queue of the force pairs evaluated again in FP64
+    long long pairs_refined = 0;
     double h_iter_max = 0;           // ... read back after the pass
     long long d_nbr_cap = 0, d_used = 0;
     bool dens_all = false;           // the density rows cover every particle (last pass had no active list)
@@ -236,6 +242,12 @@ Particles view(gz_context *c)
     ps.fabs = ptr<double>(c->fabs3);
     ps.iters = ptr<int>(c->iters);
     ps.active = ptr<unsigned char>(c->active);
+    if (c->have_bins) {
+        ps.timebin = ptr<int>(c->timebin);
+        ps.vsig_prev = ptr<double>(c->vsig_prev);
+        ps.wakeup = ptr<int>(c->wakeup);
+        ps.bin_active = c->binact_on ? ptr<int>(c->binact) : nullptr;
+    }
     return ps;
 }
 
@@ -248,7 +260,8 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->targets, &c->targets_tmp, &c->t_node, &c->t_lo, &c->t_hi, &c->t_parent, &c->t_done, &c->t_nch,
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
-            &c->s_counts, &c->rec, &c->work, &c->hmax, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl};
+            &c->s_counts, &c->rec, &c->work, &c->hmax, &c->refined, &c->rq, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl, &c->o_timebin,
+            &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out};
 }
 
 Tree tree_view(gz_context *c)
@@ -285,6 +298,52 @@ __global__ void k_gather1(int n, const int *__restrict__ perm, const double *__r
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < n) dst[s] = src[perm[s]];
+}
+
+__global__ void k_gather_int(int n, const int *__restrict__ perm, const int *__restrict__ src, int *dst)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[s] = src[perm[s]];
+}
+
+// flag[i] = 1 for a cell of an active bin with positive mass, original order
+// (make_list_of_active_particles, core/run.cc:997-1010)
+__global__ void k_active_flags(int n, const int *__restrict__ timebin, const double *__restrict__ mass,
+                               const int *__restrict__ bin_active, int *flag)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = (bin_active[timebin[i]] && mass[i] > 0) ? 1 : 0;
+}
+
+// process_wake_ups' bin rule (core/timestep.cc:1565-1700), per sorted cell, written in original order
+__global__ void k_wakeup_bins(int n, const int *__restrict__ perm, const int *__restrict__ timebin,
+                              const int *__restrict__ wakeup, const double *__restrict__ mass,
+                              const int *__restrict__ bin_active, int max_active, int lowest, int *out,
+                              unsigned long long *moved)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool mv = false;
+    if (s < n) {
+        const int binold = timebin[s];
+        int bin = binold;
+        if (wakeup[s] && mass[s] > 0 && !bin_active[binold]) {
+            int offset = 0;  // the bins WAKEUP spans: the smallest k with 2^k >= WAKEUP
+            while ((double)(1ll << offset) < kWakeup) offset++;
+            if (wakeup[s] > 0) {
+                bin = wakeup[s] - 1 - offset;  // wakeup_timebin_from_flag, core/proto.h:182
+                if (bin < 0) bin = 0;
+                if (bin < lowest) bin = lowest;
+            } else {
+                bin = max_active;
+            }
+            if (bin > max_active) bin = max_active;
+            if (bin >= binold) bin = binold;
+        }
+        out[perm[s]] = bin;
+        mv = bin != binold;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, mv);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(moved, (unsigned long long)__popc(b));
 }
 
 __global__ void k_inverse(int n, const int *__restrict__ perm, int *inv)
@@ -334,14 +393,16 @@ __global__ void k_density_prep(int na, const int *__restrict__ t, double *h, dou
                                unsigned long long *hmax)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= na) return;
-    const int i = t[a];
-    double hv = h[i];
-    if ((hv < 0) || !isfinite(hv) || (hv > 0.99 * maxsoft)) hv = 0.99 * maxsoft;  // density_loop.cc:837-840
-    h[i] = hv;
-    atomicMax(hmax, (unsigned long long)__double_as_longlong(hv));  // hv >= 0: bits order like values
-    DensityScratch z{};
-    sc[i] = z;
+    double hv = 0;
+    if (a < na) {
+        const int i = t[a];
+        hv = h[i];
+        if ((hv < 0) || !isfinite(hv) || (hv > 0.99 * maxsoft)) hv = 0.99 * maxsoft;  // density_loop.cc:837-840
+        h[i] = hv;
+        DensityScratch z{};
+        sc[i] = z;
+    }
+    warp_atomic_max_nonneg(hmax, hv);  // every lane of the (whole) block's warps
 }
 
 // search radius of the density rows about to be built for t[0..na)
@@ -796,6 +857,12 @@ static int stage_inputs(gz_context *c)
             k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(*f.src), ptr<double>(*f.dst));
             c->launches += 1;
         }
+        if (c->have_bins) {
+            k_gather_int<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->o_timebin), ptr<int>(c->timebin));
+            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->o_vsig), ptr<double>(c->vsig_prev));
+            GZ_CUDA(c, cudaMemsetAsync(c->wakeup.p, 0, sizeof(int) * (size_t)n, s));
+            c->launches += 2;
+        }
         DevBuf *zero[] = {&c->num_ngb, &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig,
                           &c->dtmass, &c->dmass};
         for (DevBuf *b : zero) GZ_CUDA(c, cudaMemsetAsync(b->p, 0, sizeof(double) * (size_t)n, s));
@@ -850,6 +917,22 @@ int gz_upload(gz_context *c, const gz_particles *in)
         for (auto &f : f1) {
             if (f.src) GZ_CUDA(c, cudaMemcpyAsync(f.dst->p, f.src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
             else GZ_CUDA(c, cudaMemsetAsync(f.dst->p, 0, sizeof(double) * (size_t)n, s));
+        }
+    }
+    c->have_bins = in->timebin != nullptr;
+    if (c->have_bins) {
+        if (ensure(c, c->o_timebin, sizeof(int) * N) || ensure(c, c->o_vsig, sizeof(double) * N) ||
+            ensure(c, c->timebin, sizeof(int) * N) || ensure(c, c->vsig_prev, sizeof(double) * N) ||
+            ensure(c, c->wakeup, sizeof(int) * N))
+            return c->err;
+        for (int k = 0; k < n; k++)
+            if (in->timebin[k] < 0 || in->timebin[k] >= GZ_TIMEBINS) return fail(c, GZ_ERR_ARG, "timebin out of range");
+        if (n > 0) {
+            GZ_CUDA(c, cudaMemcpyAsync(c->o_timebin.p, in->timebin, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+            if (in->vsig)
+                GZ_CUDA(c, cudaMemcpyAsync(c->o_vsig.p, in->vsig, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+            else
+                GZ_CUDA(c, cudaMemsetAsync(c->o_vsig.p, 0, sizeof(double) * (size_t)n, s));
         }
     }
     if (stage_inputs(c)) return c->err;
@@ -995,10 +1078,11 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
     const EventPair *ev = na > 0 ? timer_launch(c, GZ_TIMER_GRADIENTS, na) : nullptr;
-    if (c->prm.precision == GZ_PRECISION_MIXED)
-        gradients_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
-    else
-        gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
+    // Both forms take the gradient pair terms in FP64: the pass is bound by its
+    // record gathers, not by arithmetic (FP32 terms saved 0.6 of 26 ms per step
+    // at 256^3), and FP64 gradients make the mixed form's force inputs the FP64
+    // form's exactly (FP32 terms left 9 of 16.8M particles above 1e-5).
+    gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
     if (na > 0) c->launches++;
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
@@ -1026,28 +1110,57 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     }
     Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
     Particles ps = view(c);
+    if (c->have_bins && c->n > 0) GZ_CUDA(c, cudaMemsetAsync(c->wakeup.p, 0, sizeof(int) * (size_t)c->n, c->stream));
     force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
     c->fabs_valid = c->pp.diag_flux_abs != 0;
-    // every particle a target: each pair evaluated once, its flux kept per row
-    // entry (when that scratch can be had; otherwise each row evaluates all)
+    // The pairs go through a flux per row entry when that scratch can be had:
+    // every particle a target -> each pair evaluated once; an active subset ->
+    // each row entry. The mixed form needs it (its fragile pairs are evaluated
+    // again in FP64 there); the FP64 form otherwise evaluates the rows in place.
     const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
+    const bool all = active == nullptr && na == c->n && c->n > 0;
     void *flux = nullptr;
-    if (active == nullptr && na == c->n && c->n > 0 &&
-        try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)))
+    if (na > 0 && try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)std::max(c->pairs_symmetric, 1ll)))
         flux = c->pflux.p;
-    // the rows' sums before the writeback go to the density accumulators
-    // (17 x n doubles, unused between density passes)
-    const EventPair *ev = na > 0 ? timer_launch(c, GZ_TIMER_FORCE, flux ? c->pairs_symmetric / 2 : c->pairs_symmetric)
-                                 : nullptr;
-    if (mixed)
-        force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                    ptr<double>(c->acc), ev, c->stream);
-    else
-        force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p, flux,
-                   ptr<double>(c->acc), ev, c->stream);
-    if (na > 0) c->launches += flux ? 4 : 3;
-    GZ_CUDA(c, cudaGetLastError());
+    if (mixed && na > 0 && !flux) return fail(c, GZ_ERR_CAPACITY, "mixed-form force pass: no room for the pair fluxes");
+    // Mixed form: queue room for one pair in 8 of the pass (about one in 700 is
+    // queued on the Plummer mixture, one in 130 on the log-normal field). A pass
+    // over every particle that queued more runs again with room for all of
+    // them; an active subset cannot (its j-side mass writes would count twice).
+    long long cap = mixed ? std::max(65536ll, c->pairs_symmetric / 8) : 0;
+    unsigned long long refined = 0;
+    for (int attempt = 0;; attempt++) {
+        RefineQueue q{nullptr, nullptr, 0};
+        if (mixed) {
+            if (ensure(c, c->refined, sizeof(unsigned long long)) || ensure(c, c->rq, sizeof(RefineItem) * (size_t)cap))
+                return c->err;
+            GZ_CUDA(c, cudaMemsetAsync(c->refined.p, 0, sizeof(unsigned long long), c->stream));
+            q = RefineQueue{ptr<RefineItem>(c->rq), ptr<unsigned long long>(c->refined), cap};
+        }
+        // the rows' sums before the writeback go to the density accumulators
+        // (17 x n doubles, unused between density passes)
+        const EventPair *ev =
+            na > 0 ? timer_launch(c, GZ_TIMER_FORCE, (flux && all) ? c->pairs_symmetric / 2 : c->pairs_symmetric)
+                   : nullptr;
+        if (mixed)
+            force_mixed(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p,
+                        flux, all, q, ptr<double>(c->acc), ev, c->stream);
+        else
+            force_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p,
+                       flux, all, ptr<double>(c->acc), ev, c->stream);
+        if (na > 0) c->launches += flux ? (mixed ? 5 : 4) : 3;
+        GZ_CUDA(c, cudaGetLastError());
+        if (!q.item) break;
+        GZ_CUDA(c, cudaMemcpyAsync(&refined, c->refined.p, sizeof(refined), cudaMemcpyDeviceToHost, c->stream));
+        GZ_CUDA(c, cudaStreamSynchronize(c->stream));
+        if ((long long)refined <= cap) break;
+        if (!all || attempt > 0)
+            return fail(c, GZ_ERR_CAPACITY, "mixed-form force pass: more fragile pairs than the refine queue holds");
+        cap = (long long)refined;
+        force_preloop(c->pp, ps, ptr<int>(c->targets), na, c->stream);
+    }
     if (read_status(c)) return c->err;
+    c->pairs_refined = (long long)refined;
     return GZ_OK;
 }
 
@@ -1095,6 +1208,13 @@ int gz_download(gz_context *c, const gz_outputs *o)
         k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters), ptr<int>(c->dl));
         c->launches++;
         GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+    }
+    if (o->wakeup) {
+        if (!c->have_bins) return fail(c, GZ_ERR_ORDER, "wakeup: no timebins were uploaded");
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->wakeup), ptr<int>(c->dl));
+        c->launches++;
+        GZ_CUDA(c, cudaMemcpyAsync(o->wakeup, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
     }
     GZ_CUDA(c, cudaGetLastError());
     GZ_CUDA(c, cudaStreamSynchronize(s));
@@ -1232,6 +1352,90 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
     return read_status(c) ? c->err : GZ_OK;
 }
 
+int gz_set_bin_active(gz_context *c, const int *bin_active)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!bin_active) { c->binact_on = false; return GZ_OK; }
+    if (ensure(c, c->binact, sizeof(int) * GZ_TIMEBINS)) return c->err;
+    GZ_CUDA(c, cudaMemcpyAsync(c->binact.p, bin_active, sizeof(int) * GZ_TIMEBINS, cudaMemcpyHostToDevice, c->stream));
+    GZ_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->binact_on = true;
+    return GZ_OK;
+}
+
+int gz_active_list(gz_context *c, const int *bin_active, int *out, int *n_out)
+{
+    if (!c || !bin_active || !n_out) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid || !c->have_bins) return fail(c, GZ_ERR_ORDER, "active list: no timebins were uploaded");
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)std::max(n, 1);
+    DevBuf tab;  // this call's table; the wake-up keeps the one gz_set_bin_active gave
+    if (ensure(c, tab, sizeof(int) * GZ_TIMEBINS) || ensure(c, c->sel_flags, sizeof(int) * N) ||
+        ensure(c, c->sel_out, sizeof(int) * N) || ensure(c, c->n_sel, sizeof(int) * 2) ||
+        ensure(c, c->targets_tmp, sizeof(int) * N))
+        return c->err;
+    GZ_CUDA(c, cudaMemcpyAsync(tab.p, bin_active, sizeof(int) * GZ_TIMEBINS, cudaMemcpyHostToDevice, s));
+    *n_out = 0;
+    if (n > 0) {
+        k_iota<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->targets_tmp));
+        k_active_flags<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->o_timebin), ptr<double>(c->o_mass), ptr<int>(tab),
+                                                       ptr<int>(c->sel_flags));
+        c->launches += 2;
+        size_t tmp = 0;
+        cub::DeviceSelect::Flagged(nullptr, tmp, ptr<int>(c->targets_tmp), ptr<int>(c->sel_flags), ptr<int>(c->sel_out),
+                                   ptr<int>(c->n_sel), n, s);
+        if (ensure(c, c->cub_tmp, tmp)) { release(tab); return c->err; }
+        cub::DeviceSelect::Flagged(c->cub_tmp.p, tmp, ptr<int>(c->targets_tmp), ptr<int>(c->sel_flags),
+                                   ptr<int>(c->sel_out), ptr<int>(c->n_sel), n, s);
+        int k = 0;
+        GZ_CUDA(c, cudaMemcpyAsync(&k, c->n_sel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+        *n_out = k;
+        if (out && k > 0) {
+            GZ_CUDA(c, cudaMemcpyAsync(out, c->sel_out.p, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost, s));
+            GZ_CUDA(c, cudaStreamSynchronize(s));
+        }
+    }
+    release(tab);
+    GZ_CUDA(c, cudaGetLastError());
+    return GZ_OK;
+}
+
+int gz_wakeup_bins(gz_context *c, const int *bin_active, int max_time_bin_active, int lowest_occupied_active_bin,
+                   int *timebin_out, int *n_moved)
+{
+    if (!c || !bin_active || !timebin_out) return GZ_ERR_ARG;
+    if (max_time_bin_active < 0 || max_time_bin_active >= GZ_TIMEBINS) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid || !c->have_bins) return fail(c, GZ_ERR_ORDER, "wakeup bins: no timebins were uploaded");
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    DevBuf tab, moved;
+    if (ensure(c, tab, sizeof(int) * GZ_TIMEBINS) || ensure(c, moved, sizeof(unsigned long long)) ||
+        ensure(c, c->dl, sizeof(double) * 9 * (size_t)std::max(n, 1)))
+        return c->err;
+    GZ_CUDA(c, cudaMemcpyAsync(tab.p, bin_active, sizeof(int) * GZ_TIMEBINS, cudaMemcpyHostToDevice, s));
+    GZ_CUDA(c, cudaMemsetAsync(moved.p, 0, sizeof(unsigned long long), s));
+    unsigned long long m = 0;
+    if (n > 0) {
+        k_wakeup_bins<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->timebin), ptr<int>(c->wakeup),
+                                                      ptr<double>(c->m), ptr<int>(tab), max_time_bin_active,
+                                                      lowest_occupied_active_bin, ptr<int>(c->dl),
+                                                      ptr<unsigned long long>(moved));
+        c->launches++;
+        GZ_CUDA(c, cudaMemcpyAsync(timebin_out, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaMemcpyAsync(&m, moved.p, sizeof(m), cudaMemcpyDeviceToHost, s));
+    }
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    release(tab);
+    release(moved);
+    if (n_moved) *n_moved = (int)m;
+    return GZ_OK;
+}
+
 int gz_status(gz_context *c, gz_status_info *info)
 {
     if (!c || !info) return GZ_ERR_ARG;
@@ -1249,6 +1453,7 @@ int gz_status(gz_context *c, gz_status_info *info)
     }
     info->density_iterations = c->last_iters;
     info->h_iter_max = c->h_iter_max;
+    info->pairs_refined = c->pairs_refined;
     info->kernel_launches = c->launches;
     info->pairs_density = c->pairs_density;
     info->pairs_symmetric = c->pairs_symmetric;

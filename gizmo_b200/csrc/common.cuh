@@ -65,6 +65,22 @@ GZ_DEV uint32_t compact3(uint32_t x)
     return x;
 }
 
+// Raises *slot (non-negative doubles as their bit patterns, which order like
+// the values) to the largest v of the warp; every lane of the warp calls it,
+// at one call site (a lane with nothing to report passes 0). One lane reads
+// the slot and takes the atomic only when the warp's maximum is larger, so a
+// launch of millions of threads costs a few atomics, not millions on one
+// address.
+GZ_DEV void warp_atomic_max_nonneg(unsigned long long *slot, double v)
+{
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+        if (x > b) b = x;
+    }
+    if ((threadIdx.x & 31) == 0 && b > *(volatile unsigned long long *)slot) atomicMax(slot, b);
+}
+
 GZ_DEV double warp_sum(double v, unsigned mask, int width)
 {
     for (int o = width / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, width);

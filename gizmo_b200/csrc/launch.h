@@ -66,15 +66,21 @@ size_t force_record_bytes(int mixed);  // the force record and the gather record
 size_t pair_flux_bytes(int mixed);  // per symmetric row entry, for a force pass evaluating each pair once
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
                     void *rec, const EventPair *ev, cudaStream_t s);
-void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     void *rec, const EventPair *ev, cudaStream_t s);
 // flux: NULL, or (every particle a target, targets[s] = s) scratch for one
 // evaluation per pair: n_entries x pair_flux_bytes. sums: 13 x n doubles of
 // scratch (the row sums before the writeback).
+// `all`: every particle is a target (flux then holds each pair once). The
+// mixed form needs flux; q receives its fragile pairs (cap >= 1).
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s);
+                DevStatus *st, void *rec, void *flux, bool all, double *sums, const EventPair *ev, cudaStream_t s);
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s);
+                 DevStatus *st, void *rec, void *flux, bool all, const RefineQueue &q, double *sums,
+                 const EventPair *ev, cudaStream_t s);
+// The queued pairs of a mixed-form pass evaluated in FP64 from the FP64 mirror
+// (the FP64 form's arithmetic bit for bit), their fluxes stored over the FP32
+// ones at both entries; the queue's count stays on the device.
+void force_refine(const PassParams &p, const Particles &ps, const RefineQueue &q, PairFlux<float> *flux,
+                  DevStatus *st, cudaStream_t s);
 void force_preloop(const PassParams &p, const Particles &ps, const int *targets, int n_targets, cudaStream_t s);
 
 }  // namespace gz

@@ -9,6 +9,8 @@
 // epilogue (finalize) in FP64.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "launch.h"
 
 namespace gz {
@@ -343,6 +345,17 @@ template <typename T> GZ_DEV void load_side(const Particles &ps, int i, double g
     S.prd = P / rho;
 }
 
+// Gas-gamma constants of the Riemann solvers (GAMMA_G0..G9, reimann.h:1-10).
+template <typename T> GZ_DEV GConst<T> make_gconst(double G0, int mfv)
+{
+    GConst<T> gc;
+    gc.G0 = T(G0); gc.G1 = T((G0 - 1.0) / (2.0 * G0)); gc.G2 = T((G0 + 1.0) / (2.0 * G0));
+    gc.G3 = T((2.0 * G0 / (G0 - 1.0))); gc.G4 = T(2.0 / (G0 - 1.0)); gc.G5 = T(2.0 / (G0 + 1.0));
+    gc.G6 = T((G0 - 1.0) / (G0 + 1.0)); gc.G7 = T(0.5 * (G0 - 1.0)); gc.G8 = T(1.0 / G0); gc.G9 = T(G0 - 1.0);
+    gc.mfv = mfv;
+    return gc;
+}
+
 // What a force row reads of each neighbour: FP64 position, h, mass and
 // density (membership, the j filters, the MFV mass bookkeeping), the
 // particle's side of the face in the pair type, and whether it is active
@@ -416,14 +429,7 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
     const int i = targets[slot];
     const size_t n = (size_t)ps.n;
     const int mfv = p.method == 1;
-    GConst<T> gc;
-    {
-        const double G0 = p.gamma;
-        gc.G0 = T(G0); gc.G1 = T((G0 - 1.0) / (2.0 * G0)); gc.G2 = T((G0 + 1.0) / (2.0 * G0));
-        gc.G3 = T((2.0 * G0 / (G0 - 1.0))); gc.G4 = T(2.0 / (G0 - 1.0)); gc.G5 = T(2.0 / (G0 + 1.0));
-        gc.G6 = T((G0 - 1.0) / (G0 + 1.0)); gc.G7 = T(0.5 * (G0 - 1.0)); gc.G8 = T(1.0 / G0); gc.G9 = T(G0 - 1.0);
-        gc.mfv = mfv;
-    }
+    const GConst<T> gc = make_gconst<T>(p.gamma, mfv);
     const double mi = ps.m[i], rhoi = ps.rho[i];
     const bool enabled = (mi > 0 && rhoi > 0);
     const double xi = ps.x[i], yi = ps.y[i], zi = ps.z[i], hid = ps.h[i], dti = ps.dt[i];
@@ -470,9 +476,11 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
                 const T dp[3] = {T(sgn * dx), T(sgn * dy), T(sgn * dz)};
                 // both sides are read from the records in place (global memory, L1-resident)
                 const ForceRec<T> *pl = fwd ? rip : rjp, *pr = fwd ? rjp : rip;
+                Guard<T> g;  // kBoth runs in the FP64 form only (the mixed form goes through the flux buffer)
                 force_pair(p.kernel, mfv, p.selfgravity_off, gc, pl->s, pr->s, dp, r2, fwd ? hid : hjd,
-                           fwd ? hjd : hid, F, stop);
+                           fwd ? hjd : hid, F, stop, g);
                 if (!F.valid) continue;
+                wakeup_test(ps, i, j, (double)F.vsig_ts);
             }
             const double sign = (i < j) ? 1.0 : -1.0;
             const double frho = sign * (double)F.rho;
@@ -588,9 +596,30 @@ __global__ void __launch_bounds__(256) k_force_finish(PassParams p, Particles ps
 // fluxes.
 constexpr int kPairRows = 32;
 
+// Queues this lane's pair for the FP64 re-evaluation when `fragile`. Called by
+// every lane that reaches it; the lanes that arrive together take one atomic
+// for all of their pushes (the count is one address for the whole launch).
+GZ_DEV void push_refine(const RefineQueue &q, bool fragile, long long e, long long a, int i, int j, int t)
+{
+    namespace cg = cooperative_groups;
+    if (!q.item) return;
+    const cg::coalesced_group grp = cg::coalesced_threads();
+    const unsigned want = grp.ballot(fragile);
+    if (!want) return;
+    const unsigned below = want & ((1u << grp.thread_rank()) - 1u);
+    unsigned long long base = 0;
+    if (grp.thread_rank() == (unsigned)(__ffs(want) - 1)) base = atomicAdd(q.count, (unsigned long long)__popc(want));
+    base = grp.shfl(base, __ffs(want) - 1);
+    if (fragile) {
+        const unsigned long long k = base + __popc(below);
+        if ((long long)k < q.cap) q.item[k] = RefineItem{e, a, i, j, t, 0};
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps, int n_rows, Csr rows, DevStatus *st,
-                                                     const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux)
+                                                     const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux,
+                                                     RefineQueue q)
 {
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -619,14 +648,7 @@ __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps,
     }
     const int total = __shfl_sync(full, incl, 31);
     const int mfv = p.method == 1;
-    GConst<T> gc;
-    {
-        const double G0 = p.gamma;
-        gc.G0 = T(G0); gc.G1 = T((G0 - 1.0) / (2.0 * G0)); gc.G2 = T((G0 + 1.0) / (2.0 * G0));
-        gc.G3 = T((2.0 * G0 / (G0 - 1.0))); gc.G4 = T(2.0 / (G0 - 1.0)); gc.G5 = T(2.0 / (G0 + 1.0));
-        gc.G6 = T((G0 - 1.0) / (G0 + 1.0)); gc.G7 = T(0.5 * (G0 - 1.0)); gc.G8 = T(1.0 / G0); gc.G9 = T(G0 - 1.0);
-        gc.mfv = mfv;
-    }
+    const GConst<T> gc = make_gconst<T>(p.gamma, mfv);
     int stop = 0, stop_index = -1;
     for (int base = 0; base < total; base += 32) {
         const int f = base + lane;
@@ -651,12 +673,15 @@ __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps,
         F.rho = F.p = T(0);
         F.v[0] = F.v[1] = F.v[2] = T(0);
         F.vsig_ts = T(0);
+        Guard<T> g;
         if (rip->m > 0 && rip->rho > 0 && rjp->m > 0 && rjp->rho > 0) {
             double dx, dy, dz;
             const double r2 = sep2(rip->x, rip->y, rip->z, rjp->x, rjp->y, rjp->z, p.box, p.half, dx, dy, dz);
             const T dp[3] = {T(dx), T(dy), T(dz)};
             int pstop = 0;
-            force_pair(p.kernel, mfv, p.selfgravity_off, gc, rip->s, rjp->s, dp, r2, rip->h, rjp->h, F, pstop);
+            force_pair(p.kernel, mfv, p.selfgravity_off, gc, rip->s, rjp->s, dp, r2, rip->h, rjp->h, F, pstop, g);
+            // a fragile pair's flux (and stop code) comes from its FP64 evaluation, queued below
+            if (g.fragile()) pstop = 0;
             if (pstop && !stop) { stop = pstop; stop_index = i; }
         }
         flux[e] = F;
@@ -672,6 +697,83 @@ __global__ void __launch_bounds__(128) k_force_pairs(PassParams p, Particles ps,
             continue;
         }
         flux[a] = F;
+        push_refine(q, g.fragile(), e, a, i, j, -1);
+    }
+    if (stop) record_status(st, stop, stop_index);
+}
+
+// Every entry of the rows of a pass over an active subset, each written at its
+// own entry: a pair of two active particles is evaluated once per row, as the
+// reference does, in the canonical orientation (lower sorted index as the i
+// side), so both evaluations are bit-identical. A warp takes kPairRows rows and
+// spreads their entries over its lanes, one entry per lane per round; the flux
+// goes to k_force<kGather> like the pairs of a pass over every particle. The
+// wake-up test of an inactive neighbour (hydro_functions.h:534-544) runs here.
+template <typename T>
+__global__ void __launch_bounds__(128) k_force_entries(PassParams p, Particles ps, const int *__restrict__ targets,
+                                                       int n_rows, Csr rows, DevStatus *st,
+                                                       const ForceRec<T> *__restrict__ rec, PairFlux<T> *flux,
+                                                       RefineQueue q)
+{
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long r0 = warp * kPairRows;
+    if (r0 >= n_rows) return;  // the whole warp leaves together
+    const unsigned full = 0xffffffffu;
+    long long first = 0;
+    int cnt = 0;
+    if (lane < kPairRows && r0 + lane < n_rows) {
+        first = rows.off[r0 + lane];
+        cnt = (int)(rows.off[r0 + lane + 1] - first);
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(full, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    const int mfv = p.method == 1;
+    const GConst<T> gc = make_gconst<T>(p.gamma, mfv);
+    int stop = 0, stop_index = -1;
+    for (int base = 0; base < total; base += 32) {
+        const int f = base + lane;
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int v = __shfl_sync(full, incl, k + step - 1);
+            if (v <= f) k += step;
+        }
+        const int excl_k = __shfl_sync(full, incl - cnt, k);
+        const long long first_k = __shfl_sync(full, first, k);
+        if (f >= total) continue;
+        const int t = targets[r0 + k];
+        const long long e = first_k + (f - excl_k);
+        const int j = rows.nbr[e];
+        const int lo = t < j ? t : j, hi = t < j ? j : t;
+        const ForceRec<T> rl = ldg_record(rec + lo), rh = ldg_record(rec + hi);
+        PairFlux<T> F;
+        F.valid = 0;
+        F.rho = F.p = T(0);
+        F.v[0] = F.v[1] = F.v[2] = T(0);
+        F.vsig_ts = T(0);
+        Guard<T> g;
+        if (rl.m > 0 && rl.rho > 0 && rh.m > 0 && rh.rho > 0) {
+            double dx, dy, dz;
+            const double r2 = sep2(rl.x, rl.y, rl.z, rh.x, rh.y, rh.z, p.box, p.half, dx, dy, dz);
+            const T dp[3] = {T(dx), T(dy), T(dz)};
+            int pstop = 0;
+            force_pair(p.kernel, mfv, p.selfgravity_off, gc, rl.s, rh.s, dp, r2, rl.h, rh.h, F, pstop, g);
+            // the wake-up test of an inactive neighbour, on the pair's signal speed
+            const bool wake_test = F.valid && ps.bin_active && !ps.bin_active[ps.timebin[j]];
+            const double wake_at = wake_test ? kWakeup * ps.vsig_prev[j] : 0.0;
+            if (wake_test) g.near(F.vsig_ts, T(wake_at), F.vsig_ts, 38);
+            if (g.fragile()) pstop = 0;
+            else if (wake_test && (double)F.vsig_ts > wake_at) atomicMax(ps.wakeup + j, ps.timebin[t] + 1);
+            if (pstop && !stop) { stop = pstop; stop_index = t; }
+        }
+        flux[e] = F;
+        push_refine(q, g.fragile(), e, -1, lo, hi, t);
     }
     if (stop) record_status(st, stop, stop_index);
 }
@@ -693,12 +795,16 @@ void launch_force_mode(const PassParams &p, const Particles &ps, const int *targ
     k_force_finish<T><<<(unsigned)((n_targets + 255) / 256), 256, 0, s>>>(p, ps, targets, n_targets, sums);
 }
 
-// `flux` (one PairFlux<T> per row entry) given: every particle is a target
-// (targets[s] = s) and each pair is evaluated once; otherwise (NULL) each row
-// evaluates all its pairs. `sums`: kRowSums x n doubles of scratch.
+// With `fluxbuf` (one PairFlux<T> per row entry) the pairs are evaluated into
+// it -- each pair once when `all` (every particle a target, targets[s] = s),
+// otherwise each row entry -- the mixed form's fragile pairs are evaluated
+// again in FP64 (force_refine), and k_force<kGather> accumulates the rows;
+// without it (the FP64 form only) each row evaluates all its pairs in place.
+// `sums`: kRowSums x n doubles of scratch.
 template <typename T>
 void launch_force(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                  DevStatus *st, void *recbuf, void *fluxbuf, double *sums, const EventPair *ev, cudaStream_t s)
+                  DevStatus *st, void *recbuf, void *fluxbuf, bool all, const RefineQueue &q, double *sums,
+                  const EventPair *ev, cudaStream_t s)
 {
     if (n_targets <= 0) return;
     // the record scratch holds the force records, then the gather records
@@ -710,13 +816,16 @@ void launch_force(const PassParams &p, const Particles &ps, const int *targets, 
         PairFlux<T> *flux = (PairFlux<T> *)fluxbuf;
         const long long warps = (n_targets + kPairRows - 1) / kPairRows;
         if (ev) cudaEventRecord(ev->start, s);
-        k_force_pairs<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, n_targets, rows, st, rec, flux);
+        if (all) k_force_pairs<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, n_targets, rows, st, rec, flux, q);
+        else k_force_entries<T><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(p, ps, targets, n_targets, rows, st, rec,
+                                                                            flux, q);
         if (ev) cudaEventRecord(ev->stop, s);
+        if constexpr (sizeof(T) == sizeof(float)) force_refine(p, ps, q, flux, st, s);
         // one thread per row: the gather's per-entry work is short, and lanes
         // sharing a row would spend more on the cross-lane reduction and on
         // idling at the row's end than on the entries themselves
         launch_force_mode<T, kGather>(p, ps, targets, n_targets, rows, 1, st, rec, grec, flux, sums, s);
-    } else {
+    } else if constexpr (sizeof(T) == sizeof(double)) {
         if (ev) cudaEventRecord(ev->start, s);  // (also spans the writeback kernel)
         launch_force_mode<T, kBoth>(p, ps, targets, n_targets, rows, tpt, st, rec, grec, nullptr, sums, s);
         if (ev) cudaEventRecord(ev->stop, s);

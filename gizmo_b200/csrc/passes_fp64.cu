@@ -43,9 +43,60 @@ void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets
 }
 
 void force_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s)
+                DevStatus *st, void *rec, void *flux, bool all, double *sums, const EventPair *ev, cudaStream_t s)
 {
-    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, ev, s);
+    const RefineQueue none{nullptr, nullptr, 0};
+    launch_force<double>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, all, none, sums, ev, s);
+}
+
+// force_refine: one thread per queued pair, grid-stride over the count the
+// pair kernel left on the device. The pair is the FP64 form's: Side<double>
+// from the FP64 mirror exactly as k_pack_force<double> packs it, the same
+// minimum-image separation and the same force_pair<double> call in this
+// unit's arithmetic (no contraction), so the flux is the FP64 form's bit for
+// bit before it is rounded to the FP32 flux entry. The wake-up test of a pair
+// of an active-subset pass is taken here too, on the FP64 signal speed.
+__global__ void __launch_bounds__(128) k_force_refine(PassParams p, Particles ps, RefineQueue q,
+                                                      PairFlux<float> *flux, DevStatus *st)
+{
+    const unsigned long long pushed = *q.count;  // beyond cap: the host redoes the pass with a longer queue
+    const long long n = (long long)pushed < q.cap ? (long long)pushed : q.cap;
+    const int mfv = p.method == 1;
+    const GConst<double> gc = make_gconst<double>(p.gamma, mfv);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const RefineItem it = q.item[k];
+        Side<double> A, B;
+        load_side(ps, it.i, p.gamma, A);
+        load_side(ps, it.j, p.gamma, B);
+        double dx, dy, dz;
+        const double r2 = sep2(ps.x[it.i], ps.y[it.i], ps.z[it.i], ps.x[it.j], ps.y[it.j], ps.z[it.j], p.box, p.half,
+                               dx, dy, dz);
+        const double dp[3] = {dx, dy, dz};
+        PairFlux<double> F64;
+        int stop = 0;
+        Guard<double> g;
+        force_pair(p.kernel, mfv, p.selfgravity_off, gc, A, B, dp, r2, ps.h[it.i], ps.h[it.j], F64, stop, g);
+        if (stop) record_status(st, stop, it.i);
+        PairFlux<float> F;
+        F.rho = (float)F64.rho;
+        F.p = (float)F64.p;
+        F.v[0] = (float)F64.v[0]; F.v[1] = (float)F64.v[1]; F.v[2] = (float)F64.v[2];
+        F.vsig_ts = (float)F64.vsig_ts;
+        F.valid = F64.valid;
+        flux[it.e] = F;
+        if (it.a >= 0) flux[it.a] = F;
+        if (it.t >= 0 && F64.valid) wakeup_test(ps, it.t, it.t == it.i ? it.j : it.i, F64.vsig_ts);
+    }
+}
+
+void force_refine(const PassParams &p, const Particles &ps, const RefineQueue &q, PairFlux<float> *flux,
+                  DevStatus *st, cudaStream_t s)
+{
+    if (!q.item) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_force_refine<<<sms * 4, 128, 0, s>>>(p, ps, q, flux, st);
 }
 
 // DensitySpec::after_iter_body per iterating particle, plus the runner's
@@ -53,28 +104,31 @@ void force_fp64(const PassParams &p, const Particles &ps, const int *targets, in
 __global__ void k_after_iter(PassParams p, Particles ps, DensityWork w, DevStatus *st)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= w.n_todo) return;
-    const int t = w.todo[s];
-    const size_t n = (size_t)ps.n;
-    double acc[14];
-    for (int k = 0; k < 14; k++) acc[k] = w.acc[k * n + t];
-    const double h = ps.h[t];
-    DensityScratch sc = w.scratch[t];
-    double nh = h;
-    int stop = 0;
-    const int conv = after_iter(p, w.iter, h, acc, ps.cond[t], sc, nh, stop);
-    w.scratch[t] = sc;
-    ps.iters[t] = w.iter + 1;
-    if (stop) record_status(st, stop, t);
-    int regrow = 0;
-    if (!conv) {
-        ps.h[t] = nh;
-        if (w.h_iter_max) atomicMax(w.h_iter_max, (unsigned long long)__double_as_longlong(nh));
-        regrow = nh > w.h_built[t];
-        if (regrow) atomicExch(w.rebuild, 1);
+    double moved = 0;  // the radius this particle moves to (0: none), for the iteration's largest
+    if (s < w.n_todo) {
+        const int t = w.todo[s];
+        const size_t n = (size_t)ps.n;
+        double acc[14];
+        for (int k = 0; k < 14; k++) acc[k] = w.acc[k * n + t];
+        const double h = ps.h[t];
+        DensityScratch sc = w.scratch[t];
+        double nh = h;
+        int stop = 0;
+        const int conv = after_iter(p, w.iter, h, acc, ps.cond[t], sc, nh, stop);
+        w.scratch[t] = sc;
+        ps.iters[t] = w.iter + 1;
+        if (stop) record_status(st, stop, t);
+        int regrow = 0;
+        if (!conv) {
+            ps.h[t] = nh;
+            moved = nh;
+            regrow = nh > w.h_built[t];
+            if (regrow) atomicExch(w.rebuild, 1);
+        }
+        w.keep[s] = conv ? 0 : 1;
+        w.regrow[s] = (unsigned char)regrow;
     }
-    w.keep[s] = conv ? 0 : 1;
-    w.regrow[s] = (unsigned char)regrow;
+    if (w.h_iter_max) warp_atomic_max_nonneg(w.h_iter_max, moved);  // every lane of the block
 }
 
 void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s)

@@ -1,5 +1,8 @@
-// gizmo_b200/csrc/passes_mixed.cu -- mixed form: FP32 pair arithmetic, FP64
-// positions / membership / accumulation (see passes.cuh).
+// gizmo_b200/csrc/passes_mixed.cu -- mixed form: FP32 force pair arithmetic,
+// FP64 positions / membership / density and gradient sums / accumulation (see
+// passes.cuh). Built with the approximate FP32 division and square root; the
+// pairs whose FP32 branch decisions are too close to call are evaluated again
+// by force_refine in passes_fp64.cu.
 #include "passes.cuh"
 
 namespace gz {
@@ -16,16 +19,11 @@ void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityW
     density_sums_fp64(p, ps, w, tpt, s);
 }
 
-void gradients_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                     void *rec, const EventPair *ev, cudaStream_t s)
-{
-    launch_gradients<float>(p, ps, targets, n_targets, rows, tpt, rec, ev, s);
-}
-
 void force_mixed(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
-                 DevStatus *st, void *rec, void *flux, double *sums, const EventPair *ev, cudaStream_t s)
+                 DevStatus *st, void *rec, void *flux, bool all, const RefineQueue &q, double *sums,
+                 const EventPair *ev, cudaStream_t s)
 {
-    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, sums, ev, s);
+    launch_force<float>(p, ps, targets, n_targets, rows, tpt, st, rec, flux, all, q, sums, ev, s);
 }
 
 }  // namespace gz

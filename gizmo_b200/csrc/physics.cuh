@@ -27,6 +27,8 @@ template <> struct Real<double> {
     static GZ_HD bool inside(double r, double /*r2d*/, double h, double /*hd*/) { return r < h; }
     static GZ_HD double support_r(double r, double /*r2d*/) { return r; }
     static GZ_HD double below_one(double u) { return u; }
+    // 1 - u for the kernel polynomials, as the reference computes it
+    static GZ_HD double one_minus_u(double u, double /*rd*/, double /*hd*/, double /*hinv*/) { return 1.0 - u; }
 };
 template <> struct Real<float> {
     // smallest value of the same role that FP32 represents (normal float)
@@ -44,10 +46,59 @@ template <> struct Real<float> {
     static GZ_HD bool inside(double rd, double /*r2d*/, float, double hd) { return rd < hd; }
     static GZ_HD double support_r(float, double r2d) { return sqrt(r2d); }
     static GZ_HD float below_one(float u) { return u < 1.0f ? u : 0.99999994f; }
+    // 1 - u from the FP64 separation and kernel length: near the kernel's edge
+    // 1 - u computed in FP32 keeps only the few bits in which u and 1 differ,
+    // and the weight (1 - u)^3 of an edge pair would lose as many
+    static GZ_HD float one_minus_u(float, double rd, double hd, float hinv) { return float((hd - rd) * (double)hinv); }
 };
 
 template <typename T> GZ_HD T dmax(T a, T b) { return (a > b) ? a : b; }  // DMAX, macros.h:219
 template <typename T> GZ_HD T dmin(T a, T b) { return (a < b) ? a : b; }  // DMIN, macros.h:220
+
+// Branch guard of the pair arithmetic. The force pair takes discontinuous
+// decisions on values it computes (wave-speed and vacuum tests, the pressure
+// limits that trigger the Riemann retries, the face-area sign, the HLLC
+// degenerate-wave test, the exact solver's sampling, the MFM entropic
+// switch). In FP32 a decision whose two sides lie within kFragile of their
+// common scale may go the other way than in FP64: Guard<float> records that
+// (the pair is then evaluated again in FP64), Guard<double> records nothing
+// and compiles away.
+constexpr float kFragile = 1.0e-4f;
+// Besides the branch decisions, Guard<float> checks precision: a value that
+// cancels its own terms (a face state far below the terms it was formed from,
+// a star pressure whose numerator cancels, a face area whose two sides
+// cancel) carries an FP32 rounding error of 2^-24 x the terms, so it is
+// evaluated in FP64 when that error could pass kPrecise relative.
+constexpr float kPrecise = 2.0e-6f;
+
+template <typename T> struct Guard;
+template <> struct Guard<double> {
+    GZ_HD void near(double, double, double, int = 0) {}
+    GZ_HD void precise(double, double, int = 0) {}
+    GZ_HD void flag(int = 0) {}
+    GZ_HD int fragile() const { return 0; }
+};
+// The site numbers name the guarded decisions; built with GZ_GUARD_SITES the
+// guard keeps one bit per site (for studying which decisions fire), otherwise
+// a single flag.
+template <> struct Guard<float> {
+#ifdef GZ_GUARD_SITES
+    unsigned long long f = 0;
+    GZ_HD void set(bool c, int site) { if (c) f |= 1ull << site; }
+#else
+    int f = 0;
+    GZ_HD void set(bool c, int) { f |= (int)c; }
+#endif
+    // a and b (about to be compared) closer than kFragile x scale; NaN operands count as close
+    GZ_HD void near(float a, float b, float scale, int site = 0) { set(!(fabsf(a - b) > kFragile * scale), site); }
+    // `value` computed from terms of total magnitude `terms`: too cancelled to hold kPrecise (2^-23 x terms)
+    GZ_HD void precise(float value, float terms, int site = 0)
+    {
+        set(!(fabsf(value) * kPrecise > 1.1920929e-7f * terms), site);
+    }
+    GZ_HD void flag(int site = 0) { set(true, site); }
+    GZ_HD int fragile() const { return f != 0; }
+};
 
 // ---------------------------------------------------------------- kernel
 // kernel_hinv + kernel_main (mesh/kernel.h:245-438): K=3 cubic, K=6 Wendland C2.
@@ -58,16 +109,18 @@ template <typename T> GZ_HD void k_hinv(T h, T &hinv, T &hinv3, T &hinv4)
     hinv4 = hinv3 * hinv;
 }
 
-template <typename T> GZ_HD void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T &dwk)
+// k_main_t takes t1 = 1 - u from the caller (Real<T>::one_minus_u); k_main
+// computes it as the reference does. u - 1 of the inner cubic branch is -t1
+// exactly.
+template <typename T> GZ_HD void k_main_t(int kf, T u, T t1, T hinv3, T hinv4, T &wk, T &dwk)
 {
     if (u >= T(1)) { wk = T(0); dwk = T(0); return; }
     T w, dw;
     if (kf == 3) {
         if (u < T(0.5)) {
             dw = u * (T(18.0) * u - T(12.0));
-            w = (T(1.0) + T(6.0) * (u - T(1.0)) * u * u);
+            w = (T(1.0) + T(6.0) * (-t1) * u * u);
         } else {
-            T t1 = (T(1.0) - u);
             T t2 = t1 * t1;
             dw = T(-6.0) * t2;
             w = T(2.0) * t2 * t1;
@@ -75,13 +128,17 @@ template <typename T> GZ_HD void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T 
         dwk = dw * (T(8.0 / 3.14159265358979323846) * hinv4);
         wk = w * (T(8.0 / 3.14159265358979323846) * hinv3);
     } else {
-        T t1 = (T(1) - u);
         T t3 = t1 * t1 * t1;
         dw = T(-20.0) * u * t3;
         w = t3 * t1 * (T(1.0) + T(4.0) * u);
         dwk = dw * (T(21.0 / (2.0 * 3.14159265358979323846)) * hinv4);
         wk = w * (T(21.0 / (2.0 * 3.14159265358979323846)) * hinv3);
     }
+}
+
+template <typename T> GZ_HD void k_main(int kf, T u, T hinv3, T hinv4, T &wk, T &dwk)
+{
+    k_main_t(kf, u, T(1) - u, hinv3, hinv4, wk, dwk);
 }
 
 // ------------------------------------------------------------ 3x3 inverse
@@ -332,20 +389,27 @@ template <typename T> GZ_HD T nsq3(const T *a) { return a[0] * a[0] + a[1] * a[1
 // get_wavespeeds_and_pressure_star (reimann.h:485-549)
 template <typename T>
 GZ_HD void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, T hL, T hR, T &SLo, T &SRo,
-                       T ptl, const GConst<T> &gc)
+                       T ptl, const GConst<T> &gc, Guard<T> &g)
 {
     const T MR = Real<T>::min_real();
     T S_L, S_R;
+    g.near(vR - vL, dmax(cL, cR), fabs(vL) + fabs(vR) + dmax(cL, cR), 1);  // the vacuum test
     if ((vR - vL) > dmax(cL, cR)) {
         o.P_M = MR; o.S_M = S_L = S_R = T(0);
     } else {
         const T PT_L = rv.L.p, PT_R = rv.R.p;
+        const T pscale = fabs(PT_L) + fabs(PT_R);
         S_L = dmin(vL, vR) - dmax(cL, cR);
         S_R = dmax(vL, vR) + dmax(cL, cR);
         T rho_wt_L = rv.L.rho * (S_L - vL);
         T rho_wt_R = rv.R.rho * (S_R - vR);
         o.S_M = ((PT_R - PT_L) + rho_wt_L * vL - rho_wt_R * vR) / (rho_wt_L - rho_wt_R);
         o.P_M = (PT_L * rho_wt_R - PT_R * rho_wt_L + rho_wt_L * rho_wt_R * (vR - vL)) / (rho_wt_R - rho_wt_L);
+        // the star pressure's sign (the clamp at MIN_REAL zeroes the wave speeds), on the scale
+        // of the terms its numerator cancels (rho_wt_L < 0 < rho_wt_R: the denominator cannot)
+        g.precise(PT_L * rho_wt_R - PT_R * rho_wt_L + rho_wt_L * rho_wt_R * (vR - vL),
+                  fabs(PT_L * rho_wt_R) + fabs(PT_R * rho_wt_L) + fabs(rho_wt_L * rho_wt_R * (vR - vL)), 3);
+        g.near(o.P_M, ptl, ptl, 4);
         if (o.P_M <= MR) { o.P_M = MR; o.S_M = S_L = S_R = T(0); }
         if ((o.P_M <= T(0)) || Real<T>::isnan_(o.P_M) || (o.P_M > ptl)) {
             const T sL = Real<T>::sqrt_(rv.L.rho), sR = Real<T>::sqrt_(rv.R.rho);
@@ -361,6 +425,8 @@ GZ_HD void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T c
             rho_wt_L = -rv.L.rho * (S_L - vL);
             o.S_M = ((rho_wt_R * vR + rho_wt_L * vL) + (PT_L - PT_R)) / (rho_wt_R + rho_wt_L);
             o.P_M = rv.L.rho * (vL - S_L) * (vL - o.S_M) + PT_L;
+            g.near(o.P_M, T(0), pscale + fabs(rv.L.rho * (vL - S_L) * (vL - o.S_M)), 6);
+            g.near(o.P_M, ptl, ptl, 7);
             if (o.P_M <= MR) { o.P_M = MR; o.S_M = S_L = S_R = T(0); }
             if ((o.P_M <= T(0)) || Real<T>::isnan_(o.P_M) || (o.P_M > ptl)) {
                 o.P_M = T(0.5) * ((PT_L + PT_R) + (vL - vR) * T(0.25) * (rv.L.rho + rv.R.rho) * (cL + cR));
@@ -369,6 +435,7 @@ GZ_HD void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T c
                 S_L = -S_plus; S_R = S_plus;
                 if (o.S_M < S_L) o.S_M = S_L;
                 if (o.S_M > S_R) o.S_M = S_R;
+                g.near(o.P_M, T(0), pscale + fabs((vL - vR) * T(0.25) * (rv.L.rho + rv.R.rho) * (cL + cR)), 8);
                 if (o.P_M <= MR) { o.P_M = MR; o.S_M = S_L = S_R = T(0); }
             }
         }
@@ -379,12 +446,19 @@ GZ_HD void wavespeeds(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T c
 
 // HLLC_fluxes, MFV, face frame (reimann.h:559-615)
 template <typename T>
-GZ_HD void hllc_fluxes(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T hL, T hR, T S_L, T S_R)
+GZ_HD void hllc_fluxes(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T hL, T hR, T S_L, T S_R, Guard<T> &g)
 {
     const T P_M = o.P_M, S_M = o.S_M;
     if ((P_M <= T(0)) || Real<T>::isnan_(P_M)) return;
     T nfac, eK, dv2, vf = T(0);
     {
+        // the FP64 tolerance is 1e-12 of the wave speeds: in FP32 a contact this close to an outer
+        // wave (where nfac divides by S_L - S_M or S_R - S_M) is decided in FP64; wave speeds all
+        // zeroed by the vacuum or star-pressure clamps take the degenerate flux in both forms
+        if (fabs(S_L) + fabs(S_R) > T(0)) {
+            g.near(S_M, S_L, fabs(S_L) + fabs(S_R), 9);
+            g.near(S_M, S_R, fabs(S_L) + fabs(S_R), 10);
+        }
         const T tol_s = Real<T>::hllc_tol(fabs(S_L) + fabs(S_R));
         if ((fabs(S_M - S_L) < tol_s) || (fabs(S_M - S_R) < tol_s) || (fabs(S_M - vf) < tol_s)) {
             o.F.rho = T(0);
@@ -477,12 +551,13 @@ GZ_HD T guess_pressure(const RVec<T> &rv, T vL, T vR, T cL, T cR, const GConst<T
 
 // iterative_Riemann_solver (reimann.h:965-1020), NMAX_ITER 1000, TOL_ITER 1e-6
 template <typename T>
-GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T cR, const GConst<T> &gc, Guard<T> &g)
 {
     T Pg, Pg_prev, W_L = T(0), W_R = T(0), Z_L, Z_R, tol, pratio;
     int niter = 0;
     const T dvel = vR - vL;
     const T check_vel = gc.G4 * (cR + cL) - dvel;
+    g.near(gc.G4 * (cR + cL), dvel, gc.G4 * (cR + cL) + fabs(vL) + fabs(vR), 11);  // vacuum generation
     if (check_vel < T(0)) return 0;
     tol = T(100.0);
     Pg = guess_pressure(rv, vL, vR, cL, cR, gc);
@@ -517,6 +592,7 @@ GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T c
         o.S_M = T(0.5) * (vL + vR) + T(0.5) * (W_R - W_L);
         return 1;
     }
+    g.flag(12);  // no convergence: the vacuum sampling follows; decided in FP64
     return 0;
 }
 
@@ -575,12 +651,18 @@ GZ_HD void sample_vac_internal(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, 
     }
 }
 
+// The sampled face state jumps across the contact (S_M = 0) and across a shock
+// (S_L or S_R = 0): those signs are guarded; at the edges of a rarefaction fan
+// the state is continuous.
 template <typename T>
-GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc)
+GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR, const GConst<T> &gc,
+                            Guard<T> &g)
 {
     if (!gc.mfv) return;
     const T S = T(0);
     T C_eff, S_eff;
+    const T sscale = fabs(vL) + fabs(vR) + cL + cR;
+    g.near(o.S_M, S, sscale, 13);
     if (S <= o.S_M) {
         if (o.P_M <= rv.L.p) {
             if (S <= vL - cL) { o.F.p = rv.L.p; o.F.rho = rv.L.rho; for (int k = 0; k < 3; k++) o.F.v[k] = rv.L.v[k]; return; }
@@ -601,6 +683,7 @@ GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR
         if (rv.L.p > T(0)) {
             const T pml = o.P_M / rv.L.p;
             const T S_L = vL - cL * Real<T>::sqrt_(gc.G2 * pml + gc.G1);
+            g.near(S_L, S, sscale, 14);
             if (S <= S_L) { o.F.p = rv.L.p; o.F.rho = rv.L.rho; for (int k = 0; k < 3; k++) o.F.v[k] = rv.L.v[k]; return; }
             o.F.rho = rv.L.rho * (pml + gc.G6) / (pml * gc.G6 + T(1.0));
             o.F.p = o.P_M;
@@ -616,6 +699,7 @@ GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR
         if (rv.R.p > T(0)) {
             const T pmr = o.P_M / rv.R.p;
             const T S_R = vR + cR * Real<T>::sqrt_(gc.G2 * pmr + gc.G1);
+            g.near(S_R, S, sscale, 15);
             if (S >= S_R) { o.F.p = rv.R.p; o.F.rho = rv.R.rho; for (int k = 0; k < 3; k++) o.F.v[k] = rv.R.v[k]; return; }
             o.F.rho = rv.R.rho * (pmr + gc.G6) / (pmr * gc.G6 + T(1.0));
             o.F.p = o.P_M;
@@ -660,7 +744,7 @@ template <typename T> GZ_HD void face_to_flux(ROut<T> &o, const T *n, const GCon
 // register budget of the common HLLC path.
 template <typename T>
 __host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR, T cL, T cR,
-                                                    const GConst<T> &gc, int &stop)
+                                                    const GConst<T> &gc, int &stop, Guard<T> &g)
 {
     if ((rv.L.p == T(0) && rv.R.p == T(0)) || (rv.L.rho == T(0) && rv.R.rho == T(0))) {
         o.P_M = o.S_M = T(0);
@@ -668,7 +752,7 @@ __host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &
         return;
     }
     if ((rv.L.rho > T(0)) && (rv.R.rho > T(0))) {
-        if (riemann_iterative(rv, o, vL, vR, cL, cR, gc)) sample_standard(rv, o, n, vL, vR, cL, cR, gc);
+        if (riemann_iterative(rv, o, vL, vR, cL, cR, gc, g)) sample_standard(rv, o, n, vL, vR, cL, cR, gc, g);
         else sample_vac_internal(rv, o, n, vL, vR, cL, cR, gc);
     } else {
         if ((rv.L.rho < T(0)) || (rv.R.rho < T(0))) { stop = 1234545; return; }
@@ -680,7 +764,7 @@ __host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &
 
 // Riemann_solver, hydro branch (reimann.h:282-370); rv taken by value as in the reference
 template <typename T>
-GZ_HD void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GConst<T> &gc, int &stop)
+GZ_HD void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GConst<T> &gc, int &stop, Guard<T> &g)
 {
     if ((rv.L.p < T(0) && rv.R.p < T(0)) || (rv.L.rho < T(0)) || (rv.R.rho < T(0))) { o.P_M = T(0); return; }
     rv.L.cs = Real<T>::sqrt_(gc.G0 * rv.L.p / rv.L.rho);
@@ -692,51 +776,87 @@ GZ_HD void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GCons
     const T hR = rv.R.p / rv.R.rho + rv.R.u + T(0.5) * nsq3(rv.R.v);
     const T vL = dot3(rv.L.v, n), vR = dot3(rv.R.v, n);
     T S_L, S_R;
-    wavespeeds(rv, o, n, vL, vR, cL, cR, hL, hR, S_L, S_R, ptl, gc);  // HLLC_Riemann_solver, reimann.h:382-396
+    wavespeeds(rv, o, n, vL, vR, cL, cR, hL, hR, S_L, S_R, ptl, gc, g);  // HLLC_Riemann_solver, reimann.h:382-396
     if (gc.mfv) {
-        if ((o.P_M >= T(0)) && (!Real<T>::isnan_(o.P_M))) hllc_fluxes(rv, o, n, vL, vR, hL, hR, S_L, S_R);
+        if ((o.P_M >= T(0)) && (!Real<T>::isnan_(o.P_M))) hllc_fluxes(rv, o, n, vL, vR, hL, hR, S_L, S_R, g);
     } else {
         o.F.rho = T(0);
         for (int k = 0; k < 3; k++) o.F.v[k] = n[k] * o.P_M;
         o.F.p = o.P_M * o.S_M;
     }
-    if ((o.P_M < T(0)) || Real<T>::isnan_(o.P_M)) riemann_kt(rv, o, n, vL, vR, cL, cR, hL, hR, gc);
-    if ((o.P_M < T(0)) || Real<T>::isnan_(o.P_M) || (o.P_M > ptl)) riemann_exact(rv, o, n, vL, vR, cL, cR, gc, stop);
+    if ((o.P_M < T(0)) || Real<T>::isnan_(o.P_M)) {
+        g.flag(20);  // only a NaN star pressure gets here: decided in FP64
+        riemann_kt(rv, o, n, vL, vR, cL, cR, hL, hR, gc);
+    }
+    g.near(o.P_M, ptl, ptl, 21);
+    if ((o.P_M < T(0)) || Real<T>::isnan_(o.P_M) || (o.P_M > ptl)) riemann_exact(rv, o, n, vL, vR, cL, cR, gc, stop, g);
 }
 
-// reconstruct_face_states, non-MHD (reimann.h:125-244)
+// reconstruct_face_states, non-MHD (reimann.h:125-244).
+// `scale` bounds the magnitudes Q_i and Q_j were computed from (they may be
+// differences, e.g. v - v_frame; 0 for density and pressure): the
+// sign-preserving clamps jump where Qmax, Qmin or their extended bounds cross
+// zero, so a crossing within the FP32 error of that scale is decided in FP64.
 template <typename T>
-GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, const T *d_j, T &Q_L, T &Q_R, int mode)
+GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, const T *d_j, T &Q_L, T &Q_R, int mode,
+                        T scale, Guard<T> &g)
 {
     if (mode == 0) { Q_R = Q_i; Q_L = Q_j; return; }
     if (Q_i == Q_j) { Q_L = Q_R = Q_i; return; }
     Q_R = Q_i + g_i[0] * d_i[0] + g_i[1] * d_i[1] + g_i[2] * d_i[2];
     Q_L = Q_j + g_j[0] * d_j[0] + g_j[1] * d_j[1] + g_j[2] * d_j[2];
+    // the magnitude of the terms each candidate face value is a sum of (its
+    // FP32 rounding error is 2^-24 of that), carried with the value it chooses
+    T tR = fabs(Q_i) + fabs(g_i[0] * d_i[0]) + fabs(g_i[1] * d_i[1]) + fabs(g_i[2] * d_i[2]);
+    T tL = fabs(Q_j) + fabs(g_j[0] * d_j[0]) + fabs(g_j[1] * d_j[1]) + fabs(g_j[2] * d_j[2]);
     T Qmin, Qmax, Qmed, Qmax_eff, Qmin_eff, fac, Qmed_max, Qmed_min;
     Qmed = T(0.5) * (Q_i + Q_j);
     if (Q_i < Q_j) { Qmax = Q_j; Qmin = Q_i; } else { Qmax = Q_i; Qmin = Q_j; }
     fac = T(0.5) * (Qmax - Qmin);
     Qmax_eff = Qmax + fac;
     Qmin_eff = Qmin - fac;
+    T tmaxe = T(1.5) * fabs(Qmax) + T(0.5) * fabs(Qmin), tmine = T(1.5) * fabs(Qmin) + T(0.5) * fabs(Qmax);
     if (mode > 0) {
-        if (Qmax < T(0)) { if (Qmax_eff > T(0)) Qmax_eff = Qmax * Qmax / (Qmax - (Qmax_eff - Qmax)); }
-        if (Qmin > T(0)) { if (Qmin_eff < T(0)) Qmin_eff = Qmin * Qmin / (Qmin + (Qmin - Qmin_eff)); }
+        // Qmax and Qmin carry the error of the values they were computed from
+        // (none for rho and P, whose signs are exact); the extended bounds that
+        // of their own terms
+        if (scale > T(0)) {
+            g.near(Qmax, T(0), scale, 22);
+            g.near(Qmin, T(0), scale, 23);
+        }
+        const T sc = scale + fabs(Qmax) + fabs(Qmin);
+        g.near(Qmax_eff, T(0), sc, 24);
+        g.near(Qmin_eff, T(0), sc, 25);
+        // the sign-preserving bounds divide by a sum of like-signed terms: well conditioned
+        if (Qmax < T(0)) {
+            if (Qmax_eff > T(0)) { Qmax_eff = Qmax * Qmax / (Qmax - (Qmax_eff - Qmax)); tmaxe = T(4) * fabs(Qmax_eff); }
+        }
+        if (Qmin > T(0)) {
+            if (Qmin_eff < T(0)) { Qmin_eff = Qmin * Qmin / (Qmin + (Qmin - Qmin_eff)); tmine = T(4) * fabs(Qmin_eff); }
+        }
     }
     fac = T(0.375) * (Qmax - Qmin);
     Qmed_max = Qmed + fac;
     Qmed_min = Qmed - fac;
-    if (Qmed_max > Qmax_eff) Qmed_max = Qmax_eff;
-    if (Qmed_min < Qmin_eff) Qmed_min = Qmin_eff;
+    T tmedx = T(0.5) * (fabs(Q_i) + fabs(Q_j)) + T(0.375) * (fabs(Qmax) + fabs(Qmin)), tmedn = tmedx;
+    if (Qmed_max > Qmax_eff) { Qmed_max = Qmax_eff; tmedx = tmaxe; }
+    if (Qmed_min < Qmin_eff) { Qmed_min = Qmin_eff; tmedn = tmine; }
     if (Q_i < Q_j) {
-        if (Q_R < Qmin_eff) Q_R = Qmin_eff;
-        if (Q_R > Qmed_max) Q_R = Qmed_max;
-        if (Q_L > Qmax_eff) Q_L = Qmax_eff;
-        if (Q_L < Qmed_min) Q_L = Qmed_min;
+        if (Q_R < Qmin_eff) { Q_R = Qmin_eff; tR = tmine; }
+        if (Q_R > Qmed_max) { Q_R = Qmed_max; tR = tmedx; }
+        if (Q_L > Qmax_eff) { Q_L = Qmax_eff; tL = tmaxe; }
+        if (Q_L < Qmed_min) { Q_L = Qmed_min; tL = tmedn; }
     } else {
-        if (Q_R > Qmax_eff) Q_R = Qmax_eff;
-        if (Q_R < Qmed_min) Q_R = Qmed_min;
-        if (Q_L < Qmin_eff) Q_L = Qmin_eff;
-        if (Q_L > Qmed_max) Q_L = Qmed_max;
+        if (Q_R > Qmax_eff) { Q_R = Qmax_eff; tR = tmaxe; }
+        if (Q_R < Qmed_min) { Q_R = Qmed_min; tR = tmedn; }
+        if (Q_L < Qmin_eff) { Q_L = Qmin_eff; tL = tmine; }
+        if (Q_L > Qmed_max) { Q_L = Qmed_max; tL = tmedx; }
+    }
+    // density and pressure enter the Riemann problem relatively: their face
+    // states must hold their relative precision
+    if (scale == T(0)) {
+        g.precise(Q_R, tR, 35);
+        g.precise(Q_L, tL, 36);
     }
 }
 
@@ -768,9 +888,12 @@ template <typename T> struct __align__(16) PairFlux {
 // compute_finitevol_faces_functions.h:46-168. dp = x_i - x_j (min image),
 // r2 its exact FP64 square. The support test uses r2 in FP64 so both forms
 // pick the same pairs.
+// `g` collects the pair's fragile decisions (Guard<float>: a mixed-form pair
+// whose branch may differ from the FP64 form's, or whose arithmetic cancels
+// beyond FP32's reach; the caller evaluates it again in FP64).
 template <typename T>
 GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc, const Side<T> &I, const Side<T> &J,
-                       const T dp[3], double r2d, double hi_d, double hj_d, PairFlux<T> &out, int &stop)
+                       const T dp[3], double r2d, double hi_d, double hj_d, PairFlux<T> &out, int &stop, Guard<T> &g)
 {
     out.valid = 0;
     out.rho = out.p = T(0);
@@ -790,9 +913,15 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
     T wk_i = T(0), dwk_i = T(0), wk_j = T(0), dwk_j = T(0);
     const double r_sup = Real<T>::support_r(r, r2d);
     k_hinv(I.h, hinv_i, hinv3_i, hinv4_i);
-    if (Real<T>::inside(r_sup, r2d, I.h, hi_d)) k_main(kf, Real<T>::below_one(r * hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
+    if (Real<T>::inside(r_sup, r2d, I.h, hi_d)) {
+        const T u = Real<T>::below_one(r * hinv_i);
+        k_main_t(kf, u, Real<T>::one_minus_u(u, r_sup, hi_d, hinv_i), hinv3_i, hinv4_i, wk_i, dwk_i);
+    }
     k_hinv(J.h, hinv_j, hinv3_j, hinv4_j);
-    if (Real<T>::inside(r_sup, r2d, J.h, hj_d)) k_main(kf, Real<T>::below_one(r * hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
+    if (Real<T>::inside(r_sup, r2d, J.h, hj_d)) {
+        const T u = Real<T>::below_one(r * hinv_j);
+        k_main_t(kf, u, Real<T>::one_minus_u(u, r_sup, hj_d, hinv_j), hinv3_j, hinv4_j, wk_j, dwk_j);
+    }
     // explicitly rounded FP64 (no contraction in either build)
     const double cnumcrit2 = cr::sub(cr::mul(kCnDanger, kCnDanger), cr::mul(I.condd, I.condd));
     const double cnum2 = cr::mul(J.condd, J.condd);
@@ -823,7 +952,13 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
             const T si = wk_i * wt_i, sj = wk_j * wt_j;
             for (int k = 0; k < 3; k++) FA[k] = (ai[k] * si + aj[k] * sj) * (T(1.0) * T(1.0));
             FAN = nsq3(FA);
+            // the face area holds its relative precision where the two sides' terms cancel, and
+            // its sign against dp is decided on the same scale (|dp_k| <= r)
+            const T fterms = (fabs(ai[0]) + fabs(ai[1]) + fabs(ai[2])) * fabs(si) +
+                             (fabs(aj[0]) + fabs(aj[1]) + fabs(aj[2])) * fabs(sj);
+            g.precise(fabs(FA[0]) + fabs(FA[1]) + fabs(FA[2]), fterms, 37);
             const T fn_dot_dp = dot3(FA, dp);
+            g.near(fn_dot_dp, T(0), fterms * r, 26);
             if ((cnum2 > cr::add(1.0e12, cnumcrit2)) || (fn_dot_dp < T(0))) {
                 T fk = -(wt_i * V_i * dwk_i + wt_j * V_j * dwk_j) / r;
                 fk *= T(1.0) * T(1.0);
@@ -860,11 +995,11 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         if (vdotf2_phys < T(0)) v2_approach = dmax(v2_approach, vdotf2_phys * vdotf2_phys);
         int recon_mode = 1;
         if (leak_vs_tol > 1.0) recon_mode = 0;
-        reconstruct(I.rho, I.grho, J.rho, J.grho, d_i, d_j, rv.L.rho, rv.R.rho, recon_mode);
-        reconstruct(Pressure_i, I.gp, Pressure_j, J.gp, d_i, d_j, rv.L.p, rv.R.p, recon_mode);
+        reconstruct(I.rho, I.grho, J.rho, J.grho, d_i, d_j, rv.L.rho, rv.R.rho, recon_mode, T(0), g);
+        reconstruct(Pressure_i, I.gp, Pressure_j, J.gp, d_i, d_j, rv.L.p, rv.R.p, recon_mode, T(0), g);
         for (int k = 0; k < 3; k++)
             reconstruct(I.v[k] - vframe[k], I.gv + 3 * k, J.v[k] - vframe[k], J.gv + 3 * k, d_i, d_j, rv.L.v[k],
-                        rv.R.v[k], recon_mode);
+                        rv.R.v[k], recon_mode, fabs(I.v[k]) + fabs(J.v[k]) + fabs(vframe[k]), g);
         const T press_i_tot = Pressure_i + I.rho * v2_approach;
         const T press_j_tot = Pressure_j + J.rho * v2_approach;
         T ptl = T(1.1) * T(1.0) * dmax(press_i_tot, press_j_tot);
@@ -887,9 +1022,13 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
                 }
                 lim = attempt == 1 ? T(1.4) * ptl : T(2.0) * ptl;
             }
-            riemann_solver(rv, ro, n, lim, gc, stop);
+            riemann_solver(rv, ro, n, lim, gc, stop, g);
             bool retry = (ro.P_M < T(0)) || Real<T>::isnan_(ro.P_M);
-            if (attempt == 0) retry = retry || (ro.P_M > T(1.4) * ptl);
+            if (attempt == 0) {
+                g.near(ro.P_M, T(1.4) * ptl, ptl, 27);
+                retry = retry || (ro.P_M > T(1.4) * ptl);
+            }
+            if (Real<T>::isnan_(ro.P_M)) g.flag(28);  // a NaN star pressure: decided in FP64
             if (!retry) break;
             if (attempt == 2) stop = 1234;
         }
@@ -914,6 +1053,23 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
                 const T du_new = T(0.5) * (PdV_i - PdV_j + facenorm_pm * (face_vel_i + face_vel_j));
                 const double ratio = 1.001;
                 const double to_i = I.prd, to_j = J.prd;
+                // The switch's tests (SM/c against eps_big and eps_small, and the signs and sizes of
+                // the energy changes each side would see) choose between du_old and du_new: a flip
+                // moves the flux by |du_new - du_old|. Guarded only where that is not negligible on
+                // the scale of the face's work terms.
+                const T es = fabs(du_old) + fabs(du_new) + fabs(facenorm_pm * face_vel_i) +
+                             fabs(facenorm_pm * face_vel_j);
+                if (fabs(du_new - du_old) > T(1e-6) * es) {
+                    g.near(SM_over_ceff, eps_big, eps_big, 29);
+                    if (cnum2 < cnumcrit2) {
+                        const T dtoj = -du_old + facenorm_pm * face_vel_j, dtoi = +du_old - facenorm_pm * face_vel_i;
+                        g.near(SM_over_ceff, eps_small, eps_small, 30);
+                        g.near(dtoj, T(0), es, 31);
+                        g.near(dtoi, T(0), es, 32);
+                        g.near(dtoj, -du_new + facenorm_pm * face_vel_j, es, 33);
+                        g.near(dtoi, +du_new - facenorm_pm * face_vel_i, es, 34);
+                    }
+                }
                 if (use && SM_over_ceff > eps_small && cnum2 < cnumcrit2) {
                     if (to_i > cr::mul(ratio, to_j)) {
                         const T dtoj = -du_old + facenorm_pm * face_vel_j;

@@ -30,7 +30,22 @@ struct Particles {
     double *fabs;                   // [3][n] sums of |mass|, |momentum|, |energy| pair fluxes (diagnostic)
     int *iters;
     const unsigned char *active;    // 1 for particles of the current active set
+    // wake-up of inactive neighbours (hydro_functions.h:534-544); bin_active null: off
+    const int *timebin;             // P.TimeBin
+    const double *vsig_prev;        // CellP.MaxSignalVel from each cell's last force pass
+    int *wakeup;                    // out: largest waker bin + 1 (0: none)
+    const int *bin_active;          // TimeBinActive[60]
 };
+
+constexpr double kWakeup = 4.1;  // WAKEUP (declarations/constants.h:11-13; no GR, slope-limiter tolerance > 0)
+
+// The wake-up test of one evaluated pair: `t` the active row owner, `j` its
+// neighbour, vsig_ts the pair's timestep signal speed (hydro_functions.h:534-544).
+GZ_DEV void wakeup_test(const Particles &ps, int t, int j, double vsig_ts)
+{
+    if (ps.bin_active && !ps.bin_active[ps.timebin[j]] && vsig_ts > kWakeup * ps.vsig_prev[j])
+        atomicMax(ps.wakeup + j, ps.timebin[t] + 1);  // wakeup_flag_from_timebin, core/proto.h:181
+}
 
 // Octree over the Morton-sorted particles (63-bit keys, 21 levels): node i
 // owns the sorted run [first, first + count); an internal node's children
@@ -62,6 +77,23 @@ struct __align__(16) DensRec {
 // (null: not timed).
 struct EventPair {
     cudaEvent_t start, stop;
+};
+
+// Mixed-form force pairs whose FP32 branch decisions were too close to call
+// (Guard<float>): each names the flux entries it was stored at (row i's and,
+// for a pair evaluated once, row j's; -1 if none) and the pair in canonical
+// orientation (i the lower sorted index). force_refine evaluates them again in
+// FP64 and overwrites those entries before the rows are accumulated.
+struct RefineItem {
+    long long e, a;
+    int i, j;
+    int t;      // the active row owner for the wake-up test (-1: none; every particle active)
+    int pad;
+};
+struct RefineQueue {
+    RefineItem *item;            // null: nothing is queued (the FP64 form)
+    unsigned long long *count;   // items pushed (may pass cap: the pass then runs again with room for all)
+    long long cap;
 };
 
 struct Csr {

@@ -102,7 +102,9 @@ class HydroPass:
         return int(self.lib.gz_stream(self._ctx) or 0)
 
     # -- data ---------------------------------------------------------------
-    def upload(self, pos, vel, mass, u, dt, h, cond=None):
+    def upload(self, pos, vel, mass, u, dt, h, cond=None, timebin=None, vsig=None):
+        """Inputs in the caller's order; timebin (P.TimeBin) and vsig (the stored
+        CellP.MaxSignalVel) are for the individual-timestep wake-up (optional)."""
         n = int(np.asarray(mass).shape[0])
         arrs = dict(pos=_f64(pos, (n, 3)), vel=_f64(vel, (n, 3)), mass=_f64(mass, (n,)), u=_f64(u, (n,)),
                     dt=_f64(dt, (n,)), h=_f64(h, (n,)),
@@ -111,6 +113,15 @@ class HydroPass:
         p.n = n
         for k, a in arrs.items():
             setattr(p, k, _dp(a))
+        keep = [arrs]
+        if timebin is not None:
+            tb = np.ascontiguousarray(timebin, dtype=np.int32).reshape(n)
+            p.timebin = _ip(tb)
+            keep.append(tb)
+            if vsig is not None:
+                vs = _f64(vsig, (n,))
+                p.vsig = _dp(vs)
+                keep.append(vs)
         self._check(self.lib.gz_upload(self._ctx, C.byref(p)))
         self.n = n
 
@@ -153,10 +164,11 @@ class HydroPass:
                 a = np.zeros((n,) if k == 1 else (n, k))
                 out[name] = a
                 setattr(o, name, _dp(a))
-        if "iters" in want:
-            a = np.zeros(n, dtype=np.int32)
-            out["iters"] = a
-            o.iters = _ip(a)
+        for name in ("iters", "wakeup"):
+            if name in want:
+                a = np.zeros(n, dtype=np.int32)
+                out[name] = a
+                setattr(o, name, _ip(a))
         self._check(self.lib.gz_download(self._ctx, C.byref(o)))
         return out
 
@@ -185,6 +197,34 @@ class HydroPass:
         self.hydro_gradient_calc(active)
         self.hydro_force(active)
 
+    # -- individual timesteps ---------------------------------------------------
+    def set_bin_active(self, bin_active):
+        """TimeBinActive[60] for the wake-up test of the following force passes
+        over active subsets (None: off)."""
+        if bin_active is None:
+            self._check(self.lib.gz_set_bin_active(self._ctx, None))
+            return
+        b = np.ascontiguousarray(bin_active, dtype=np.int32).reshape(abi.TIMEBINS)
+        self._check(self.lib.gz_set_bin_active(self._ctx, _ip(b)))
+
+    def active_list(self, bin_active) -> np.ndarray:
+        """make_list_of_active_particles on the device: ascending original indices."""
+        b = np.ascontiguousarray(bin_active, dtype=np.int32).reshape(abi.TIMEBINS)
+        k = C.c_int()
+        self._check(self.lib.gz_active_list(self._ctx, _ip(b), None, C.byref(k)))
+        out = np.zeros(max(k.value, 1), dtype=np.int32)
+        self._check(self.lib.gz_active_list(self._ctx, _ip(b), _ip(out), C.byref(k)))
+        return out[: k.value]
+
+    def wakeup_bins(self, bin_active, max_time_bin_active: int, lowest_occupied_active_bin: int):
+        """(new timebin of every cell, cells moved) by process_wake_ups' bin rule."""
+        b = np.ascontiguousarray(bin_active, dtype=np.int32).reshape(abi.TIMEBINS)
+        out = np.zeros(self.n, dtype=np.int32)
+        m = C.c_int()
+        self._check(self.lib.gz_wakeup_bins(self._ctx, _ip(b), int(max_time_bin_active),
+                                            int(lowest_occupied_active_bin), _ip(out), C.byref(m)))
+        return out, m.value
+
     # -- diagnostics ----------------------------------------------------------
     def neighbors(self, mode: int, active=None):
         ap, na = self._active(active)
@@ -211,7 +251,8 @@ class HydroPass:
         return dict(code=s.code, index=s.index, density_iterations=s.density_iterations,
                     pairs_density=s.pairs_density, pairs_symmetric=s.pairs_symmetric,
                     device_bytes=s.device_bytes, kernel_launches=s.kernel_launches,
-                    message=s.message.decode(errors="replace"), h_iter_max=s.h_iter_max)
+                    message=s.message.decode(errors="replace"), h_iter_max=s.h_iter_max,
+                    pairs_refined=s.pairs_refined)
 
     def _check(self, rc: int):
         if rc:

@@ -88,6 +88,10 @@ typedef struct gz_particles {
     const double *dt;     /* [n]    get_particle_timestep_in_physical(i) */
     const double *h;      /* [n]    P[i].KernelRadius seed for the density iteration */
     const double *cond;   /* [n]    CellP[i].ConditionNumber from the previous step (0 if none) */
+    /* individual timesteps (both may be NULL: no wake-up) */
+    const int32_t *timebin; /* [n]  P[i].TimeBin */
+    const double  *vsig;    /* [n]  CellP[i].MaxSignalVel from the cell's last force pass: the wake-up
+                               test (hydro_functions.h:534-544) reads it for inactive neighbours */
 } gz_particles;
 
 /* Outputs; any pointer may be NULL to skip that field. */
@@ -112,6 +116,10 @@ typedef struct gz_outputs {
     double *dmass;     /* [n]    CellP.dMass (MFV) */
     double *gravwork;  /* [n][3] CellP.GravWorkTerm (MFV) */
     int    *iters;     /* [n]    density iterations taken */
+    int32_t *wakeup;   /* [n]    the wake-up flag the last force pass gave each cell (hydro_functions.h:
+                          534-544): the largest bin + 1 of an active neighbour whose pair signal speed
+                          exceeded WAKEUP (4.1) x the cell's stored MaxSignalVel; 0 for none. Merge it
+                          into P.wakeup with a max (the reference's HYDRO_ATOMIC_MAX) */
     double *flux_abs;  /* [n][3] diagnostic (GZ_DIAG_FLUX_ABS), no reference counterpart: the sums over the
                           force row of |mass flux|, |momentum flux| and |energy flux| of
                           the pairs, the scale against which the cancelling sums dtmass,
@@ -131,6 +139,9 @@ typedef struct gz_status_info {
     double   h_iter_max;        /* the largest kernel length at which the last density pass took
                                    sums: its seeds (after the clamp of density_loop.cc:837-840) and
                                    every radius its iteration moved to */
+    int64_t  pairs_refined;     /* mixed form: pairs of the last force pass evaluated again in FP64
+                                   because an FP32 branch decision was too close to call or its
+                                   arithmetic cancelled beyond FP32's reach */
 } gz_status_info;
 
 typedef struct gz_context gz_context;
@@ -170,6 +181,30 @@ int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
 
 /* Copy outputs device -> host (original order). */
 int gz_download(gz_context *ctx, const gz_outputs *out);
+
+/* Individual timesteps. GZ_TIMEBINS is TIMEBINS (declarations/allvars.h). */
+#define GZ_TIMEBINS 60
+/* TimeBinActive[GZ_TIMEBINS] for the wake-up test of the following force
+ * passes over an active subset (hydro_functions.h:534-544; the reference reads
+ * the global table). NULL switches the wake-up off, the default. Needs the
+ * timebin and vsig inputs of gz_upload. */
+int gz_set_bin_active(gz_context *ctx, const int *bin_active);
+/* make_list_of_active_particles (core/run.cc:997-1010) on the device: the
+ * cells whose TimeBin is active in bin_active[GZ_TIMEBINS] and whose mass is
+ * positive, as original indices in ascending order (the reference walks the
+ * bins' lists; the passes accept any order). *n_out receives the count; out
+ * (NULL: count only) holds it. */
+int gz_active_list(gz_context *ctx, const int *bin_active, int *out, int *n_out);
+/* The bin rule of process_wake_ups (core/timestep.cc:1565-1700) on the device,
+ * for the cells the last force pass woke: bin = the waker's bin less the bins
+ * WAKEUP spans (3), floored at lowest_occupied_active_bin, capped at
+ * max_time_bin_active (the highest bin active at the next kick) and never
+ * above the cell's own; active cells and cells without mass keep theirs.
+ * timebin_out[n] (original order) receives every cell's bin, *n_moved the
+ * cells that moved. The timebin lists, the step truncation and the kicks of
+ * the woken cells stay with the caller (gz_kick gives the kicks). */
+int gz_wakeup_bins(gz_context *ctx, const int *bin_active, int max_time_bin_active, int lowest_occupied_active_bin,
+                   int *timebin_out, int *n_moved);
 
 /* Error/progress record of the context (device status word included). */
 int gz_status(gz_context *ctx, gz_status_info *info);

@@ -963,6 +963,23 @@ static void riemann_exact(const rvec *rv, rout *o, const double *n, double vL, d
     if (gc->mfv) face_to_flux(o, n, gc);
 }
 
+/* Pair evaluations of the last force pass that took each rare branch of the
+ * Riemann cascade (test instrumentation: which fallbacks a case exercises):
+ * [0] Kurganov-Tadmor, [1] the exact iterative solver, [2] the second attempt
+ * (cell-centred states), [3] the third attempt (at rest). */
+static long long g_riemann_branches[4];
+
+void orc_riemann_branches(long long out[4])
+{
+    for (int k = 0; k < 4; k++) out[k] = g_riemann_branches[k];
+}
+
+static void count_branch(int k)
+{
+#pragma omp atomic
+    g_riemann_branches[k]++;
+}
+
 /* Riemann_solver, hydro branch (reimann.h:282-370); rv by value as in the reference */
 static void riemann_solver(rvec rv, rout *o, const double *n, double ptl, const gconst *gc, int *stop)
 {
@@ -985,8 +1002,11 @@ static void riemann_solver(rvec rv, rout *o, const double *n, double ptl, const 
         for (int k = 0; k < 3; k++) o->F.v[k] = n[k] * o->P_M;
         o->F.p = o->P_M * o->S_M;
     }
-    if ((o->P_M < 0) || isnan(o->P_M)) riemann_kt(&rv, o, n, vL, vR, cL, cR, hL, hR, gc);
-    if ((o->P_M < 0) || isnan(o->P_M) || (o->P_M > ptl)) riemann_exact(&rv, o, n, vL, vR, cL, cR, gc, stop);
+    if ((o->P_M < 0) || isnan(o->P_M)) { count_branch(0); riemann_kt(&rv, o, n, vL, vR, cL, cR, hL, hR, gc); }
+    if ((o->P_M < 0) || isnan(o->P_M) || (o->P_M > ptl)) {
+        count_branch(1);
+        riemann_exact(&rv, o, n, vL, vR, cL, cR, gc, stop);
+    }
 }
 
 /* reconstruct_face_states, non-MHD (reimann.h:125-244) */
@@ -1167,11 +1187,13 @@ static void force_pair(const gz_params *p, const gconst *gc, const fside *I, con
         if (recon_mode == 0) ptl = DMAX(ptl, DMAX(DMAX(Pressure_i, Pressure_j), 2. * DMAX(I->rho, J->rho) * v2_approach));
         riemann_solver(rv, &ro, n, ptl, gc, stop);
         if ((ro.P_M < 0) || isnan(ro.P_M) || (ro.P_M > 1.4 * ptl)) {
+            count_branch(2);
             rv.R.p = Pressure_i; rv.L.p = Pressure_j;
             rv.R.rho = I->rho; rv.L.rho = J->rho;
             for (int k = 0; k < 3; k++) { rv.R.v[k] = I->v[k] - vframe[k]; rv.L.v[k] = J->v[k] - vframe[k]; }
             riemann_solver(rv, &ro, n, 1.4 * ptl, gc, stop);
             if ((ro.P_M < 0) || isnan(ro.P_M)) {
+                count_branch(3);
                 rv.R.p = Pressure_i; rv.L.p = Pressure_j;
                 rv.R.rho = I->rho; rv.L.rho = J->rho;
                 for (int k = 0; k < 3; k++) { rv.R.v[k] = 0; rv.L.v[k] = 0; }
@@ -1288,6 +1310,7 @@ int orc_force_wakeup(const gz_params *p, orc_state *s, const int *active, int n_
     gconst gc;
     make_gconst(p, &gc);
     const int mfv = gc.mfv;
+    for (int k = 0; k < 4; k++) g_riemann_branches[k] = 0;
     /* preloop (hydro_toplevel.cc:457-565) */
     for (int a = 0; a < n_active; a++) {
         const int i = active[a];
@@ -1716,4 +1739,57 @@ int orc_timestep(const gz_params *p, const orc_timestep_params *tp, orc_timestep
         t->dt_step[i] = ti_step;
     }
     return code;
+}
+
+
+/* ------------------------------------------------------------- active sets */
+/* make_list_of_active_particles (core/run.cc:997-1010): the cells whose
+ * TimeBin is active and whose mass is positive, here in ascending index order
+ * (the reference walks the bins' linked lists; the passes do not depend on the
+ * order). Returns the count; out may be NULL. */
+int orc_active_list(int n, const int *timebin, const double *mass, const int *bin_active, int *out)
+{
+    int k = 0;
+    for (int i = 0; i < n; i++) {
+        if (bin_active[timebin[i]] && mass[i] > 0) {
+            if (out) out[k] = i;
+            k++;
+        }
+    }
+    return k;
+}
+
+/* The new timebin of each cell the last force pass woke up (P.wakeup > 0), by
+ * the rule of process_wake_ups (core/timestep.cc:1565-1700) for gas: the
+ * waker's bin (wakeup_timebin_from_flag, core/proto.h:182) less the bins that
+ * WAKEUP spans (the smallest k with 2^k >= WAKEUP), floored at the lowest
+ * occupied active bin, capped at the highest bin active at the next kick, and
+ * never above the cell's own bin; active cells and cells without mass keep
+ * theirs. The linked-list moves, the step truncation and the kicks that
+ * follow stay with the caller. Returns the number of cells moved. */
+int orc_wakeup_bins(int n, const int *timebin, const int *wakeup, const double *mass, const int *bin_active,
+                    int max_time_bin_active, int lowest_occupied_active_bin, int *out)
+{
+    int offset = 0;
+    while ((1ll << offset) < (long long)WAKEUP) offset++;
+    int moved = 0;
+    for (int i = 0; i < n; i++) {
+        int bin = timebin[i];
+        out[i] = bin;
+        if (!wakeup[i] || !(mass[i] > 0)) continue;
+        const int binold = timebin[i];
+        if (bin_active[binold]) continue;
+        if (wakeup[i] > 0) {
+            const int waker_bin = wakeup[i] - 1;
+            bin = waker_bin - offset > 0 ? waker_bin - offset : 0;
+            if (bin < lowest_occupied_active_bin) bin = lowest_occupied_active_bin;
+        } else {
+            bin = max_time_bin_active;
+        }
+        if (bin > max_time_bin_active) bin = max_time_bin_active;
+        if (bin >= binold) bin = binold;
+        out[i] = bin;
+        if (bin != binold) moved++;
+    }
+    return moved;
 }

@@ -89,6 +89,20 @@ int orc_force(const gz_params *p, orc_state *s, const int *active, int n_active,
 int orc_force_wakeup(const gz_params *p, orc_state *s, const int *active, int n_active, int n_threads,
                      const int *bin_active);
 
+/* Pair evaluations of the last orc_force that took each rare branch of the
+ * Riemann cascade (test instrumentation): [0] Kurganov-Tadmor, [1] the exact
+ * iterative solver, [2] the second attempt (cell-centred states), [3] the
+ * third attempt (at rest). */
+void orc_riemann_branches(long long out[4]);
+
+/* make_list_of_active_particles (core/run.cc:997-1010), ascending: returns
+ * the count and writes the indices into out (may be NULL). */
+int orc_active_list(int n, const int *timebin, const double *mass, const int *bin_active, int *out);
+/* The timebin each woken cell moves to, by process_wake_ups' rule
+ * (core/timestep.cc:1565-1700); returns the number of cells moved. */
+int orc_wakeup_bins(int n, const int *timebin, const int *wakeup, const double *mass, const int *bin_active,
+                    int max_time_bin_active, int lowest_occupied_active_bin, int *out);
+
 /* Density sums at a fixed kernel length, no iteration: writes the raw
  * accumulator of density_loop.h:1140-1385 for each active into acc[a][14]:
  * {Ngb, Rho, DrkernNgb, DivVel, NV_T xx,yy,zz,xy,yz,xz, face x,y,z, 0}

@@ -197,6 +197,17 @@ def _setup(lib: C.CDLL, prefix: str) -> C.CDLL:
     f = getattr(lib, f"{prefix}_timestep")
     f.argtypes = [C.POINTER(GzParams), C.POINTER(OrcTimestepParams), C.POINTER(OrcTimestepState)]
     f.restype = C.c_int
+    if hasattr(lib, f"{prefix}_active_list"):
+        f = getattr(lib, f"{prefix}_active_list")
+        f.argtypes = [C.c_int, _ip, _dp, _ip, _ip]
+        f.restype = C.c_int
+        f = getattr(lib, f"{prefix}_wakeup_bins")
+        f.argtypes = [C.c_int, _ip, _ip, _dp, _ip, C.c_int, C.c_int, _ip]
+        f.restype = C.c_int
+    if hasattr(lib, f"{prefix}_riemann_branches"):
+        f = getattr(lib, f"{prefix}_riemann_branches")
+        f.argtypes = [C.POINTER(C.c_longlong)]
+        f.restype = None
     if hasattr(lib, f"{prefix}_density_h_iter_max"):
         f = getattr(lib, f"{prefix}_density_h_iter_max")
         f.argtypes = []
@@ -265,6 +276,12 @@ class Oracle:
 
     def density(self, st, active=None):
         return self._run("density", st, active)
+
+    def riemann_branches(self) -> dict:
+        """Pair evaluations of the last force pass per rare Riemann branch (port only)."""
+        out = (C.c_longlong * 4)()
+        getattr(self.lib, f"{self.prefix}_riemann_branches")(out)
+        return dict(zip(("kt", "exact", "retry_centred", "retry_at_rest"), (int(v) for v in out)))
 
     def density_h_iter_max(self) -> float:
         """The largest kernel length at which the last density pass took sums (port only)."""
@@ -347,3 +364,29 @@ def neighbors(params: GzParams, st: dict, mode: int, active=None, n_threads: int
     nb = np.ctypeslib.as_array(out.nbrs, shape=(max(int(off[-1]), 1),))[: int(off[-1])].astype(np.int32).copy()
     lib.orc_csr_free(C.byref(out))
     return off, nb
+
+
+def active_list(timebin, mass, bin_active) -> np.ndarray:
+    """make_list_of_active_particles (core/run.cc:997-1010), ascending indices."""
+    lib = Oracle(GzParams(), "port").lib
+    tb = np.ascontiguousarray(timebin, dtype=np.int32)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    ba = np.ascontiguousarray(bin_active, dtype=np.int32)
+    out = np.zeros(max(len(tb), 1), dtype=np.int32)
+    k = lib.orc_active_list(len(tb), tb.ctypes.data_as(_ip), m.ctypes.data_as(_dp), ba.ctypes.data_as(_ip),
+                            out.ctypes.data_as(_ip))
+    return out[:k]
+
+
+def wakeup_bins(timebin, wakeup, mass, bin_active, max_time_bin_active: int, lowest_occupied_active_bin: int):
+    """(new timebins, cells moved) by process_wake_ups' rule (core/timestep.cc:1565-1700)."""
+    lib = Oracle(GzParams(), "port").lib
+    tb = np.ascontiguousarray(timebin, dtype=np.int32)
+    wk = np.ascontiguousarray(wakeup, dtype=np.int32)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    ba = np.ascontiguousarray(bin_active, dtype=np.int32)
+    out = np.zeros(len(tb), dtype=np.int32)
+    moved = lib.orc_wakeup_bins(len(tb), tb.ctypes.data_as(_ip), wk.ctypes.data_as(_ip), m.ctypes.data_as(_dp),
+                                ba.ctypes.data_as(_ip), int(max_time_bin_active), int(lowest_occupied_active_bin),
+                                out.ctypes.data_as(_ip))
+    return out, int(moved)

@@ -78,3 +78,33 @@ def load_golden(path: str):
 def workload_from(params, inputs, name="fixture") -> Workload:
     return Workload(name, params, inputs["pos"], inputs["vel"], inputs["mass"], inputs["u"], inputs["dt"],
                     inputs["h"], inputs["cond"])
+
+
+def riemann_fallback_case(method: int, seed: int = 0, n1: int = 10, mach: float = 50.0):
+    """A Sedov lattice given Gaussian random velocities at rms Mach ~`mach` of
+    the background sound speed: so many faces collide or separate supersonically
+    that the HLLC star pressure often exceeds the pressure limit, sending those
+    faces to the exact iterative Riemann solver (reimann.h:625-664) and through
+    the retry with cell-centred states (hydro_core_meshless_functions.h:350-427)."""
+    from gizmo_b200 import ics
+    wl = ics.sedov(n1, seed=seed)
+    wl.params.method = method
+    rng = np.random.default_rng(1000 + seed)
+    cs = np.sqrt(wl.params.gamma * (wl.params.gamma - 1.0) * np.median(wl.u))
+    wl.vel = rng.standard_normal((wl.n, 3)) * mach * cs
+    return wl
+
+
+def riemann_failure_case(method: int):
+    """A Sedov set with one particle of NaN internal energy: its pressure is NaN,
+    so every face it reaches (and, through the gradients, its neighbours' faces)
+    has a NaN star pressure. That is the only way the HLLC stage, whose star
+    pressure is clamped at MIN_REAL, hands a face to the Kurganov-Tadmor solver
+    (reimann.h:445-477); the exact solver and both retries fail too, and the
+    pass stops with 1234 (hydro_core_meshless_functions.h:403-425)."""
+    from gizmo_b200 import ics
+    wl = ics.sedov(8, seed=1)
+    wl.params.method = method
+    wl.u = wl.u.copy()
+    wl.u[100] = float("nan")
+    return wl

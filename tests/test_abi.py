@@ -57,7 +57,9 @@ int main(void) {
     assert got == want
 
 
-@pytest.mark.parametrize("cname,mirror", [("gz_kick_fields", abi.GzKickFields), ("gz_drift_fields", abi.GzDriftFields)])
+@pytest.mark.parametrize("cname,mirror", [("gz_kick_fields", abi.GzKickFields), ("gz_drift_fields", abi.GzDriftFields),
+                                          ("gz_params", abi.GzParams), ("gz_particles", abi.GzParticles),
+                                          ("gz_outputs", abi.GzOutputs), ("gz_status_info", abi.GzStatusInfo)])
 def test_device_field_structs_match_c_field_by_field(tmp_path, cname, mirror):
     """Every field of the ctypes mirror sits at the C offset of the field of the same name: two
     pointer fields in swapped order would keep the size and hand the kernel the wrong arrays."""

@@ -23,7 +23,8 @@ import pytest
 from gizmo_b200 import abi, ics
 from gizmo_b200.hydro import GizmoHydroError, HydroPass
 from oracle import oracle as O
-from tests._util import DENSITY_FIELDS, FORCE_FIELDS, GRADIENT_FIELDS, field_err, norm_err, rel_err, row_rel_err
+from tests._util import (DENSITY_FIELDS, FORCE_FIELDS, GRADIENT_FIELDS, field_err, norm_err, rel_err,
+                         riemann_failure_case, riemann_fallback_case, row_rel_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -370,3 +371,53 @@ def test_kernel_timers_count_the_pass():
     assert t["gradients"]["units"] == wl.n
     assert t["force"]["units"] == st["pairs_symmetric"] // 2
     assert all(v["launches"] == 0 and v["units"] == 0 for v in again.values())
+
+
+@pytest.mark.parametrize("method", [abi.METHOD_MFM, abi.METHOD_MFV], ids=["mfm", "mfv"])
+def test_riemann_fallbacks_match_oracle(method):
+    """Supersonic faces that take the exact iterative Riemann solver and the
+    retry with cell-centred states (hundreds of them, counted by the oracle):
+    the FP64 form matches the oracle pass by pass, and the mixed form stays
+    within the form's bar."""
+    from gizmo_b200 import accuracy
+    wl = riemann_fallback_case(method)
+    st = O.new_state(wl.n, wl.inputs())
+    orc = O.Oracle(wl.params, "port")
+    assert orc.density(st) == 0 and orc.gradients(st) == 0 and orc.force(st) == 0
+    assert orc.riemann_branches()["exact"] > 100
+    check_passwise(wl)
+    out = {}
+    for precision in (abi.PRECISION_FP64, abi.PRECISION_MIXED):
+        wl.params.precision = precision
+        with HydroPass(wl.params) as hp:
+            hp.upload_workload(wl)
+            hp.set_diagnostics(flux_abs=True)
+            hp.full_pass()
+            out[precision] = hp.download(list(accuracy.FIELDS) + ["flux_abs"])
+            out[precision]["status"] = hp.status()
+    o64, o32 = out[abi.PRECISION_FP64], out[abi.PRECISION_MIXED]
+    cs = accuracy.sound_speed(wl.params.gamma, o64["pressure"], o64["rho"])
+    scales = accuracy.flux_scales(wl.vel, wl.mass, wl.u, o64["flux_abs"], method == abi.METHOD_MFV, cs)
+    s = accuracy.summary(accuracy.per_particle(o32, o64, scales), 1e-5)
+    assert s["particles_above_bar_any_field"] == 0, {f: s[f]["max"] for f in accuracy.FIELDS}
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+@pytest.mark.parametrize("method", [abi.METHOD_MFM, abi.METHOD_MFV], ids=["mfm", "mfv"])
+def test_riemann_failure_stops_with_1234(method, precision):
+    """The Kurganov-Tadmor fallback, the exact solver and both retries all fail
+    on a NaN star pressure: the pass stops with the reference's 1234, as the
+    oracle does."""
+    wl = riemann_failure_case(method)
+    wl.params.precision = precision
+    st = O.new_state(wl.n, wl.inputs())
+    orc = O.Oracle(wl.params, "port")
+    assert orc.density(st) == 0 and orc.gradients(st) == 0
+    assert orc.force(st) == abi.ERR_RIEMANN
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.density()
+        hp.hydro_gradient_calc()
+        with pytest.raises(GizmoHydroError) as e:
+            hp.hydro_force()
+        assert e.value.code == abi.ERR_RIEMANN

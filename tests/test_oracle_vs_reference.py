@@ -4,9 +4,9 @@ active subsets, the first-step tolerance, and both methods and kernels."""
 import numpy as np
 import pytest
 
-from gizmo_b200 import ics
+from gizmo_b200 import abi, ics
 from oracle import oracle as O
-from tests._util import DENSITY_FIELDS, GRADIENT_FIELDS, FORCE_FIELDS
+from tests._util import DENSITY_FIELDS, FORCE_FIELDS, GRADIENT_FIELDS, riemann_fallback_case, riemann_failure_case
 
 
 def _cases():
@@ -68,3 +68,44 @@ def test_density_sums_fixed_h_reference():
     a1, p1 = O.Oracle(wl.params, "port", n_threads=1).density_sums(st)
     a2, p2 = O.Oracle(wl.params, "reference", n_threads=1).density_sums(st)
     assert np.array_equal(a1, a2) and np.array_equal(p1, p2)
+
+
+@pytest.mark.parametrize("method", [abi.METHOD_MFM, abi.METHOD_MFV], ids=["mfm", "mfv"])
+def test_riemann_fallbacks_port_equals_reference(method):
+    """Faces that take the exact iterative Riemann solver and the retry with
+    cell-centred states: the port equals the reference bit for bit."""
+    wl = riemann_fallback_case(method)
+    if not O.ref_available(wl.params):
+        pytest.skip("reference build not present")
+    res = {}
+    for kind in ("port", "reference"):
+        st = O.new_state(wl.n, wl.inputs())
+        orc = O.Oracle(wl.params, kind, n_threads=1)
+        assert orc.density(st) == 0 and orc.gradients(st) == 0 and orc.force(st) == 0
+        if kind == "port":
+            branches = orc.riemann_branches()
+        res[kind] = st
+    assert branches["exact"] > 100 and branches["retry_centred"] > 100, branches
+    for f in DENSITY_FIELDS + GRADIENT_FIELDS + FORCE_FIELDS:
+        a, b = res["port"][f], res["reference"][f]
+        if f == "dmass":
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-14 * np.abs(b).max() + 1e-300)
+        else:
+            assert np.array_equal(a, b), f
+
+
+@pytest.mark.parametrize("method", [abi.METHOD_MFM, abi.METHOD_MFV], ids=["mfm", "mfv"])
+def test_riemann_failure_stops_like_the_reference(method):
+    """A NaN star pressure runs the whole cascade -- Kurganov-Tadmor, the exact
+    solver, both retries -- and stops the pass with 1234 on both sides."""
+    wl = riemann_failure_case(method)
+    if not O.ref_available(wl.params):
+        pytest.skip("reference build not present")
+    for kind in ("port", "reference"):
+        st = O.new_state(wl.n, wl.inputs())
+        orc = O.Oracle(wl.params, kind, n_threads=1)
+        assert orc.density(st) == 0 and orc.gradients(st) == 0
+        assert orc.force(st) == abi.ERR_RIEMANN, kind
+        if kind == "port":
+            b = orc.riemann_branches()
+            assert b["kt"] > 0 and b["exact"] > 0 and b["retry_centred"] > 0 and b["retry_at_rest"] > 0, b
