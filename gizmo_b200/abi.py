@@ -29,6 +29,8 @@ ERR_DENSITY_MAXITER = 1155
 ERR_EMPTY_BRACKET = 90001009
 ERR_RIEMANN = 1234
 ERR_NO_PAST_DRIFT = 90001004
+ERR_MIN_TIMESTEP = 888
+ERR_END_OF_TIMELINE = 90001005
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -110,12 +112,26 @@ class GzDriftFields(C.Structure):
         "dudt", "h", "pressure", "ti_current", "status")]
 
 
+class GzTimestepParams(C.Structure):
+    """gz_timestep_params."""
+    _fields_ = [("err_tol_int_accuracy", C.c_double), ("courant_fac", C.c_double),
+                ("max_size_timestep", C.c_double), ("min_size_timestep", C.c_double), ("timebase", C.c_double),
+                ("ti_current", C.c_int64), ("bin_active", C.c_int32 * 60)]
+
+
+class GzTimestepFields(C.Structure):
+    """gz_timestep_fields: device pointers (as integers) of one timestep update."""
+    _fields_ = [("n", C.c_int64)] + [(name, C.c_void_p) for name in (
+        "grav", "accel", "vsig", "h", "num_ngb", "divvel", "mass", "softening", "aphys", "ti_want", "bin",
+        "ti_begstep", "dt_step", "status")]
+
+
 EXPORTED_SYMBOLS = [
     "gz_create", "gz_destroy", "gz_set_params", "gz_set_diagnostics", "gz_upload", "gz_restage", "gz_hydro_density",
     "gz_hydro_gradients", "gz_hydro_force", "gz_download", "gz_status", "gz_stream", "gz_kernel_timing",
     "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
-    "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins",
+    "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins", "gz_timestep",
 ]
 TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
@@ -160,6 +176,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_kick.argtypes = [C.POINTER(GzParams), C.POINTER(GzKickFields), C.c_int, C.c_double, C.c_double, vp]
     lib.gz_drift.argtypes = [C.POINTER(GzParams), C.POINTER(GzDriftFields), C.c_int64, C.c_double, C.c_double,
                              vp]
+    lib.gz_timestep.argtypes = [C.POINTER(GzParams), C.POINTER(GzTimestepParams), C.POINTER(GzTimestepFields), vp]
     lib.gz_set_bin_active.argtypes = [vp, _ip]
     lib.gz_active_list.argtypes = [vp, _ip, _ip, _ip]
     lib.gz_wakeup_bins.argtypes = [vp, _ip, C.c_int, C.c_int, _ip, _ip]

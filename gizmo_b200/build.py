@@ -32,6 +32,7 @@ UNITS = {
     "noalloc.cu": ["-fmad=false"],
     "kick.cu": ["-fmad=false"],
     "drift.cu": ["-fmad=false"],
+    "timestep.cu": ["-fmad=false"],
 }
 
 

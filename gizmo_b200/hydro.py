@@ -334,3 +334,37 @@ def drift(params: abi.GzParams, fields: dict, time1: int, timebase: float, min_e
                                      stream)
     if rc:
         raise GizmoHydroError(rc, "gz_drift")
+
+
+TIMESTEP_DTYPES = {name: "torch.float64" for name in (
+    "grav", "accel", "vsig", "h", "num_ngb", "divvel", "mass", "softening", "aphys")}
+TIMESTEP_DTYPES.update({"ti_want": "torch.int64", "bin": "torch.int32", "ti_begstep": "torch.int64",
+                        "dt_step": "torch.int64", "status": "torch.int32"})
+TIMESTEP_VECTORS = ("grav", "accel")
+
+
+def timestep(params: abi.GzParams, tp: abi.GzTimestepParams, fields: dict, stream: int | None = None) -> None:
+    """New timesteps and bins of a particle set held in device memory, in
+    place: get_timestep (src/core/timestep.cc:357-1416) and the per-particle
+    binning of find_timesteps (timestep.cc:176-215, 265-270).
+
+    ``fields`` maps the gz_timestep_fields names to contiguous CUDA tensors in
+    the caller's order ([n] or [n, 3]); ``grav``, ``softening``, ``aphys``,
+    ``ti_want`` and ``status`` (a one-element int32 tensor that receives 888 or
+    90001005) may be left out. Queued on ``stream`` without waiting."""
+    n = int(fields["mass"].shape[0])
+    f = abi.GzTimestepFields()
+    f.n = n
+    for name, dtype in TIMESTEP_DTYPES.items():
+        t = fields.get(name)
+        if t is None:
+            continue
+        rows = 3 if name in TIMESTEP_VECTORS else 1
+        want = 1 if name == "status" else rows * n
+        if (not t.is_cuda or not t.is_contiguous() or t.numel() != want or str(t.dtype) != dtype
+                or (name != "status" and int(t.shape[0]) != n)):
+            raise ValueError(f"timestep field {name}: want a contiguous CUDA {dtype} tensor of {want} elements")
+        setattr(f, name, t.data_ptr())
+    rc = abi.load_library().gz_timestep(C.byref(params), C.byref(tp), C.byref(f), stream)
+    if rc:
+        raise GizmoHydroError(rc, "gz_timestep")

@@ -58,6 +58,8 @@ extern "C" {
 #define GZ_ERR_EMPTY_BRACKET    90001009 /* density_loop.h:891-895 */
 #define GZ_ERR_RIEMANN          1234    /* hydro_core_meshless_functions.h:403-425 */
 #define GZ_ERR_NO_PAST_DRIFT    90001004 /* drift_particle_functions.h:90-95: a drift into the past */
+#define GZ_ERR_MIN_TIMESTEP     888      /* timestep.cc (STOP_WHEN_BELOW_MINTIMESTEP): a step below MinSizeTimestep */
+#define GZ_ERR_END_OF_TIMELINE  90001005 /* timestep.cc:265-270: a step beyond the end of the timeline */
 
 /* Run-time configuration: the All.* fields and compile-time flags the pass
  * reads. Non-cosmological (cf_atime = 1, ComovingIntegrationOn = 0). */
@@ -353,6 +355,51 @@ typedef struct gz_drift_fields {
  * at most 2 ulp and the pressure by at most 4. */
 int gz_drift(const gz_params *params, const gz_drift_fields *f, int64_t time1, double timebase, double min_egy_spec,
              void *stream);
+
+/* The timestep of every gas cell of a set the caller holds in DEVICE memory:
+ * get_timestep (core/timestep.cc:357-1416) -- the acceleration criterion on
+ * the force softening (KERNEL_CORE_SIZE of params->kernel), the Courant
+ * criterion CourantFac L / (MaxSignalVel / 2) with L = 1.61199 h / NumNgb,
+ * the 1.5 / |divv| limit, MaxSizeTimestep, the MinSizeTimestep floor and the
+ * integer step -- then the per-particle binning of find_timesteps
+ * (timestep.cc:176-215, 265-270): the largest power of two not above it, a
+ * larger bin only where it is active (synchronised), the end of the
+ * timeline; Ti_begstep moves on by the old step. Non-comoving, no dilation;
+ * every cell of the set is treated as active, as gz_kick does. Rows follow
+ * the caller's order; FP64 row-major [n][k]. */
+typedef struct gz_timestep_params {
+    double  err_tol_int_accuracy;  /* All.ErrTolIntAccuracy */
+    double  courant_fac;           /* All.CourantFac */
+    double  max_size_timestep;     /* All.MaxSizeTimestep */
+    double  min_size_timestep;     /* All.MinSizeTimestep */
+    double  timebase;              /* All.Timebase_interval */
+    int64_t ti_current;            /* All.Ti_Current */
+    int32_t bin_active[GZ_TIMEBINS]; /* TimeBinActive after this step's sync point */
+} gz_timestep_params;
+
+typedef struct gz_timestep_fields {
+    int64_t n;
+    const double *grav;       /* [n][3] P.GravAccel (NULL: zero) */
+    const double *accel;      /* [n][3] CellP.HydroAccel */
+    const double *vsig;       /* [n]    CellP.MaxSignalVel */
+    const double *h;          /* [n]    P.KernelRadius */
+    const double *num_ngb;    /* [n]    P.NumNgb (after ^(1/3)) */
+    const double *divvel;     /* [n]    P.Particle_DivVel */
+    const double *mass;       /* [n]    P.Mass */
+    const double *softening;  /* [n]    ForceSoftening_KernelRadius (NULL: zero, the kernel-size fallback) */
+    double       *aphys;      /* [n]    out: |a| as get_timestep returns it through aphys (NULL: skip) */
+    int64_t      *ti_want;    /* [n]    out: get_timestep's integer step before the binning (NULL: skip) */
+    int32_t      *bin;        /* [n]    P.TimeBin                                    in/out */
+    int64_t      *ti_begstep; /* [n]    P.Ti_begstep                                 in/out */
+    int64_t      *dt_step;    /* [n]    P.dt_step                                    in/out */
+    int32_t      *status;     /* [1]    device word: GZ_ERR_MIN_TIMESTEP or GZ_ERR_END_OF_TIMELINE is written
+                                 here unless a code is already there (NULL: not reported) */
+} gz_timestep_fields;
+
+/* New steps and bins of every cell of `f`, queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) without waiting; no context, no
+ * allocation. FP64 without contraction, bit-identical to the reference. */
+int gz_timestep(const gz_params *params, const gz_timestep_params *tp, const gz_timestep_fields *f, void *stream);
 
 #ifdef __cplusplus
 }

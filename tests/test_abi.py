@@ -59,7 +59,9 @@ int main(void) {
 
 @pytest.mark.parametrize("cname,mirror", [("gz_kick_fields", abi.GzKickFields), ("gz_drift_fields", abi.GzDriftFields),
                                           ("gz_params", abi.GzParams), ("gz_particles", abi.GzParticles),
-                                          ("gz_outputs", abi.GzOutputs), ("gz_status_info", abi.GzStatusInfo)])
+                                          ("gz_outputs", abi.GzOutputs), ("gz_status_info", abi.GzStatusInfo),
+                                          ("gz_timestep_params", abi.GzTimestepParams),
+                                          ("gz_timestep_fields", abi.GzTimestepFields)])
 def test_device_field_structs_match_c_field_by_field(tmp_path, cname, mirror):
     """Every field of the ctypes mirror sits at the C offset of the field of the same name: two
     pointer fields in swapped order would keep the size and hand the kernel the wrong arrays."""
