@@ -132,6 +132,7 @@ EXPORTED_SYMBOLS = [
     "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
     "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins", "gz_timestep",
+    "gz_upload_device", "gz_download_device",
 ]
 TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
@@ -163,6 +164,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_kernel_timing.argtypes = [vp, C.c_int]
     lib.gz_kernel_time.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
+    lib.gz_upload_device.argtypes = [vp, C.POINTER(GzParticles)]
+    lib.gz_download_device.argtypes = [vp, C.POINTER(GzOutputs)]
     lib.gz_restage.argtypes = [vp]
     for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):
         getattr(lib, name).argtypes = [vp, _ip, C.c_int]

@@ -883,7 +883,9 @@ static int stage_inputs(gz_context *c)
     return 0;
 }
 
-int gz_upload(gz_context *c, const gz_particles *in)
+// gz_upload from host arrays (kind = kind) or from the
+// caller's device arrays (cudaMemcpyDeviceToDevice, gz_upload_device).
+static int upload_from(gz_context *c, const gz_particles *in, cudaMemcpyKind kind)
 {
     if (!c || !in || in->n < 0 || in->n > INT32_MAX / 16) return GZ_ERR_ARG;
     if (in->n > 0 && (!in->pos || !in->vel || !in->mass || !in->u || !in->dt || !in->h)) return GZ_ERR_ARG;
@@ -910,12 +912,12 @@ int gz_upload(gz_context *c, const gz_particles *in)
                                     force_record_bytes(0), force_record_bytes(1)}) * N))
         return c->err;
     if (n > 0) {
-        GZ_CUDA(c, cudaMemcpyAsync(c->stage3.p, in->pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
-        GZ_CUDA(c, cudaMemcpyAsync(c->o_vel.p, in->vel, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s));
+        GZ_CUDA(c, cudaMemcpyAsync(c->stage3.p, in->pos, sizeof(double) * 3 * (size_t)n, kind, s));
+        GZ_CUDA(c, cudaMemcpyAsync(c->o_vel.p, in->vel, sizeof(double) * 3 * (size_t)n, kind, s));
         struct { const double *src; DevBuf *dst; } f1[] = {
             {in->mass, &c->o_mass}, {in->u, &c->o_u}, {in->dt, &c->o_dt}, {in->h, &c->o_h}, {in->cond, &c->o_cond}};
         for (auto &f : f1) {
-            if (f.src) GZ_CUDA(c, cudaMemcpyAsync(f.dst->p, f.src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+            if (f.src) GZ_CUDA(c, cudaMemcpyAsync(f.dst->p, f.src, sizeof(double) * (size_t)n, kind, s));
             else GZ_CUDA(c, cudaMemsetAsync(f.dst->p, 0, sizeof(double) * (size_t)n, s));
         }
     }
@@ -925,12 +927,14 @@ int gz_upload(gz_context *c, const gz_particles *in)
             ensure(c, c->timebin, sizeof(int) * N) || ensure(c, c->vsig_prev, sizeof(double) * N) ||
             ensure(c, c->wakeup, sizeof(int) * N))
             return c->err;
-        for (int k = 0; k < n; k++)
-            if (in->timebin[k] < 0 || in->timebin[k] >= GZ_TIMEBINS) return fail(c, GZ_ERR_ARG, "timebin out of range");
+        if (kind == cudaMemcpyHostToDevice)
+            for (int k = 0; k < n; k++)
+                if (in->timebin[k] < 0 || in->timebin[k] >= GZ_TIMEBINS)
+                    return fail(c, GZ_ERR_ARG, "timebin out of range");
         if (n > 0) {
-            GZ_CUDA(c, cudaMemcpyAsync(c->o_timebin.p, in->timebin, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+            GZ_CUDA(c, cudaMemcpyAsync(c->o_timebin.p, in->timebin, sizeof(int) * (size_t)n, kind, s));
             if (in->vsig)
-                GZ_CUDA(c, cudaMemcpyAsync(c->o_vsig.p, in->vsig, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+                GZ_CUDA(c, cudaMemcpyAsync(c->o_vsig.p, in->vsig, sizeof(double) * (size_t)n, kind, s));
             else
                 GZ_CUDA(c, cudaMemsetAsync(c->o_vsig.p, 0, sizeof(double) * (size_t)n, s));
         }
@@ -939,6 +943,10 @@ int gz_upload(gz_context *c, const gz_particles *in)
     GZ_CUDA(c, cudaStreamSynchronize(s));
     return c->err;
 }
+
+int gz_upload(gz_context *c, const gz_particles *in) { return upload_from(c, in, cudaMemcpyHostToDevice); }
+
+int gz_upload_device(gz_context *c, const gz_particles *in) { return upload_from(c, in, cudaMemcpyDeviceToDevice); }
 
 int gz_restage(gz_context *c)
 {
@@ -1164,7 +1172,9 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     return GZ_OK;
 }
 
-int gz_download(gz_context *c, const gz_outputs *o)
+// gz_download into host arrays through the staging buffer, or (to_device)
+// straight into the caller's device arrays (gz_download_device).
+static int download_to(gz_context *c, const gz_outputs *o, bool to_device)
 {
     if (!c || !o) return GZ_ERR_ARG;
     if (o->flux_abs && !c->fabs_valid)
@@ -1186,8 +1196,9 @@ int gz_download(gz_context *c, const gz_outputs *o)
         if ((size_t)cnt * sizeof(double) > c->dl.bytes || (size_t)cnt * sizeof(double) > e.src->bytes)
             return fail(c, GZ_ERR_CAPACITY, "download staging smaller than the field");
         k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, e.k, ptr<int>(c->perm), ptr<double>(*e.src),
-                                                                      ptr<double>(c->dl));
+                                                                      to_device ? e.dst : ptr<double>(c->dl));
         c->launches++;
+        if (to_device) continue;
         GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaStreamSynchronize(s));
     }
@@ -1199,27 +1210,38 @@ int gz_download(gz_context *c, const gz_outputs *o)
         if ((size_t)cnt * sizeof(double) > c->dl.bytes) return fail(c, GZ_ERR_CAPACITY, "download staging too small");
         k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, k, ptr<int>(c->perm),
                                                                       ptr<double>(c->grad) + (size_t)e.off * n,
-                                                                      ptr<double>(c->dl));
+                                                                      to_device ? e.dst : ptr<double>(c->dl));
         c->launches++;
+        if (to_device) continue;
         GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
         GZ_CUDA(c, cudaStreamSynchronize(s));
     }
     if (o->iters) {
-        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters), ptr<int>(c->dl));
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters),
+                                                      to_device ? o->iters : ptr<int>(c->dl));
         c->launches++;
-        GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
-        GZ_CUDA(c, cudaStreamSynchronize(s));
+        if (!to_device) {
+            GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+            GZ_CUDA(c, cudaStreamSynchronize(s));
+        }
     }
     if (o->wakeup) {
         if (!c->have_bins) return fail(c, GZ_ERR_ORDER, "wakeup: no timebins were uploaded");
-        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->wakeup), ptr<int>(c->dl));
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->wakeup),
+                                                      to_device ? o->wakeup : ptr<int>(c->dl));
         c->launches++;
-        GZ_CUDA(c, cudaMemcpyAsync(o->wakeup, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        if (!to_device)
+            GZ_CUDA(c, cudaMemcpyAsync(o->wakeup, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
     }
     GZ_CUDA(c, cudaGetLastError());
     GZ_CUDA(c, cudaStreamSynchronize(s));
     return GZ_OK;
 }
+
+
+int gz_download(gz_context *c, const gz_outputs *o) { return download_to(c, o, false); }
+
+int gz_download_device(gz_context *c, const gz_outputs *o) { return download_to(c, o, true); }
 
 
 // Host-side reorder of rows built for the sorted targets into the caller's

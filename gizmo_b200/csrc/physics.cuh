@@ -793,11 +793,13 @@ GZ_HD void riemann_solver(RVec<T> rv, ROut<T> &o, const T *n, T ptl, const GCons
 }
 
 // reconstruct_face_states, non-MHD (reimann.h:125-244).
-// `scale` bounds the magnitudes Q_i and Q_j were computed from (they may be
-// differences, e.g. v - v_frame; 0 for density and pressure): the
-// sign-preserving clamps jump where Qmax, Qmin or their extended bounds cross
-// zero, so a crossing within the FP32 error of that scale is decided in FP64.
-template <typename T>
+// POS: density and pressure, positive and exact in sign, which enter the
+// Riemann problem relatively, so their face states are checked for relative
+// precision. Otherwise (velocities, differences v - v_frame) `scale` bounds
+// the magnitudes Q_i and Q_j were computed from: the sign-preserving clamps
+// jump where Qmax, Qmin or their extended bounds cross zero, so a crossing
+// within the FP32 error of that scale is decided in FP64.
+template <bool POS, typename T>
 GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, const T *d_j, T &Q_L, T &Q_R, int mode,
                         T scale, Guard<T> &g)
 {
@@ -820,7 +822,7 @@ GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, c
         // Qmax and Qmin carry the error of the values they were computed from
         // (none for rho and P, whose signs are exact); the extended bounds that
         // of their own terms
-        if (scale > T(0)) {
+        if constexpr (!POS) {
             g.near(Qmax, T(0), scale, 22);
             g.near(Qmin, T(0), scale, 23);
         }
@@ -852,9 +854,7 @@ GZ_HD void reconstruct(T Q_i, const T *g_i, T Q_j, const T *g_j, const T *d_i, c
         if (Q_L < Qmin_eff) { Q_L = Qmin_eff; tL = tmine; }
         if (Q_L > Qmed_max) { Q_L = Qmed_max; tL = tmedx; }
     }
-    // density and pressure enter the Riemann problem relatively: their face
-    // states must hold their relative precision
-    if (scale == T(0)) {
+    if constexpr (POS) {
         g.precise(Q_R, tR, 35);
         g.precise(Q_L, tL, 36);
     }
@@ -995,10 +995,10 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         if (vdotf2_phys < T(0)) v2_approach = dmax(v2_approach, vdotf2_phys * vdotf2_phys);
         int recon_mode = 1;
         if (leak_vs_tol > 1.0) recon_mode = 0;
-        reconstruct(I.rho, I.grho, J.rho, J.grho, d_i, d_j, rv.L.rho, rv.R.rho, recon_mode, T(0), g);
-        reconstruct(Pressure_i, I.gp, Pressure_j, J.gp, d_i, d_j, rv.L.p, rv.R.p, recon_mode, T(0), g);
+        reconstruct<true>(I.rho, I.grho, J.rho, J.grho, d_i, d_j, rv.L.rho, rv.R.rho, recon_mode, T(0), g);
+        reconstruct<true>(Pressure_i, I.gp, Pressure_j, J.gp, d_i, d_j, rv.L.p, rv.R.p, recon_mode, T(0), g);
         for (int k = 0; k < 3; k++)
-            reconstruct(I.v[k] - vframe[k], I.gv + 3 * k, J.v[k] - vframe[k], J.gv + 3 * k, d_i, d_j, rv.L.v[k],
+            reconstruct<false>(I.v[k] - vframe[k], I.gv + 3 * k, J.v[k] - vframe[k], J.gv + 3 * k, d_i, d_j, rv.L.v[k],
                         rv.R.v[k], recon_mode, fabs(I.v[k]) + fabs(J.v[k]) + fabs(vframe[k]), g);
         const T press_i_tot = Pressure_i + I.rho * v2_approach;
         const T press_j_tot = Pressure_j + J.rho * v2_approach;

@@ -184,6 +184,16 @@ int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
 /* Copy outputs device -> host (original order). */
 int gz_download(gz_context *ctx, const gz_outputs *out);
 
+/* gz_upload and gz_download with the caller's arrays in DEVICE memory (the
+ * same layouts; device-to-device copies and scatters, no host traffic), for a
+ * host that keeps its particle arena on the GPU and chains the pass with
+ * gz_timestep, gz_kick and gz_drift there. gz_upload_device does not check
+ * the timebin range (gz_upload does); gz_download_device returns with its
+ * scatters queued on the context's stream (gz_stream): order later work on
+ * other streams after it. */
+int gz_upload_device(gz_context *ctx, const gz_particles *in);
+int gz_download_device(gz_context *ctx, const gz_outputs *out);
+
 /* Individual timesteps. GZ_TIMEBINS is TIMEBINS (declarations/allvars.h). */
 #define GZ_TIMEBINS 60
 /* TimeBinActive[GZ_TIMEBINS] for the wake-up test of the following force

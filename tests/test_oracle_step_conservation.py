@@ -98,6 +98,8 @@ def _run(method, n_steps, courant=0.2):
         ti += step
     # under MFV the conserved mass still owed by the last kick's dMass is part of the total
     end = _totals(mass_true + (out["dmass"] if method == METHOD_MFV else 0.0), vel, u)
+    _run.final = {"pos": pos, "vel": vel, "u": u, "mass": mass, "mass_true": mass_true, "h": h,
+                  "dmass": out["dmass"]}
     return start, end, ti
 
 
