@@ -73,6 +73,12 @@ def parse_args():
     ap.add_argument("--n", type=int, default=1 << 24, help="particles of --kernel")
     ap.add_argument("--method", choices=["mfm", "mfv"], default="mfv", help="hydro method of --kernel")
     ap.add_argument("--reps", type=int, default=20, help="timed launches of --kernel")
+    ap.add_argument("--subsets", action="store_true",
+                    help="individual-timestep active subsets of 8,388,608 particles (log-normal, sigma 2.0): "
+                         "one JSON line of rates per active fraction, the grid reused across substeps")
+    ap.add_argument("--boxes", action="store_true",
+                    help="512 independent boxes of 1,024-65,536 particles (shock tubes and Sedov blasts): "
+                         "one JSON line of rates, mixed and FP64")
     return ap.parse_args()
 
 
@@ -642,8 +648,119 @@ def time_step_kernel(args):
                       "frac": (gbs / peak) if peak else None, "particles_per_s": n / (ms * 1e-3)}))
 
 
+# ------------------------------------------------ active subsets and batched boxes
+def run_subsets(args):
+    """Individual-timestep substeps: 8,388,608 particles of a log-normal field
+    (sigma_lnrho 2.0, Wendland C2, 64 neighbours, MFM). After one full pass the
+    active set of each fraction f in {0.001, 0.01, 0.1, 1} is the f N particles
+    of smallest h / c_s (the shortest timesteps). The grid (Morton order and
+    octree) is built once; each timed substep runs density, gradients and force
+    on the active set only, from the kernel lengths of the substep before, with
+    no restage, for the mixed and the FP64 form. Rate = active particles / s."""
+    import torch
+
+    from gizmo_b200 import abi, ics
+    from gizmo_b200.hydro import HydroPass
+
+    n = args.n if args.n != (1 << 24) else (1 << 23)
+    t0 = time.time()
+    wl = ics.lognormal(203, sigma_lnrho=2.0, seed_density=6, seed_velocity=7, n_particles=n)
+    t_gen = time.time() - t0
+    res = {"metric": "active particle-updates/s per substep", "unit": "particle-updates/s",
+           "config": {"workload": f"log-normal field sigma_lnrho=2.0, {n:,} particles, MFM, Wendland C2, 64 ngb",
+                      "active": "the f N particles of smallest h/c_s", "grid": "built once, reused by every substep",
+                      "steps": args.steps, "warmup": args.warmup, "generate_s": round(t_gen, 1)},
+           "fractions": {}}
+    with HydroPass(wl.params) as hp:  # converge once in FP64 (slices bound the cold seed's rows)
+        hp.upload_workload(wl)
+        chunk = 1 << 21
+        for a in range(0, n, chunk):
+            hp.density(np.arange(a, min(n, a + chunk), dtype=np.int32))
+        hp.hydro_gradient_calc()
+        hp.hydro_force()
+        conv = hp.download(["h", "cond", "rho", "pressure"])
+    wl.h, wl.cond = conv["h"], conv["cond"]
+    cs = np.sqrt(wl.params.gamma * conv["pressure"] / conv["rho"])
+    order = np.argsort(conv["h"] / cs, kind="stable")
+    for precision, tag in ((abi.PRECISION_MIXED, "mixed"), (abi.PRECISION_FP64, "fp64")):
+        wl.params.precision = precision
+        with HydroPass(wl.params) as hp:
+            hp.upload_workload(wl)
+            hp.full_pass()
+            stream = torch.cuda.ExternalStream(hp.stream)
+            for f in (0.001, 0.01, 0.1, 1.0):
+                k = max(1, int(round(f * n)))
+                act = np.sort(order[:k]).astype(np.int32)
+                for _ in range(args.warmup):
+                    hp.full_pass(act)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(args.steps):
+                    hp.full_pass(act)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / args.steps
+                res["fractions"].setdefault(str(f), {})[tag] = {"active": k, "ms_per_substep": ms,
+                                                                "value": k / (ms * 1e-3)}
+    for f, d in res["fractions"].items():
+        d["mixed_over_fp64"] = d["mixed"]["value"] / d["fp64"]["value"]
+    print(json.dumps(res), flush=True)
+
+
+def run_boxes(args):
+    """512 independent periodic boxes, log-uniform in [1,024, 65,536] particles
+    (seed 5; each a 3-D shock tube or a Sedov blast), one context reused across
+    the boxes: per box an upload from pinned host buffers, a full pass and the
+    download of the rates, timed over all boxes with CUDA events. Rate =
+    particles of all boxes / total time, mixed and FP64 form."""
+    import torch
+
+    from gizmo_b200 import abi, ics
+    from gizmo_b200.hydro import HydroPass
+
+    t0 = time.time()
+    boxes = ics.boxes(512, seed=5)
+    t_gen = time.time() - t0
+    total = sum(b.n for b in boxes)
+    res = {"metric": "particle-updates/s over 512 independent boxes", "unit": "particle-updates/s",
+           "config": {"workload": f"512 boxes, {total:,} particles, log-uniform 1,024-65,536 per box, shock tubes "
+                                  "and Sedov blasts, MFM, cubic, 32 ngb", "generate_s": round(t_gen, 1),
+                      "launch": "one pass per box on one context (the boxes are not yet one launch)"}}
+    for precision, tag in ((abi.PRECISION_MIXED, "mixed"), (abi.PRECISION_FP64, "fp64")):
+        params = boxes[0].params
+        params.precision = precision
+        with HydroPass(params) as hp:
+            stream = torch.cuda.ExternalStream(hp.stream)
+            for b in boxes[:8]:  # warm-up
+                hp.set_params(b.params)
+                hp.upload_workload(b)
+                hp.full_pass()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for b in boxes:
+                b.params.precision = precision
+                hp.set_params(b.params)
+                hp.upload_workload(b)
+                hp.full_pass()
+                hp.download(["accel", "dudt"])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sec = e0.elapsed_time(e1) / 1e3
+        res[tag] = {"value": total / sec, "seconds": sec}
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    print(json.dumps(res), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.subsets:
+        run_subsets(args)
+        return
+    if args.boxes:
+        run_boxes(args)
+        return
     if args.profile_pass:
         profile_pass(args)
         return

@@ -112,6 +112,10 @@ class GzDriftFields(C.Structure):
         "dudt", "h", "pressure", "ti_current", "status")]
 
 
+class GzTuning(C.Structure):
+    _fields_ = [("leaf_max", C.c_int), ("reserved", C.c_int), ("row_slots", C.c_double)]
+
+
 class GzTimestepParams(C.Structure):
     """gz_timestep_params."""
     _fields_ = [("err_tol_int_accuracy", C.c_double), ("courant_fac", C.c_double),
@@ -132,7 +136,7 @@ EXPORTED_SYMBOLS = [
     "gz_kernel_time",
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
     "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins", "gz_timestep",
-    "gz_upload_device", "gz_download_device",
+    "gz_upload_device", "gz_download_device", "gz_get_tuning", "gz_set_tuning", "gz_autotune",
 ]
 TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
@@ -165,6 +169,9 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.gz_kernel_time.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.gz_upload.argtypes = [vp, C.POINTER(GzParticles)]
     lib.gz_upload_device.argtypes = [vp, C.POINTER(GzParticles)]
+    lib.gz_get_tuning.argtypes = [vp, C.POINTER(GzTuning)]
+    lib.gz_set_tuning.argtypes = [vp, C.POINTER(GzTuning)]
+    lib.gz_autotune.argtypes = [vp, C.POINTER(GzTuning)]
     lib.gz_download_device.argtypes = [vp, C.POINTER(GzOutputs)]
     lib.gz_restage.argtypes = [vp]
     for name in ("gz_hydro_density", "gz_hydro_gradients", "gz_hydro_force"):

@@ -7,6 +7,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -94,6 +97,9 @@ struct gz_context {
     } timers[GZ_TIMERS];
     bool fabs_valid = false;         // the last force pass summed flux_abs
     int sms = 148;                   // multiprocessors of the device
+    // walk tuning (gz_tuning): neither changes a result, both change the walk's cost
+    int leaf_max = kLeafMax;         // octree leaf size
+    double row_slots = 2.5;          // padded density-row slots per expected row entry
 };
 
 namespace {
@@ -636,7 +642,7 @@ int build_tree(gz_context *c)
     const unsigned long long *keys = ptr<unsigned long long>(c->keys_sorted);
     while (cnt > 0) {
         if (ensure(c, c->t_nch, sizeof(long long) * (size_t)cnt)) return c->err;
-        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<long long>(c->t_nch), s);
+        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<long long>(c->t_nch), c->leaf_max, s);
         c->launches++;
         long long next = 0;
         if (exclusive_scan_counts(c, cnt, c->t_nch, c->t_cpos, &next)) return c->err;
@@ -1000,9 +1006,10 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
                                                                iter == 0 ? kDensityBufferFirst : kDensityBuffer,
                                                                ptr<double>(c->h_built));
             c->launches++;
-            // slots per padded row: 2.5 x the expected row length, in multiples of 32
+            // slots per padded row: row_slots (2.5 by default) x the expected row length, in multiples of 32
             const double f = iter == 0 ? kDensityBufferFirst : kDensityBuffer;
-            const int cap = std::max(32, std::min(4096, 32 * (int)std::ceil(2.5 * c->prm.des_num_ngb * f * f * f / 32.0)));
+            const int cap = std::max(
+                32, std::min(4096, 32 * (int)std::ceil(c->row_slots * c->prm.des_num_ngb * f * f * f / 32.0)));
             long long used = 0, entries = 0;
             if (build_rows_padded(c, ptr<double>(c->h_built), grow, n_grow, cap, base, &used, &entries)) return c->err;
             base = used;
@@ -1372,6 +1379,98 @@ int gz_density_sums(gz_context *c, const int *active, int n_active, double *acc,
             for (int k = 0; k < 3; k++) pv[(size_t)r * 3 + k] = t >= 0 ? a17[(size_t)(14 + k) * n + t] : 0.0;
     }
     return read_status(c) ? c->err : GZ_OK;
+}
+
+int gz_get_tuning(gz_context *c, gz_tuning *t)
+{
+    if (!c || !t) return GZ_ERR_ARG;
+    t->leaf_max = c->leaf_max;
+    t->reserved = 0;
+    t->row_slots = c->row_slots;
+    return GZ_OK;
+}
+
+int gz_set_tuning(gz_context *c, const gz_tuning *t)
+{
+    if (!c || !t || t->leaf_max < 8 || t->leaf_max > 1024 || !(t->row_slots >= 1.0 && t->row_slots <= 16.0))
+        return GZ_ERR_ARG;
+    if (t->leaf_max != c->leaf_max) c->grid_valid = c->grid_valid && c->n == 0;  // the tree is rebuilt at restage
+    c->leaf_max = t->leaf_max;
+    c->row_slots = t->row_slots;
+    return GZ_OK;
+}
+
+namespace {
+// Tuned walk settings per device, particle count (rounded to a power of two)
+// and neighbour count: a context that meets a key already tuned in this
+// process takes the result without timing again.
+struct TuneKey {
+    int device, log2n, ngb, kernel;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(device, log2n, ngb, kernel) < std::tie(o.device, o.log2n, o.ngb, o.kernel);
+    }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, gz_tuning> g_tuned;
+}  // namespace
+
+int gz_autotune(gz_context *c, gz_tuning *chosen)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "autotune before upload");
+    int log2n = 0;
+    while ((1ll << log2n) < (long long)std::max(c->n, 1)) log2n++;
+    const TuneKey key{c->device, log2n, (int)std::lround(c->prm.des_num_ngb), c->prm.kernel};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            c->leaf_max = it->second.leaf_max;
+            c->row_slots = it->second.row_slots;
+            if (chosen) *chosen = it->second;
+            return gz_restage(c);
+        }
+    }
+    // Each candidate: rebuild the grid (gz_restage: the uploaded h again) and
+    // run a density pass over every particle, timed on the context's stream.
+    // The rows, and so every result, are the same for every candidate.
+    cudaEvent_t e0, e1;
+    GZ_CUDA(c, cudaEventCreate(&e0));
+    GZ_CUDA(c, cudaEventCreate(&e1));
+    auto trial = [&](int leaf, double slots, float &ms) -> int {
+        c->leaf_max = leaf;
+        c->row_slots = slots;
+        GZ_CUDA(c, cudaEventRecord(e0, c->stream));
+        if (gz_restage(c) || gz_hydro_density(c, nullptr, 0)) return c->err;
+        GZ_CUDA(c, cudaEventRecord(e1, c->stream));
+        GZ_CUDA(c, cudaEventSynchronize(e1));
+        GZ_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+        return 0;
+    };
+    gz_tuning best{c->leaf_max, 0, c->row_slots};
+    float best_ms = 1e30f, ms = 0;
+    int rc = 0;
+    for (int leaf : {32, 64, 96, 128}) {
+        if ((rc = trial(leaf, best.row_slots, ms))) break;
+        if (ms < best_ms) { best_ms = ms; best.leaf_max = leaf; }
+    }
+    for (double slots : {1.5, 2.0, 3.0}) {
+        if (rc || (rc = trial(best.leaf_max, slots, ms))) break;
+        if (ms < best_ms) { best_ms = ms; best.row_slots = slots; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    c->leaf_max = best.leaf_max;
+    c->row_slots = best.row_slots;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[key] = best;
+    }
+    if (chosen) *chosen = best;
+    return gz_restage(c);
 }
 
 int gz_set_bin_active(gz_context *c, const int *bin_active)

@@ -5,7 +5,7 @@
 // src/mesh/gpu_neighbor_list.h:207-264). Particles are sorted by a 63-bit
 // Morton key (21 bits per axis); every octree node is then one contiguous
 // run of the sorted arrays. The tree is explicit: it is split top-down one
-// level per launch (a node with more than kLeafMax particles gets its
+// level per launch (a node with more than leaf_max particles gets its
 // non-empty children, stored contiguously), then a single bottom-up launch
 // gives every node the tight bounding box of its particles and the maximum
 // of their h. A 1e5 density contrast only adds levels where the particles
@@ -87,13 +87,13 @@ GZ_DEV void child_bounds(const unsigned long long *__restrict__ keys, int a, int
 
 // number of non-empty children of every node of one level
 __global__ void k_tree_count(const unsigned long long *__restrict__ keys, int L, const int4 *__restrict__ node,
-                             int beg, int cnt, long long *nch)
+                             int beg, int cnt, long long *nch, int leaf_max)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
     const int4 nd = node[beg + i];
     int c = 0;
-    if (nd.y > kLeafMax && L < kBits) {
+    if (nd.y > leaf_max && L < kBits) {
         int bound[9];
         child_bounds(keys, nd.x, nd.x + nd.y, L, bound);
         for (int d = 0; d < 8; d++) c += bound[d + 1] > bound[d];
@@ -648,9 +648,10 @@ void grid_keys(int n, const double *pos, double box, unsigned long long *keys, i
     if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
 }
 
-void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch, cudaStream_t s)
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch,
+                int leaf_max, cudaStream_t s)
 {
-    if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch);
+    if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch, leaf_max);
 }
 
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,

@@ -10,7 +10,8 @@ namespace gz {
 
 // grid.cu
 void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s);
-void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch, cudaStream_t s);
+void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch,
+                int leaf_max, cudaStream_t s);
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
                 const long long *cpos, int next, cudaStream_t s);
 void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,

@@ -50,11 +50,11 @@ GZ_DEV void wakeup_test(const Particles &ps, int t, int j, double vsig_ts)
 // Octree over the Morton-sorted particles (63-bit keys, 21 levels): node i
 // owns the sorted run [first, first + count); an internal node's children
 // are the nodes [child, child + nchild); a leaf (child = -1) has at most
-// kLeafMax particles unless it is at the deepest level (coincident keys).
+// leaf_max particles unless it is at the deepest level (coincident keys).
 // Leaves are tested 32 particles at a time; leaves of up to 96 particles
 // (measured against 8 to 128) cost the walk fewer node openings than the extra
 // candidate tests they bring.
-constexpr int kLeafMax = 96;
+constexpr int kLeafMax = 96;  // the default leaf size (gz_tuning.leaf_max)
 
 struct Tree {
     double box;

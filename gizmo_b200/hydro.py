@@ -197,6 +197,24 @@ class HydroPass:
         self.hydro_gradient_calc(active)
         self.hydro_force(active)
 
+    # -- walk tuning ------------------------------------------------------------
+    def tuning(self) -> dict:
+        t = abi.GzTuning()
+        self._check(self.lib.gz_get_tuning(self._ctx, C.byref(t)))
+        return {"leaf_max": t.leaf_max, "row_slots": t.row_slots}
+
+    def set_tuning(self, leaf_max: int, row_slots: float):
+        """Walk settings for the next upload/restage (no result depends on them)."""
+        t = abi.GzTuning()
+        t.leaf_max, t.row_slots = int(leaf_max), float(row_slots)
+        self._check(self.lib.gz_set_tuning(self._ctx, C.byref(t)))
+
+    def autotune(self) -> dict:
+        """Time the walk settings on the uploaded set and keep the fastest."""
+        t = abi.GzTuning()
+        self._check(self.lib.gz_autotune(self._ctx, C.byref(t)))
+        return {"leaf_max": t.leaf_max, "row_slots": t.row_slots}
+
     # -- individual timesteps ---------------------------------------------------
     def set_bin_active(self, bin_active):
         """TimeBinActive[60] for the wake-up test of the following force passes

@@ -232,8 +232,9 @@ def _solenoidal_velocity(ng: int, slope: float, rng: np.random.Generator) -> np.
 
 
 def lognormal(n1: int = 128, sigma_lnrho: float = 1.5, seed_density: int = 2, seed_velocity: int = 3,
-              grid: int | None = None, precision: int = PRECISION_FP64) -> Workload:
-    N = n1 ** 3
+              grid: int | None = None, precision: int = PRECISION_FP64, n_particles: int | None = None) -> Workload:
+    """n1^3 particles, or n_particles when given (the density grid follows n1)."""
+    N = n1 ** 3 if n_particles is None else int(n_particles)
     ng = grid or min(2 * n1, 256)
     rng = np.random.default_rng(seed_density)
     delta = _grf(ng, -3.0, rng) * sigma_lnrho

@@ -194,6 +194,29 @@ int gz_download(gz_context *ctx, const gz_outputs *out);
 int gz_upload_device(gz_context *ctx, const gz_particles *in);
 int gz_download_device(gz_context *ctx, const gz_outputs *out);
 
+/* Tuning of the neighbour walk (no reference counterpart). Neither setting
+ * changes a result -- the rows are the exact neighbour sets in ascending order
+ * whatever the tree -- both change what the walk costs:
+ *   leaf_max   octree leaf size (particles), 96 by default;
+ *   row_slots  slots per padded density row, as a multiple of the expected row
+ *              length (2.5 by default); a longer row is rebuilt behind the
+ *              padded block.
+ * gz_set_tuning takes effect at the next gz_upload or gz_restage.
+ * gz_autotune times a rebuild of the grid and a density pass over every
+ * particle of the uploaded set for leaf_max in {32, 64, 96, 128} and then
+ * row_slots in {1.5, 2.0, 2.5, 3.0}, keeps the fastest, remembers it for the
+ * device, the particle count (to a power of two), DesNumNgb and the kernel
+ * (a later context with the same key takes it without timing), and leaves
+ * the set restaged as after gz_upload. */
+typedef struct gz_tuning {
+    int    leaf_max;
+    int    reserved;
+    double row_slots;
+} gz_tuning;
+int gz_get_tuning(gz_context *ctx, gz_tuning *out);
+int gz_set_tuning(gz_context *ctx, const gz_tuning *t);
+int gz_autotune(gz_context *ctx, gz_tuning *chosen);
+
 /* Individual timesteps. GZ_TIMEBINS is TIMEBINS (declarations/allvars.h). */
 #define GZ_TIMEBINS 60
 /* TimeBinActive[GZ_TIMEBINS] for the wake-up test of the following force
