@@ -1394,7 +1394,6 @@ int gz_set_tuning(gz_context *c, const gz_tuning *t)
 {
     if (!c || !t || t->leaf_max < 8 || t->leaf_max > 1024 || !(t->row_slots >= 1.0 && t->row_slots <= 16.0))
         return GZ_ERR_ARG;
-    if (t->leaf_max != c->leaf_max) c->grid_valid = c->grid_valid && c->n == 0;  // the tree is rebuilt at restage
     c->leaf_max = t->leaf_max;
     c->row_slots = t->row_slots;
     return GZ_OK;
