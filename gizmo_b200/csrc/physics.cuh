@@ -20,6 +20,8 @@ template <> struct Real<double> {
     static GZ_HD double min_real() { return 1e-56; }  // MIN_REAL_NUMBER
     static GZ_HD double sqrt_(double x) { return sqrt(x); }
     static GZ_HD double pow_(double x, double y) { return pow(x, y); }
+    // x^y - 1 as the reference writes it (pow, then the subtraction)
+    static GZ_HD double powm1_(double x, double y) { return pow(x, y) - 1.0; }
     static GZ_HD bool isnan_(double x) { return isnan(x); }
     // HLLC degenerate-wave tolerance 1e-12 (|S_L| + |S_R| + MIN_REAL), reimann.h:570
     static GZ_HD double hllc_tol(double s) { return 1.e-12 * (s + 1e-56); }
@@ -35,6 +37,10 @@ template <> struct Real<float> {
     static GZ_HD float min_real() { return 1e-37f; }
     static GZ_HD float sqrt_(float x) { return sqrtf(x); }
     static GZ_HD float pow_(float x, float y) { return powf(x, y); }
+    // x^y - 1 through expm1(y log x): for a near-isothermal gas y = (gamma - 1) / (2 gamma) is
+    // tiny and x^y lies within a few FP32 ulps of 1, so pow(x, y) - 1 would keep no significant
+    // bit (and the exact solver's Newton iteration would converge on the rounding of it)
+    static GZ_HD float powm1_(float x, float y) { return expm1f(y * logf(x)); }
     static GZ_HD bool isnan_(float x) { return isnan(x); }
     // same tolerance, floored at the smallest normal so the all-zero vacuum
     // state (S_L = S_M = S_R = 0) is still trapped instead of dividing 0 by 0
@@ -76,6 +82,7 @@ template <> struct Guard<double> {
     GZ_HD void near(double, double, double, int = 0) {}
     GZ_HD void precise(double, double, int = 0) {}
     GZ_HD void flag(int = 0) {}
+    GZ_HD void power(double, int = 0) {}
     GZ_HD int fragile() const { return 0; }
 };
 // The site numbers name the guarded decisions; built with GZ_GUARD_SITES the
@@ -97,6 +104,10 @@ template <> struct Guard<float> {
         set(!(fabsf(value) * kPrecise > 1.1920929e-7f * terms), site);
     }
     GZ_HD void flag(int site = 0) { set(true, site); }
+    // x^y about to be taken in FP32: its relative error is |y| times that of x (2^-24 from
+    // the rounding of x, a few ulps more from the operations that formed it), beyond
+    // kPrecise for the large exponents of a near-isothermal gas (2 gamma / (gamma - 1))
+    GZ_HD void power(float y, int site = 0) { set(fabsf(y) * 4.0f * 5.9604645e-8f > kPrecise, site); }
     GZ_HD int fragile() const { return f != 0; }
 };
 
@@ -569,7 +580,7 @@ GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T c
             Z_L = a2 * (T(1.0) - T(0.5) * (Pg - rv.L.p) / (a1 + Pg));
         } else {
             pratio = Pg / rv.L.p;
-            W_L = gc.G4 * cL * (Real<T>::pow_(pratio, gc.G1) - T(1));
+            W_L = gc.G4 * cL * Real<T>::powm1_(pratio, gc.G1);
             Z_L = T(1) / (rv.L.rho * cL) * Real<T>::pow_(Pg / rv.L.p, -gc.G2);
         }
         if (Pg > rv.R.p) {
@@ -578,7 +589,7 @@ GZ_HD int riemann_iterative(const RVec<T> &rv, ROut<T> &o, T vL, T vR, T cL, T c
             Z_R = a2 * (T(1.0) - T(0.5) * (Pg - rv.R.p) / (a1 + Pg));
         } else {
             pratio = Pg / rv.R.p;
-            W_R = gc.G4 * cR * (Real<T>::pow_(pratio, gc.G1) - T(1));
+            W_R = gc.G4 * cR * Real<T>::powm1_(pratio, gc.G1);
             Z_R = T(1) / (rv.R.rho * cR) * Real<T>::pow_(pratio, -gc.G2);
         }
         if (niter < 1000 / 2) Pg -= (W_L + W_R + dvel) / (Z_L + Z_R);
@@ -675,6 +686,7 @@ GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR
             }
             S_eff = gc.G5 * (cL + gc.G7 * vL + S);
             C_eff = gc.G5 * (cL + gc.G7 * (vL - S));
+            g.power(gc.G3, 17);  // inside the left fan
             o.F.rho = rv.L.rho * Real<T>::pow_(C_eff / cL, gc.G4);
             o.F.p = rv.L.p * Real<T>::pow_(C_eff / cL, gc.G3);
             for (int k = 0; k < 3; k++) o.F.v[k] = rv.L.v[k] + n[k] * (S_eff - vL);
@@ -721,6 +733,7 @@ GZ_HD void sample_standard(const RVec<T> &rv, ROut<T> &o, const T *n, T vL, T vR
     }
     S_eff = gc.G5 * (-cR + gc.G7 * vR + S);
     C_eff = gc.G5 * (cR - gc.G7 * (vR - S));
+    g.power(gc.G3, 17);  // inside the right fan
     o.F.rho = rv.R.rho * Real<T>::pow_(C_eff / cR, gc.G4);
     o.F.p = rv.R.p * Real<T>::pow_(C_eff / cR, gc.G3);
     for (int k = 0; k < 3; k++) o.F.v[k] = rv.R.v[k] + n[k] * (S_eff - vR);
@@ -753,9 +766,13 @@ __host__ __device__ __noinline__ void riemann_exact(const RVec<T> &rv, ROut<T> &
     }
     if ((rv.L.rho > T(0)) && (rv.R.rho > T(0))) {
         if (riemann_iterative(rv, o, vL, vR, cL, cR, gc, g)) sample_standard(rv, o, n, vL, vR, cL, cR, gc, g);
-        else sample_vac_internal(rv, o, n, vL, vR, cL, cR, gc);
+        else {
+            if (gc.mfv) g.power(gc.G3, 16);  // the vacuum fans' states are powers of G3 and G4
+            sample_vac_internal(rv, o, n, vL, vR, cL, cR, gc);
+        }
     } else {
         if ((rv.L.rho < T(0)) || (rv.R.rho < T(0))) { stop = 1234545; return; }
+        if (gc.mfv) g.power(gc.G3, 16);
         if (rv.L.rho > T(0)) sample_vac_right(rv, o, n, vL, cL, gc);
         if (rv.R.rho > T(0)) sample_vac_left(rv, o, n, vR, cR, gc);
     }
@@ -1043,27 +1060,29 @@ GZ_HD void force_pair(int kf, int mfv, int selfgravity_off, const GConst<T> &gc,
         for (int k = 0; k < 3; k++) Fl.v[k] = ro.F.v[k] * FAN;
         if (!mfv) {  // MFM face entropic switch, hydro_core_meshless_functions.h:515-574
             const T SM_over_ceff = fabs(ro.S_M) / dmin(I.cs, J.cs);
+            const T facenorm_pm = ro.P_M * FAN;
+            const T PdV_fac = ro.P_M * vdotr2_phys / T(1.0);
+            const T PdV_i = dwk_i * V_i * V_i * I.drk * PdV_fac;
+            const T PdV_j = dwk_j * V_j * V_j * J.drk * PdV_fac;
+            const T du_old = facenorm_pm * (ro.S_M + face_area_dot_vel);
+            const T du_new = T(0.5) * (PdV_i - PdV_j + facenorm_pm * (face_vel_i + face_vel_j));
+            // The switch's tests (SM/c against eps_big, which opens the switch, and eps_small, and
+            // the signs and sizes of the energy changes each side would see) choose between du_old
+            // and du_new: a flip moves the flux by |du_new - du_old|. Guarded only where that is
+            // not negligible on the scale of the face's work terms; the opening test is guarded
+            // whichever way FP32 takes it.
+            const T es = fabs(du_old) + fabs(du_new) + fabs(facenorm_pm * face_vel_i) +
+                         fabs(facenorm_pm * face_vel_j);
+            const bool switch_matters = fabs(du_new - du_old) > T(1e-6) * es;
+            if (switch_matters && !(leak_vs_tol > 1.0)) g.near(SM_over_ceff, eps_big, eps_big, 29);
             if ((SM_over_ceff < eps_big) || (leak_vs_tol > 1.0)) {
                 int use = 1;
-                const T facenorm_pm = ro.P_M * FAN;
-                const T PdV_fac = ro.P_M * vdotr2_phys / T(1.0);
-                const T PdV_i = dwk_i * V_i * V_i * I.drk * PdV_fac;
-                const T PdV_j = dwk_j * V_j * V_j * J.drk * PdV_fac;
-                const T du_old = facenorm_pm * (ro.S_M + face_area_dot_vel);
-                const T du_new = T(0.5) * (PdV_i - PdV_j + facenorm_pm * (face_vel_i + face_vel_j));
                 const double ratio = 1.001;
                 const double to_i = I.prd, to_j = J.prd;
-                // The switch's tests (SM/c against eps_big and eps_small, and the signs and sizes of
-                // the energy changes each side would see) choose between du_old and du_new: a flip
-                // moves the flux by |du_new - du_old|. Guarded only where that is not negligible on
-                // the scale of the face's work terms.
-                const T es = fabs(du_old) + fabs(du_new) + fabs(facenorm_pm * face_vel_i) +
-                             fabs(facenorm_pm * face_vel_j);
-                if (fabs(du_new - du_old) > T(1e-6) * es) {
-                    g.near(SM_over_ceff, eps_big, eps_big, 29);
+                if (switch_matters) {
                     if (cnum2 < cnumcrit2) {
                         const T dtoj = -du_old + facenorm_pm * face_vel_j, dtoi = +du_old - facenorm_pm * face_vel_i;
-                        g.near(SM_over_ceff, eps_small, eps_small, 30);
+                        g.near(SM_over_ceff, eps_small, T(0.1), 30);  // S_M to ~1e-6 c (the exact solver's tolerance)
                         g.near(dtoj, T(0), es, 31);
                         g.near(dtoi, T(0), es, 32);
                         g.near(dtoj, -du_new + facenorm_pm * face_vel_j, es, 33);

@@ -6,7 +6,8 @@ fluxes summed into them (gizmo_b200/accuracy.py states the denominators).
 The cases are the named generators at sizes a GPU pass takes in milliseconds:
 the Plummer mixture (MFV, HLLC, cubic kernel, 32 neighbours, density contrast
 ~1e5) and the log-normal field (MFM, Wendland C2, 64 neighbours, rms Mach 2)
-at 64^3 = 262,144 particles, and the Sedov blast at its full 32^3. Both forms
+at 64^3 = 262,144 particles, the Sedov blast at its full 32^3, and the
+log-normal field at its full 128^3 from the benchmark's steady-state seed. Both forms
 start from the same inputs and converge to bit-identical h (their density sums
 and h-iteration are the same FP64 kernels), and their gradients are the same
 FP64 sums, so these fields must agree exactly; the force pair is FP32 in the
@@ -21,10 +22,27 @@ from gizmo_b200.hydro import HydroPass
 
 pytestmark = pytest.mark.gpu
 
+
+def _steady(wl):
+    """The timed-pass seed of the benchmark: h converged once in FP64, then
+    moved by U(-5%, 5%) (ics.steady_state_seed)."""
+    wl.params.precision = abi.PRECISION_FP64
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.density()
+        conv = hp.download(["h", "cond"])
+    wl.h = ics.steady_state_seed(conv["h"], 4)
+    wl.cond = conv["cond"]
+    return wl
+
+
 CASES = {
     "plummer64": lambda: ics.plummer_mix(64, seed=4),
     "lognormal64": lambda: ics.lognormal(64, seed_density=2, seed_velocity=3),
     "sedov32": lambda: ics.sedov(32, seed=1),
+    # the log-normal field's full size (2,097,152 particles, gamma = 1.0001): the near-isothermal
+    # exact-solver pairs and the faces at the entropic switch's opening test
+    "lognormal128": lambda: _steady(ics.lognormal(128, seed_density=2, seed_velocity=3)),
 }
 
 
