@@ -257,52 +257,70 @@ def run_ours(args, world, rank, local):
     hpm = HydroPass(pmix, device=local)
     hpm.upload_workload(wl)
 
-    def run_steps(hp, K, W, record_clock=False):
+    def run_steps(hp, K, W, record_clock=False, graph=True, timing=False):
+        """K timed steps of restage + pass after W untimed ones. graph: the pass
+        as one CUDA graph (gz_hydro_pass), events around the restage and the
+        graph; otherwise the three plain calls with events between them (and,
+        with timing, the library's per-kernel timers)."""
         stream = torch.cuda.ExternalStream(hp.stream)
         for _ in range(W):
             hp.restage()
-            hp.full_pass()
+            if graph:
+                hp.hydro_pass(graph=True)
+            else:
+                hp.full_pass()
         torch.cuda.synchronize()
         dist_barrier(world)
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if record_clock else None
-        if record_clock:
+        if timing:
             hp.kernel_timing(True)
         l0 = hp.status()["kernel_launches"]
-        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+        names = ["grid", "pass"] if graph else ["grid", "density", "gradients", "force"]
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)] for _ in range(K)]
         for k in range(K):
             ev[k][0].record(stream)
             hp.restage()
             ev[k][1].record(stream)
-            hp.density()
-            ev[k][2].record(stream)
-            hp.hydro_gradient_calc()
-            ev[k][3].record(stream)
-            hp.hydro_force()
-            ev[k][4].record(stream)
+            if graph:
+                hp.hydro_pass(graph=True)
+                ev[k][2].record(stream)
+            else:
+                hp.density()
+                ev[k][2].record(stream)
+                hp.hydro_gradient_calc()
+                ev[k][3].record(stream)
+                hp.hydro_force()
+                ev[k][4].record(stream)
         torch.cuda.synchronize()
         dist_barrier(world)
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         launches = hp.status()["kernel_launches"] - l0
         ktimes = None
-        if record_clock:
+        if timing:
             ktimes = hp.kernel_times()
             hp.kernel_timing(False)
-        total = ev[0][0].elapsed_time(ev[K - 1][4]) / 1e3
+        total = ev[0][0].elapsed_time(ev[K - 1][len(names)]) / 1e3
         parts = {nm: float(np.mean([ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(K)])) / 1e3
-                 for i, nm in enumerate(["grid", "density", "gradients", "force"])}
+                 for i, nm in enumerate(names)}
         return total, parts, clocks, launches, ktimes
 
     K, W = args.steps, args.warmup
-    t_mix, parts_mix, clocks, launches, ktimes = run_steps(hpm, K, W, record_clock=True)
+    # the headline: each step a restage (grid build) and the pass as one CUDA graph
+    t_mix, graph_mix, clocks, launches, _ = run_steps(hpm, K, W, record_clock=True)
     st_mix = hpm.status()
-    t_64, parts_64, _, _, _ = run_steps(hp64, max(1, min(K, 3)), max(1, min(W, 2)))
+    gstats = hpm.graph_stats()
     K64 = max(1, min(K, 3))
+    t_64, graph_64, _, _, _ = run_steps(hp64, K64, max(1, min(W, 2)))
     t_mix = dist_max(t_mix, world, "ours")
     t_64 = dist_max(t_64, world, "ours")
     value = world * N * K / t_mix
     value64 = world * N * K64 / t_64
+    # stage breakdown and per-kernel timers: plain passes (the graph has no
+    # events inside), a few steps of each form
+    _, parts_mix, _, _, ktimes = run_steps(hpm, K64, 1, graph=False, timing=True)
+    _, parts_64, _, _, _ = run_steps(hp64, K64, 1, graph=False)
 
     # Accuracy of the mixed form against the FP64 form (same inputs), per
     # particle and field (gizmo_b200/accuracy.py): h, rho, pressure, vsig
@@ -438,6 +456,13 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
         "pass_ms": {form: {k: round(1e3 * v, 2) for k, v in parts.items()}
                     for form, parts in (("mixed", parts_mix), ("fp64", parts_64))},
+        "graph": {"steps_ms": {form: {k: round(1e3 * v, 2) for k, v in parts.items()}
+                               for form, parts in (("mixed", graph_mix), ("fp64", graph_64))},
+                  "captures": gstats["captures"], "replays": gstats["replays"], "fallbacks": gstats["fallbacks"],
+                  "kernels_per_replay": gstats["kernels_top"] + gstats["kernels_after"]
+                  + gstats["kernels_per_iteration"] * st_mix["density_iterations"],
+                  "what": "value and fp64_value: restage + gz_hydro_pass(GZ_PASS_GRAPH) per step; pass_ms and the "
+                          "kernel rooflines: plain calls with events between the stages"},
         "conservation": cons, "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
     }
     # the long tables go to stderr (the one stdout line stays short)
@@ -452,7 +477,7 @@ def run_ours(args, world, rank, local):
         stream = torch.cuda.ExternalStream(hpm.stream)
         for _ in range(max(1, min(W, 2))):
             hpm.upload_raw(N, {k: t.data_ptr() for k, t in pin.items()})
-            hpm.full_pass()
+            hpm.hydro_pass(graph=True)
             hpm.download_raw({k: t.data_ptr() for k, t in pout.items()})
         torch.cuda.synchronize()
         dist_barrier(world)
@@ -461,7 +486,7 @@ def run_ours(args, world, rank, local):
         e0.record(stream)
         for _ in range(Ke):
             hpm.upload_raw(N, {k: t.data_ptr() for k, t in pin.items()})
-            hpm.full_pass()
+            hpm.hydro_pass(graph=True)
             hpm.download_raw({k: t.data_ptr() for k, t in pout.items()})
         e1.record(stream)
         torch.cuda.synchronize()

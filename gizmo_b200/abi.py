@@ -116,6 +116,12 @@ class GzTuning(C.Structure):
     _fields_ = [("leaf_max", C.c_int), ("reserved", C.c_int), ("row_slots", C.c_double)]
 
 
+class GzGraphInfo(C.Structure):
+    """gz_graph_info."""
+    _fields_ = [("captures", C.c_int64), ("replays", C.c_int64), ("fallbacks", C.c_int64),
+                ("kernels_top", C.c_int64), ("kernels_per_iteration", C.c_int64), ("kernels_after", C.c_int64)]
+
+
 class GzTimestepParams(C.Structure):
     """gz_timestep_params."""
     _fields_ = [("err_tol_int_accuracy", C.c_double), ("courant_fac", C.c_double),
@@ -137,7 +143,9 @@ EXPORTED_SYMBOLS = [
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
     "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins", "gz_timestep",
     "gz_upload_device", "gz_download_device", "gz_get_tuning", "gz_set_tuning", "gz_autotune",
+    "gz_hydro_pass", "gz_graph_stats",
 ]
+PASS_GRAPH = 1  # GZ_PASS_GRAPH
 TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS

@@ -100,6 +100,18 @@ struct gz_context {
     // walk tuning (gz_tuning): neither changes a result, both change the walk's cost
     int leaf_max = kLeafMax;         // octree leaf size
     double row_slots = 2.5;          // padded density-row slots per expected row entry
+    // the pass over every particle captured as one CUDA graph (gz_hydro_pass)
+    struct Graph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaStream_t body[2] = {nullptr, nullptr};  // streams the conditional bodies are captured on
+        std::vector<unsigned long long> sig;        // what the graph was captured for (buffers, sizes, settings)
+        long long kernels_top = 0, kernels_loop = 0, kernels_sym = 0, kernels_tail = 0;
+        long long rq_cap = 0;                       // refine-queue room the graph was captured with
+        long long replays = 0, captures = 0, fallbacks = 0;
+        bool capturing = false;                     // no timer events while a graph is captured
+    } g;
+    DevBuf gstate, g_hseed, g_cseed, g_over_list, g_over_off, g_sel;
 };
 
 namespace {
@@ -122,7 +134,7 @@ int lanes_per_row(const gz_context *c, long long rows, int min_lanes)
 // when no event could be had: that launch then goes untimed).
 const EventPair *timer_launch(gz_context *c, int id, long long units)
 {
-    if (!c->timing) return nullptr;
+    if (!c->timing || c->g.capturing) return nullptr;
     gz_context::Timer &t = c->timers[id];
     if (t.used == t.ev.size()) {
         EventPair e{nullptr, nullptr};
@@ -267,7 +279,8 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->t_cpos, &c->acc, &c->h_built, &c->scratch, &c->keep, &c->regrow, &c->todo_a, &c->todo_b, &c->grow,
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
             &c->s_counts, &c->rec, &c->work, &c->hmax, &c->refined, &c->rq, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl, &c->o_timebin,
-            &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out};
+            &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out,
+            &c->gstate, &c->g_hseed, &c->g_cseed, &c->g_over_list, &c->g_over_off, &c->g_sel};
 }
 
 Tree tree_view(gz_context *c)
@@ -746,6 +759,630 @@ int build_sym_rows(gz_context *c, int rows, bool all)
     return 0;
 }
 
+// ------------------------------------------------- the pass as one CUDA graph
+// gz_hydro_pass over every particle: density (the iteration as a WHILE node
+// whose body is one iteration, sized from the device state), then, if every
+// target converged, the symmetric rows from the density rows, and, if those
+// fit their buffers, gradients and force (two nested IF nodes). The kernels
+// are the plain pass's (the density rows, sums, after_iter, symmetric rows,
+// gradient and force kernels) or their device-sized forms, which give every
+// row the same entries and sums: only the order of the targets in the
+// iteration's lists differs, and no result depends on it. A buffer that
+// would overflow stops the graph's work (GraphState::fail); the host then
+// restores the kernel lengths and condition numbers the graph started from
+// and runs the plain pass.
+
+__global__ void k_g_init(GraphState *gs, int n)
+{
+    GraphState g{};
+    g.n_todo = n;
+    g.n_grow = n;
+    *gs = g;
+}
+
+// start of an iteration: this iteration's padded block and density lanes
+__global__ void k_g_prep(GraphState *gs, int cap0, int cap1, long long nbr_cap, int n_particles,
+                         long long group_warps, int sms)
+{
+    GraphState &g = *gs;
+    g.n_next = 0;
+    g.n_regrow = 0;
+    g.n_over = 0;
+    g.sums_next = 0;
+    g.after_next = 0;
+    g.extra = 0;
+    g.next_group[0] = g.next_group[1] = 0;
+    // lanes per density row: lanes_per_row(n_todo, 4)
+    const long long want = (long long)sms * 2048 * 8;
+    int tpt = 4;
+    while (tpt < 16 && (long long)g.n_todo * tpt < want) tpt *= 2;
+    g.tpt = tpt;
+    g.need = g.base;
+    if (g.n_grow > 0) {
+        g.cap = g.iter == 0 ? cap0 : cap1;
+        g.need = g.base + (long long)g.n_grow * g.cap;
+        if (g.need > nbr_cap) g.fail |= kGraphFailRows;
+        // the walk mode of walk_rows (both modes write the same rows)
+        const bool sparse = (long long)g.n_grow * 4 < n_particles;
+        g.walk_solo = (g.n_grow == 1 || (sparse && (g.n_grow + 31) / 32 < group_warps)) ? 1 : 0;
+    }
+}
+
+__global__ void k_g_row_radius(const GraphState *gs, const int *__restrict__ first, const int *__restrict__ grow,
+                               const double *__restrict__ h, double f0, double f1, double *h_built)
+{
+    if (gs->fail) return;
+    const int n = gs->n_grow;
+    const int *t = gs->iter == 0 ? first : grow;
+    const double f = gs->iter == 0 ? f0 : f1;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) h_built[t[a]] = h[t[a]] * f;
+}
+
+// After the padded fill: a row that fit gets [base + a cap, + count), a longer
+// one a place behind the block (its fill walk follows); the entries are counted.
+__global__ void k_g_padded_rows(GraphState *gs, const int *__restrict__ first, const int *__restrict__ grow,
+                                const long long *__restrict__ counts, long long *beg, long long *end, int *over_list,
+                                long long *over_off)
+{
+    if (gs->fail) return;
+    const int n = gs->n_grow, cap = gs->cap;
+    const long long base = gs->base, need = gs->need;
+    const int *t = gs->iter == 0 ? first : grow;
+    long long built = 0;
+    for (int a0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); a0 < n; a0 += gridDim.x * blockDim.x) {
+        const int a = a0 + (threadIdx.x & 31);
+        if (a < n) {
+            const long long c = counts[a];
+            built += c;
+            const int i = t[a];
+            if (c <= cap) {
+                beg[i] = base + (long long)a * cap;
+                end[i] = base + (long long)a * cap + c;
+            } else {
+                const int k = atomicAdd(&gs->n_over, 1);
+                const long long o = (long long)atomicAdd((unsigned long long *)&gs->extra, (unsigned long long)c);
+                over_list[k] = i;
+                over_off[k] = o;
+                beg[i] = need + o;
+                end[i] = need + o + c;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) built += __shfl_xor_sync(0xffffffffu, built, o);
+    if ((threadIdx.x & 31) == 0 && built) atomicAdd((unsigned long long *)&gs->entries, (unsigned long long)built);
+}
+
+// the overflow rows' room, then the entries in use after this iteration
+__global__ void k_g_over_check(GraphState *gs, long long nbr_cap)
+{
+    GraphState &g = *gs;
+    if (g.fail || g.n_grow == 0) return;
+    if (g.need + g.extra > nbr_cap) { g.fail |= kGraphFailRows; return; }
+    g.base = g.need + g.extra;
+}
+
+// Stable selection of the flagged slots of this iteration's list (count on
+// the device), in three steps over chunks of kSelChunk slots: each chunk's
+// counts, their exclusive scan (one block), then each chunk's writes at its
+// offset in slot order: the order CUB's DeviceSelect::Flagged gives the plain
+// pass. Two flag arrays at once: still iterating -> `next`, radius outgrew
+// its row -> `grow`.
+constexpr int kSelChunk = 1024;
+__global__ void __launch_bounds__(kSelChunk) k_sel_count(const GraphState *gs, const unsigned char *__restrict__ fa,
+                                                         const unsigned char *__restrict__ fb, int *ca, int *cb)
+{
+    __shared__ int sa[32], sb[32];
+    if (gs->fail) return;
+    const int n = gs->n_todo, chunks = (n + kSelChunk - 1) / kSelChunk;
+    for (int ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+        const int i = ch * kSelChunk + threadIdx.x;
+        const int a = (i < n) ? fa[i] : 0, b = (i < n) ? fb[i] : 0;
+        const int wa = __popc(__ballot_sync(0xffffffffu, a)), wb = __popc(__ballot_sync(0xffffffffu, b));
+        if ((threadIdx.x & 31) == 0) { sa[threadIdx.x >> 5] = wa; sb[threadIdx.x >> 5] = wb; }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int x = sa[threadIdx.x], y = sb[threadIdx.x];
+            for (int o = 16; o > 0; o >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, o); y += __shfl_xor_sync(0xffffffffu, y, o); }
+            if (threadIdx.x == 0) { ca[ch] = x; cb[ch] = y; }
+        }
+        __syncthreads();
+    }
+}
+
+// exclusive scan of the chunk counts in place; the totals into the state
+__global__ void __launch_bounds__(kSelChunk) k_sel_scan(GraphState *gs, int *ca, int *cb)
+{
+    __shared__ int pa[kSelChunk], pb[kSelChunk];
+    if (gs->fail) return;
+    const int n = gs->n_todo, chunks = (n + kSelChunk - 1) / kSelChunk;
+    // each thread scans a contiguous run of chunks, then the run totals are scanned
+    const int per = (chunks + kSelChunk - 1) / kSelChunk;
+    const int c0 = threadIdx.x * per, c1 = min(chunks, c0 + per);
+    int ta = 0, tb = 0;
+    for (int c = c0; c < c1; c++) { ta += ca[c]; tb += cb[c]; }
+    pa[threadIdx.x] = ta;
+    pb[threadIdx.x] = tb;
+    __syncthreads();
+    for (int o = 1; o < kSelChunk; o <<= 1) {
+        const int xa = threadIdx.x >= o ? pa[threadIdx.x - o] : 0, xb = threadIdx.x >= o ? pb[threadIdx.x - o] : 0;
+        __syncthreads();
+        pa[threadIdx.x] += xa;
+        pb[threadIdx.x] += xb;
+        __syncthreads();
+    }
+    int oa = pa[threadIdx.x] - ta, ob = pb[threadIdx.x] - tb;  // exclusive
+    for (int c = c0; c < c1; c++) {
+        const int xa = ca[c], xb = cb[c];
+        ca[c] = oa;
+        cb[c] = ob;
+        oa += xa;
+        ob += xb;
+    }
+    if (threadIdx.x == kSelChunk - 1) {
+        gs->n_next = pa[kSelChunk - 1];
+        gs->n_regrow = pb[kSelChunk - 1];
+    }
+}
+
+__global__ void __launch_bounds__(kSelChunk) k_sel_write(const GraphState *gs, const int *__restrict__ todo,
+                                                         const unsigned char *__restrict__ fa,
+                                                         const unsigned char *__restrict__ fb,
+                                                         const int *__restrict__ ca, const int *__restrict__ cb,
+                                                         int *next, int *grow)
+{
+    __shared__ int sa[32], sb[32];
+    if (gs->fail) return;
+    const int n = gs->n_todo, chunks = (n + kSelChunk - 1) / kSelChunk;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+        const int i = ch * kSelChunk + threadIdx.x;
+        const bool a = (i < n) && fa[i], b = (i < n) && fb[i];
+        const unsigned ma = __ballot_sync(0xffffffffu, a), mb = __ballot_sync(0xffffffffu, b);
+        if (lane == 0) { sa[w] = __popc(ma); sb[w] = __popc(mb); }
+        __syncthreads();
+        if (w == 0) {  // exclusive scan of the 32 warp counts
+            int x = sa[lane], y = sb[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int px = __shfl_up_sync(0xffffffffu, x, o), py = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) { x += px; y += py; }
+            }
+            sa[lane] = x - sa[lane];
+            sb[lane] = y - sb[lane];
+        }
+        __syncthreads();
+        const unsigned below = (1u << lane) - 1u;
+        if (a) next[ca[ch] + sa[w] + __popc(ma & below)] = todo[i];
+        if (b) grow[cb[ch] + sb[w] + __popc(mb & below)] = todo[i];
+        __syncthreads();
+    }
+}
+
+// end of an iteration: the targets still iterating (selected in order into
+// `next`) become the list, the next iteration's counts are set, and whether it
+// runs (thread 0 of block 0; the others copy)
+__global__ void k_g_next(GraphState *gs, const int *__restrict__ next, int *todo, cudaGraphConditionalHandle loop)
+{
+    const int m = gs->fail ? 0 : gs->n_next;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < m; a += gridDim.x * blockDim.x) todo[a] = next[a];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        GraphState &g = *gs;
+        g.n_todo = m;
+        g.n_grow = g.fail ? 0 : g.n_regrow;
+        g.iter++;
+        g.todo_left = g.n_todo;
+        cudaGraphSetConditional(loop, (!g.fail && g.n_todo > 0 && g.iter < kMaxIter) ? 1u : 0u);
+    }
+}
+
+// after the loop: the symmetric rows follow only if every target converged
+__global__ void k_g_if_converged(const GraphState *gs, cudaGraphConditionalHandle h)
+{
+    cudaGraphSetConditional(h, (!gs->fail && gs->todo_left == 0) ? 1u : 0u);
+}
+
+// the symmetric rows' total against their buffers and the pair-flux buffer
+__global__ void k_g_sym_check(GraphState *gs, const long long *total, long long cap, cudaGraphConditionalHandle h)
+{
+    const long long t = *total;
+    gs->sym_total = t;
+    const bool ok = t <= cap;
+    if (!ok) gs->fail |= kGraphFailSym;
+    cudaGraphSetConditional(h, ok ? 1u : 0u);
+}
+
+int density_caps(const gz_context *c, int *cap0, int *cap1)
+{
+    const double fs[2] = {kDensityBufferFirst, kDensityBuffer};
+    int *out[2] = {cap0, cap1};
+    for (int k = 0; k < 2; k++) {
+        const double f = fs[k];
+        *out[k] = std::max(32, std::min(4096, 32 * (int)std::ceil(c->row_slots * c->prm.des_num_ngb * f * f * f / 32.0)));
+    }
+    return 0;
+}
+
+// Room the graph works in: the plain pass's buffers at their sizes after a
+// plain pass, the row buffers with a margin. Symmetric rows, pair fluxes and
+// the refine queue take the last pass's count plus a quarter. Returns kNoRoom
+// (no error recorded) when the device has no room for them: the pass then
+// runs plain.
+constexpr int kNoRoom = -1;
+int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap)
+{
+    const int n = c->n;
+    const size_t N = (size_t)std::max(n, 1);
+    int cap0 = 0, cap1 = 0;
+    density_caps(c, &cap0, &cap1);
+    const long long nbr_need = (long long)n * cap0 + std::max<long long>(n / 8, 4096) * cap1;
+    if (nbr_need > (long long)INT32_MAX * 4) return kNoRoom;
+    const long long sc = c->pairs_symmetric + c->pairs_symmetric / 4 + 1024;
+    const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
+    const long long rq = mixed ? std::max(65536ll, sc / 8) : 0;
+    if (ensure(c, c->targets, sizeof(int) * N) || ensure(c, c->todo_a, sizeof(int) * N) ||
+        ensure(c, c->todo_b, sizeof(int) * N) || ensure(c, c->grow, sizeof(int) * N) ||
+        ensure(c, c->counts, sizeof(long long) * N) || ensure(c, c->hmax, sizeof(unsigned long long)) ||
+        ensure(c, c->gstate, sizeof(GraphState)) || ensure(c, c->g_hseed, sizeof(double) * N) ||
+        ensure(c, c->g_cseed, sizeof(double) * N) || ensure(c, c->g_over_list, sizeof(int) * N) ||
+        ensure(c, c->g_over_off, sizeof(long long) * N) || ensure(c, c->s_acnt, sizeof(int) * N) ||
+        ensure(c, c->s_bcnt, sizeof(int) * N) || ensure(c, c->s_counts, sizeof(long long) * N) ||
+        ensure(c, c->s_off, sizeof(long long) * (N + 1)) || ensure(c, c->refined, sizeof(unsigned long long)) ||
+        ensure(c, c->keep, N) || ensure(c, c->regrow, N) ||
+        ensure(c, c->g_sel, sizeof(int) * 2 * (N / kSelChunk + 1)))
+        return c->err;
+    // the large buffers: without room for them the pass runs plain (which
+    // allocates what it needs again)
+    if (c->d_nbr_cap < nbr_need || !c->d_nbr.p) {
+        if (!try_ensure(c->d_nbr, sizeof(int) * (size_t)nbr_need)) { c->d_nbr_cap = 0; return kNoRoom; }
+        c->d_nbr_cap = nbr_need;
+    }
+    if (!try_ensure(c->s_tmp, sizeof(int) * (size_t)sc)) return kNoRoom;
+    if ((long long)(c->s_nbr.bytes / sizeof(int)) < sc || !c->s_nbr.p) {
+        if (!try_ensure(c->s_nbr, sizeof(int) * (size_t)sc)) { c->s_nbr_cap = 0; return kNoRoom; }
+        c->s_nbr_cap = (long long)(c->s_nbr.bytes / sizeof(int));
+    }
+    if (!try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)sc)) return kNoRoom;
+    if (mixed && !try_ensure(c->rq, sizeof(RefineItem) * (size_t)rq)) return kNoRoom;
+    size_t tmp = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tmp, ptr<long long>(c->s_counts), ptr<long long>(c->s_off) + 1, n,
+                                  c->stream);
+    if (ensure(c, c->cub_tmp, tmp)) return c->err;
+    *sym_cap = std::min<long long>({sc, (long long)(c->s_nbr.bytes / sizeof(int)), (long long)(c->s_tmp.bytes / sizeof(int)),
+                                    (long long)(c->pflux.bytes / pair_flux_bytes(mixed))});
+    *rq_cap = rq;
+    return 0;
+}
+
+// what a captured graph depends on: every buffer's address and size, the
+// particle count, the pass settings
+std::vector<unsigned long long> graph_signature(gz_context *c)
+{
+    std::vector<unsigned long long> v;
+    for (DevBuf *b : all_buffers(c)) { v.push_back((unsigned long long)(uintptr_t)b->p); v.push_back(b->bytes); }
+    v.push_back((unsigned long long)c->n);
+    const unsigned char *pp = (const unsigned char *)&c->pp;
+    for (size_t k = 0; k < sizeof(PassParams); k++) v.push_back(pp[k]);
+    v.push_back((unsigned long long)c->prm.precision);
+    v.push_back((unsigned long long)(c->row_slots * 1024));
+    v.push_back((unsigned long long)(c->have_bins ? 1 : 0) | (c->binact_on ? 2 : 0));
+    v.push_back((unsigned long long)c->d_nbr_cap);
+    v.push_back((unsigned long long)c->s_nbr_cap);
+    v.push_back((unsigned long long)c->sms);
+    return v;
+}
+
+void graph_release(gz_context *c)
+{
+    if (c->g.exec) cudaGraphExecDestroy(c->g.exec);
+    if (c->g.graph) cudaGraphDestroy(c->g.graph);
+    c->g.exec = nullptr;
+    c->g.graph = nullptr;
+    c->g.sig.clear();
+}
+
+// the runtime's last error, recorded against `where`
+int check_last(gz_context *c, const char *where)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return 0;
+    char b[200];
+    snprintf(b, sizeof(b), "captured pass, %s: %s", where, cudaGetErrorString(e));
+    return fail(c, GZ_ERR_CUDA, b);
+}
+
+// A conditional handle of the graph being captured on `s` (reset to
+// `default_value` at every launch of the graph).
+int make_handle(gz_context *c, cudaStream_t s, cudaGraphConditionalHandle *h, unsigned int default_value)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    GZ_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
+    if (st != cudaStreamCaptureStatusActive) return fail(c, GZ_ERR_CUDA, "captured pass: stream not capturing");
+    GZ_CUDA(c, cudaGraphConditionalHandleCreate(h, g, default_value, cudaGraphCondAssignDefault));
+    return 0;
+}
+
+// A conditional node after the work captured so far on `s`; the stream's
+// later work depends on it. Returns its body graph.
+int add_conditional(gz_context *c, cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t *body)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    GZ_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) return fail(c, GZ_ERR_CUDA, "captured pass: stream not capturing");
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    GZ_CUDA(c, cudaGraphAddNode(&node, g, deps, nd, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    GZ_CUDA(c, cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return 0;
+}
+
+// The work of the three bodies, captured on `s` (a body stream).
+int capture_density_iteration(gz_context *c, cudaStream_t s, cudaGraphConditionalHandle loop)
+{
+    const int n = c->n;
+    int cap0 = 0, cap1 = 0;
+    density_caps(c, &cap0, &cap1);
+    GraphState *gs = ptr<GraphState>(c->gstate);
+    Particles ps = view(c);
+    Tree t = tree_view(c);
+    const int blocks = c->sms * 8;
+    k_g_prep<<<1, 1, 0, s>>>(gs, cap0, cap1, c->d_nbr_cap, n, walk_group_warps(), c->sms);
+    k_g_row_radius<<<blocks, 256, 0, s>>>(gs, ptr<int>(c->targets), ptr<int>(c->grow), ptr<double>(c->h),
+                                          kDensityBufferFirst, kDensityBuffer, ptr<double>(c->h_built));
+    walk_rows_graph(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), ptr<double>(c->h_built),
+                    ptr<int>(c->targets), ptr<int>(c->grow), gs, ptr<long long>(c->counts), ptr<int>(c->d_nbr),
+                    ptr<DevStatus>(c->status), s);
+    k_g_padded_rows<<<blocks, 256, 0, s>>>(gs, ptr<int>(c->targets), ptr<int>(c->grow), ptr<long long>(c->counts),
+                                           ptr<long long>(c->d_beg), ptr<long long>(c->d_end), ptr<int>(c->g_over_list),
+                                           ptr<long long>(c->g_over_off));
+    k_g_over_check<<<1, 1, 0, s>>>(gs, c->d_nbr_cap);
+    walk_over_graph(t, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), ptr<double>(c->h_built),
+                    ptr<int>(c->g_over_list), ptr<long long>(c->g_over_off), gs, ptr<int>(c->d_nbr),
+                    ptr<DevStatus>(c->status), c->sms * 4, s);
+    DensityWork w{};
+    w.beg = ptr<long long>(c->d_beg);
+    w.end = ptr<long long>(c->d_end);
+    w.nbr = ptr<int>(c->d_nbr);
+    w.rec = ptr<DensRec>(c->rec);
+    w.acc = ptr<double>(c->acc);
+    w.h_built = ptr<double>(c->h_built);
+    w.scratch = ptr<DensityScratch>(c->scratch);
+    w.h_iter_max = ptr<unsigned long long>(c->hmax);
+    w.keep = ptr<unsigned char>(c->keep);
+    w.regrow = ptr<unsigned char>(c->regrow);
+    density_sums_graph(c->pp, ps, w, gs, ptr<int>(c->todo_a), c->sms * 6, s);
+    density_after_iter_graph(c->pp, ps, w, ptr<DevStatus>(c->status), gs, ptr<int>(c->todo_a), c->sms * 16, s);
+    int *ca = ptr<int>(c->g_sel), *cb = ca + (n + kSelChunk - 1) / kSelChunk;
+    k_sel_count<<<c->sms * 2, kSelChunk, 0, s>>>(gs, ptr<unsigned char>(c->keep), ptr<unsigned char>(c->regrow), ca, cb);
+    k_sel_scan<<<1, kSelChunk, 0, s>>>(gs, ca, cb);
+    k_sel_write<<<c->sms * 2, kSelChunk, 0, s>>>(gs, ptr<int>(c->todo_a), ptr<unsigned char>(c->keep),
+                                                 ptr<unsigned char>(c->regrow), ca, cb, ptr<int>(c->todo_b),
+                                                 ptr<int>(c->grow));
+    k_g_next<<<c->sms * 4, 256, 0, s>>>(gs, ptr<int>(c->todo_b), ptr<int>(c->todo_a), loop);
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// The symmetric rows' counts and offsets, then (if they fit) the body that
+// builds them and runs gradients and force, returned in *body_gf.
+int capture_sym_rows(gz_context *c, cudaStream_t s, long long sym_cap, cudaGraph_t *body_gf)
+{
+    const int n = c->n;
+    const size_t N = (size_t)std::max(n, 1);
+    GZ_CUDA(c, cudaMemsetAsync(c->s_bcnt.p, 0, sizeof(int) * N, s));
+    sym_split(n, ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z), ptr<double>(c->h), c->prm.box_size,
+              ptr<long long>(c->d_beg), ptr<long long>(c->d_end), ptr<int>(c->d_nbr), ptr<int>(c->s_acnt),
+              ptr<int>(c->s_bcnt), s);
+    sym_counts(n, ptr<int>(c->s_acnt), ptr<int>(c->s_bcnt), ptr<long long>(c->s_counts), s);
+    GZ_CUDA(c, cudaMemsetAsync(c->s_off.p, 0, sizeof(long long), s));
+    size_t tmp = c->cub_tmp.bytes;
+    cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, ptr<long long>(c->s_counts), ptr<long long>(c->s_off) + 1, n, s);
+    GZ_CUDA(c, cudaGetLastError());
+    cudaGraphConditionalHandle h;
+    if (make_handle(c, s, &h, 0)) return c->err;
+    k_g_sym_check<<<1, 1, 0, s>>>(ptr<GraphState>(c->gstate), ptr<long long>(c->s_off) + n, sym_cap, h);
+    GZ_CUDA(c, cudaGetLastError());
+    return add_conditional(c, s, h, cudaGraphCondTypeIf, body_gf);
+}
+
+int capture_gradients_force(gz_context *c, cudaStream_t s, long long rq_cap)
+{
+    const int n = c->n;
+    const size_t N = (size_t)std::max(n, 1);
+    GZ_CUDA(c, cudaMemsetAsync(c->s_bcnt.p, 0, sizeof(int) * N, s));  // reused as the B cursors
+    sym_scatter(n, ptr<long long>(c->d_beg), ptr<int>(c->d_nbr), ptr<int>(c->s_acnt), ptr<long long>(c->s_off),
+                ptr<int>(c->s_bcnt), ptr<int>(c->s_tmp), s);
+    sym_sort(n, ptr<long long>(c->s_off), ptr<int>(c->s_acnt), ptr<int>(c->s_tmp), ptr<int>(c->s_nbr), s);
+    Csr rows{ptr<long long>(c->s_off), ptr<int>(c->s_nbr)};
+    Particles ps = view(c);
+    gradients_fp64(c->pp, ps, ptr<int>(c->targets), n, rows, lanes_per_row(c, n, 1), c->rec.p, nullptr, s);
+    if (c->have_bins) GZ_CUDA(c, cudaMemsetAsync(c->wakeup.p, 0, sizeof(int) * N, s));
+    force_preloop(c->pp, ps, ptr<int>(c->targets), n, s);
+    if (c->prm.precision == GZ_PRECISION_MIXED) {
+        GZ_CUDA(c, cudaMemsetAsync(c->refined.p, 0, sizeof(unsigned long long), s));
+        const RefineQueue q{ptr<RefineItem>(c->rq), ptr<unsigned long long>(c->refined), rq_cap};
+        force_mixed(c->pp, ps, ptr<int>(c->targets), n, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p,
+                    c->pflux.p, true, q, ptr<double>(c->acc), nullptr, s);
+    } else {
+        force_fp64(c->pp, ps, ptr<int>(c->targets), n, rows, c->tpt_force, ptr<DevStatus>(c->status), c->rec.p,
+                   c->pflux.p, true, ptr<double>(c->acc), nullptr, s);
+    }
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// Captures the pass into c->g (graph_buffers has sized everything it uses).
+int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
+{
+    graph_release(c);
+    for (auto &b : c->g.body)
+        if (!b) GZ_CUDA(c, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    const int n = c->n;
+    const size_t N = (size_t)n;
+    cudaStream_t s = c->stream;
+    cudaStream_t s1 = c->g.body[0], s2 = c->g.body[1];
+    Particles ps = view(c);
+    walk_group_warps();  // its occupancy query runs before the capture
+    GZ_CUDA(c, cudaGetLastError());
+    const long long launches0 = c->launches;
+    cudaGraph_t body_loop = nullptr, body_sym = nullptr, body_gf = nullptr;
+    cudaGraphConditionalHandle h_loop, h_conv;
+    int rc = 0;
+    cudaGraph_t g = nullptr;
+    GZ_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    c->g.capturing = true;
+    // the bodies are captured on their own streams into the nodes' graphs
+    auto body = [&](cudaStream_t bs, cudaGraph_t bg, auto &&fill) -> int {
+        if (cudaStreamBeginCaptureToGraph(bs, bg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            return fail(c, GZ_ERR_CUDA, "captured pass: cannot capture a body");
+        const int r = fill();
+        cudaGraph_t out = bg;
+        const cudaError_t e = cudaStreamEndCapture(bs, &out);
+        if (r) return r;
+        if (e != cudaSuccess) return fail(c, GZ_ERR_CUDA, cudaGetErrorString(e));
+        return 0;
+    };
+    do {
+        // the inputs a plain pass would restart from
+        cudaMemcpyAsync(c->g_hseed.p, c->h.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(c->g_cseed.p, c->cond.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
+        int na = 0;
+        if ((rc = sort_targets(c, nullptr, 0, &na))) break;
+        cudaMemsetAsync(c->hmax.p, 0, sizeof(unsigned long long), s);
+        k_density_prep<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->targets), ptr<double>(c->h),
+                                                       c->prm.max_kernel_radius, ptr<DensityScratch>(c->scratch),
+                                                       ptr<unsigned long long>(c->hmax));
+        cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * N, cudaMemcpyDeviceToDevice, s);
+        density_pack(ps, ptr<DensRec>(c->rec), s);
+        k_g_init<<<1, 1, 0, s>>>(ptr<GraphState>(c->gstate), n);
+        if ((rc = check_last(c, "density setup"))) break;
+        if ((rc = make_handle(c, s, &h_loop, 1))) break;
+        if ((rc = add_conditional(c, s, h_loop, cudaGraphCondTypeWhile, &body_loop))) break;
+        if ((rc = body(s1, body_loop, [&] { return capture_density_iteration(c, s1, h_loop); }))) break;
+        if ((rc = check_last(c, "density iteration"))) break;
+        density_finalize(c->pp, ps, ptr<double>(c->acc), ptr<int>(c->targets), n, s);
+        if ((rc = make_handle(c, s, &h_conv, 0))) break;
+        k_g_if_converged<<<1, 1, 0, s>>>(ptr<GraphState>(c->gstate), h_conv);
+        if ((rc = add_conditional(c, s, h_conv, cudaGraphCondTypeIf, &body_sym))) break;
+        rc = body(s1, body_sym, [&] {
+            int r = capture_sym_rows(c, s1, sym_cap, &body_gf);
+            if (!r) r = check_last(c, "symmetric rows");
+            if (r) return r;
+            r = body(s2, body_gf, [&] { return capture_gradients_force(c, s2, rq_cap); });
+            if (!r) r = check_last(c, "gradients and force");
+            return r;
+        });
+        if (rc) break;
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(c, GZ_ERR_CUDA, "captured pass: a launch failed"); break; }
+    } while (0);
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    c->g.capturing = false;
+    c->launches = launches0;
+    if (!rc && e != cudaSuccess) rc = fail(c, GZ_ERR_CUDA, cudaGetErrorString(e));
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc;
+    }
+    c->g.graph = g;
+    if (check_last(c, "end of capture")) { graph_release(c); return c->err; }
+    // this library's kernels in each part (the key sort and scans are CUB's):
+    // setup (targets, active flags, prep, pack, state) + finalize + the
+    // convergence test; per iteration prep, radii, two walk modes, padded
+    // rows, overflow check, overflow walk, three sums instances, after_iter,
+    // the selection's three steps, next; the rows' split, counts and check;
+    // scatter, sort, the gradient pack and rows, the force preloop, pack,
+    // pairs, (refine,) gather, finish
+    c->g.kernels_top = 7;
+    c->g.kernels_loop = 15;
+    c->g.kernels_sym = 3;
+    c->g.kernels_tail = c->prm.precision == GZ_PRECISION_MIXED ? 10 : 9;
+    (void)body_loop;
+    const cudaError_t ie = cudaGraphInstantiate(&c->g.exec, g, 0);
+    if (ie != cudaSuccess) {
+        char b[200];
+        snprintf(b, sizeof(b), "captured pass: cannot instantiate the graph: %s", cudaGetErrorString(ie));
+        cudaGetLastError();
+        graph_release(c);
+        return fail(c, GZ_ERR_CUDA, b);
+    }
+    if (check_last(c, "instantiation")) { graph_release(c); return c->err; }
+    c->g.rq_cap = rq_cap;
+    c->g.captures++;
+    return 0;
+}
+
+// One replay of the captured pass; a buffer overflow (or more fragile pairs
+// than the refine queue holds) is answered by the plain pass from the
+// graph's starting kernel lengths and condition numbers.
+int graph_pass(gz_context *c)
+{
+    cudaStream_t s = c->stream;
+    const int n = c->n;
+    long long sym_cap = 0, rq_cap = 0;
+    const int room = graph_buffers(c, &sym_cap, &rq_cap);
+    if (room == kNoRoom) {  // no room for the graph's buffers: the plain pass
+        int rc = gz_hydro_density(c, nullptr, 0);
+        if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
+        if (!rc) rc = gz_hydro_force(c, nullptr, 0);
+        return rc;
+    }
+    if (room) return room;
+    std::vector<unsigned long long> sig = graph_signature(c);
+    if (!c->g.exec || sig != c->g.sig) {
+        if (graph_capture(c, sym_cap, rq_cap)) return c->err;
+        c->g.sig = sig;
+    }
+    if (check_last(c, "before the launch")) return c->err;
+    GZ_CUDA(c, cudaGraphLaunch(c->g.exec, s));
+    GraphState gs{};
+    unsigned long long refined = 0, hbits = 0;
+    const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
+    GZ_CUDA(c, cudaMemcpyAsync(&gs, c->gstate.p, sizeof(gs), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaMemcpyAsync(&hbits, c->hmax.p, sizeof(hbits), cudaMemcpyDeviceToHost, s));
+    if (mixed) GZ_CUDA(c, cudaMemcpyAsync(&refined, c->refined.p, sizeof(refined), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    if (check_last(c, "graph launch")) return c->err;
+    c->g.replays++;
+    const bool converged = gs.todo_left == 0 && !gs.fail;
+    c->launches += c->g.kernels_top + c->g.kernels_loop * gs.iter + (converged ? c->g.kernels_sym : 0) +
+                   ((converged && !(gs.fail & kGraphFailSym)) ? c->g.kernels_tail : 0);
+    if (gs.fail || (long long)refined > c->g.rq_cap) {
+        c->g.fallbacks++;
+        GZ_CUDA(c, cudaMemcpyAsync(c->h.p, c->g_hseed.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        GZ_CUDA(c, cudaMemcpyAsync(c->cond.p, c->g_cseed.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        int rc = gz_hydro_density(c, nullptr, 0);
+        if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
+        if (!rc) rc = gz_hydro_force(c, nullptr, 0);
+        return rc;
+    }
+    c->last_iters = gs.iter;
+    c->d_used = gs.base;
+    memcpy(&c->h_iter_max, &hbits, sizeof(double));
+    c->pairs_density = gs.entries;
+    if (read_status(c)) return c->err;
+    if (gs.todo_left > 0) return fail(c, GZ_ERR_DENSITY_MAXITER, "density did not converge in MAXITER iterations");
+    c->have_density = true;
+    c->dens_all = false;  // the symmetric rows consumed the density rows
+    c->pairs_symmetric = gs.sym_total;
+    c->sym_rows = n;
+    c->sym_valid = true;
+    c->sym_all = true;
+    c->sym_active.clear();
+    c->have_gradients = true;
+    c->fabs_valid = c->pp.diag_flux_abs != 0;
+    c->pairs_refined = (long long)refined;
+    return GZ_OK;
+}
+
 }  // namespace
 
 // ===================================================================== ABI
@@ -779,6 +1416,9 @@ int gz_destroy(gz_context *c)
     if (!c) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    graph_release(c);
+    for (auto &b : c->g.body)
+        if (b) cudaStreamDestroy(b);
     for (DevBuf *b : all_buffers(c)) release(*b);
     for (auto &t : c->timers)
         for (auto &e : t.ev) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
@@ -1098,7 +1738,7 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     // at 256^3), and FP64 gradients make the mixed form's force inputs the FP64
     // form's exactly (FP32 terms left 9 of 16.8M particles above 1e-5).
     gradients_fp64(c->pp, ps, ptr<int>(c->targets), na, rows, lanes_per_row(c, na, 1), c->rec.p, ev, c->stream);
-    if (na > 0) c->launches++;
+    if (na > 0) c->launches += 2;  // the record pack and the rows
     GZ_CUDA(c, cudaGetLastError());
     if (read_status(c)) return c->err;
     c->have_gradients = true;
@@ -1176,6 +1816,34 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     }
     if (read_status(c)) return c->err;
     c->pairs_refined = (long long)refined;
+    return GZ_OK;
+}
+
+int gz_hydro_pass(gz_context *c, int flags)
+{
+    if (!c || (flags & ~GZ_PASS_GRAPH)) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "pass before upload");
+    // the graph needs the counts of a plain pass to size its buffers, and the
+    // kernel timers need plain launches
+    const bool graph = (flags & GZ_PASS_GRAPH) && c->n > 0 && c->pairs_symmetric > 0 && !c->timing;
+    if (graph) return graph_pass(c);
+    int rc = gz_hydro_density(c, nullptr, 0);
+    if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
+    if (!rc) rc = gz_hydro_force(c, nullptr, 0);
+    return rc;
+}
+
+int gz_graph_stats(gz_context *c, gz_graph_info *out)
+{
+    if (!c || !out) return GZ_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    out->captures = c->g.captures;
+    out->replays = c->g.replays;
+    out->fallbacks = c->g.fallbacks;
+    out->kernels_top = c->g.kernels_top;
+    out->kernels_per_iteration = c->g.kernels_loop;
+    out->kernels_after = c->g.kernels_sym + c->g.kernels_tail;
     return GZ_OK;
 }
 

@@ -457,11 +457,11 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
 // or one target in SOLO mode) from a counter until none is left, so warps
 // that draw a group on both sides of a Morton jump do not hold up a wave.
 template <bool SYM, bool FILL, bool SOLO>
-__global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
-                                              const double *__restrict__ z, const double *__restrict__ reach,
-                                              const double *__restrict__ hsym, const int *__restrict__ targets,
-                                              int n_targets, long long *counts, const long long *__restrict__ off,
-                                              int *nbr, int cap, DevStatus *st, int *next_group)
+__device__ __forceinline__ void walk_groups(const Tree &t, const double *__restrict__ x, const double *__restrict__ y,
+                                            const double *__restrict__ z, const double *__restrict__ reach,
+                                            const double *__restrict__ hsym, const int *__restrict__ targets,
+                                            int n_targets, long long *counts, const long long *__restrict__ off,
+                                            int *nbr, int cap, DevStatus *st, int *next_group)
 {
     __shared__ StackNode s_stack[kWarps][kStack];
     __shared__ double4 s_c[kWarps][32];
@@ -479,6 +479,43 @@ __global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__
                                     s_c, s_cf, s_lo, s_hi, s_nd);
         __syncwarp();
     }
+}
+
+template <bool SYM, bool FILL, bool SOLO>
+__global__ void __launch_bounds__(256) k_walk(Tree t, const double *__restrict__ x, const double *__restrict__ y,
+                                              const double *__restrict__ z, const double *__restrict__ reach,
+                                              const double *__restrict__ hsym, const int *__restrict__ targets,
+                                              int n_targets, long long *counts, const long long *__restrict__ off,
+                                              int *nbr, int cap, DevStatus *st, int *next_group)
+{
+    walk_groups<SYM, FILL, SOLO>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, next_group);
+}
+
+// The padded density-row fill of a captured pass: the rows of this iteration
+// (every target at iteration 0, the regrow list afterwards), their number,
+// slots and place in the row buffer come from the device state; the instance
+// of the state's walk mode runs (both modes write the same rows).
+template <bool SOLO>
+__global__ void __launch_bounds__(256) k_walk_graph(Tree t, const double *__restrict__ x, const double *__restrict__ y,
+                                                    const double *__restrict__ z, const double *__restrict__ reach,
+                                                    const int *__restrict__ first, const int *__restrict__ grow,
+                                                    GraphState *gs, long long *counts, int *nbr, DevStatus *st)
+{
+    if (gs->fail || gs->walk_solo != (int)SOLO || gs->n_grow == 0) return;
+    walk_groups<false, true, SOLO>(t, x, y, z, reach, reach, gs->iter == 0 ? first : grow, gs->n_grow, counts,
+                                   nullptr, nbr + gs->base, gs->cap, st, &gs->next_group[0]);
+}
+
+// The rows longer than their slots, at their exact offsets behind the block.
+__global__ void __launch_bounds__(256) k_walk_graph_over(Tree t, const double *__restrict__ x,
+                                                         const double *__restrict__ y, const double *__restrict__ z,
+                                                         const double *__restrict__ reach, const int *__restrict__ list,
+                                                         const long long *__restrict__ off, GraphState *gs, int *nbr,
+                                                         DevStatus *st)
+{
+    if (gs->fail || gs->n_over == 0) return;
+    walk_groups<false, true, true>(t, x, y, z, reach, reach, list, gs->n_over, nullptr, off, nbr + gs->need, 0, st,
+                                   &gs->next_group[1]);
 }
 
 // ------------------------------------------------ symmetric rows from density rows
@@ -696,18 +733,11 @@ static void launch_walk(const Tree &t, const double *x, const double *y, const d
                                                             nbr, cap, st, next_group);
 }
 
-void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
-               const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
-               const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
+// Warps the group-mode walk holds resident on the current device (looked up
+// once per device; concurrent first calls store the same value).
+long long walk_group_warps()
 {
-    if (n_targets <= 0) return;
-    // Group mode (32 targets per warp) for dense lists and for lists whose
-    // groups fill the warps the GPU holds resident: its traversal tests 32
-    // targets per ballot where the one-target mode tests one. A short sparse
-    // list (the rows rebuilt after an h regrowth, scattered through the box)
-    // gets one warp per target instead: as groups it would run on a few
-    // warps, each walking 32 unrelated regions one after another.
-    static std::atomic<long long> group_warps_of[kMaxWalkDevices];  // per device, as in launch_walk
+    static std::atomic<long long> group_warps_of[kMaxWalkDevices];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= kMaxWalkDevices) dev = 0;
@@ -719,6 +749,21 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
         group_warps = (long long)(sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarps;
         group_warps_of[dev].store(group_warps, std::memory_order_relaxed);
     }
+    return group_warps;
+}
+
+void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+               const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
+               const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s)
+{
+    if (n_targets <= 0) return;
+    // Group mode (32 targets per warp) for dense lists and for lists whose
+    // groups fill the warps the GPU holds resident: its traversal tests 32
+    // targets per ballot where the one-target mode tests one. A short sparse
+    // list (the rows rebuilt after an h regrowth, scattered through the box)
+    // gets one warp per target instead: as groups it would run on a few
+    // warps, each walking 32 unrelated regions one after another.
+    const long long group_warps = walk_group_warps();
     const bool sparse = (long long)n_targets * 4 < (long long)t.n_particles;
     const bool solo = n_targets == 1 || (sparse && (n_targets + 31) / 32 < group_warps);
 #define GZ_WALK(S, F, O) launch_walk<S, F, O>(t, x, y, z, reach, hsym, targets, n_targets, counts, off, nbr, cap, st, next_group, s)
@@ -730,6 +775,37 @@ void walk_rows(const Tree &t, const double *x, const double *y, const double *z,
         else { if (nbr) GZ_WALK(false, true, false); else GZ_WALK(false, false, false); }
     }
 #undef GZ_WALK
+}
+
+void walk_rows_graph(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                     const int *first, const int *grow, GraphState *gs, long long *counts, int *nbr, DevStatus *st,
+                     cudaStream_t s)
+{
+    static std::atomic<int> resident_of[kMaxWalkDevices][2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxWalkDevices) dev = 0;
+    int res[2];
+    for (int m = 0; m < 2; m++) {
+        res[m] = resident_of[dev][m].load(std::memory_order_relaxed);
+        if (res[m] == 0) {
+            int sms = 0, per_sm = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (m == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_graph<false>, 32 * kWarps, 0);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_graph<true>, 32 * kWarps, 0);
+            res[m] = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+            resident_of[dev][m].store(res[m], std::memory_order_relaxed);
+        }
+    }
+    k_walk_graph<false><<<res[0], 32 * kWarps, 0, s>>>(t, x, y, z, reach, first, grow, gs, counts, nbr, st);
+    k_walk_graph<true><<<res[1], 32 * kWarps, 0, s>>>(t, x, y, z, reach, first, grow, gs, counts, nbr, st);
+}
+
+void walk_over_graph(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                     const int *list, const long long *off, GraphState *gs, int *nbr, DevStatus *st, int blocks,
+                     cudaStream_t s)
+{
+    k_walk_graph_over<<<blocks, 32 * kWarps, 0, s>>>(t, x, y, z, reach, list, off, gs, nbr, st);
 }
 
 }  // namespace gz

@@ -19,6 +19,17 @@ void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, 
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
                const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s);
+// The padded density-row fill of a captured pass (both walk modes launched;
+// the state names the one that runs) and the fill of its overflow rows.
+void walk_rows_graph(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                     const int *first, const int *grow, GraphState *gs, long long *counts, int *nbr, DevStatus *st,
+                     cudaStream_t s);
+// warps the group-mode walk holds resident (the walk takes one warp per
+// target when a sparse list's groups would not fill them)
+long long walk_group_warps();
+void walk_over_graph(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
+                     const int *list, const long long *off, GraphState *gs, int *nbr, DevStatus *st, int blocks,
+                     cudaStream_t s);
 // rows of a padded fill (cap > 0 above): [beg, end) for the rows that fit, over[a] = 1 for the others
 void padded_rows(int na, const int *t, const long long *counts, int cap, long long base, long long *beg,
                  long long *end, unsigned char *over, cudaStream_t s);
@@ -58,6 +69,13 @@ void density_pack(const Particles &ps, DensRec *rec, cudaStream_t s);
 void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
 void density_sums_mixed(const PassParams &p, const Particles &ps, const DensityWork &w, int tpt, cudaStream_t s);
 void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s);
+// Captured-pass forms (GraphState): every TPT instance is launched with `blocks`
+// blocks and the one the device state names runs; after_iter writes the
+// per-slot flags of w.keep and w.regrow for the iteration's target count.
+void density_sums_graph(const PassParams &p, const Particles &ps, const DensityWork &w, GraphState *gs,
+                        const int *todo, int blocks, cudaStream_t s);
+void density_after_iter_graph(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st,
+                              GraphState *gs, const int *todo, int blocks, cudaStream_t s);
 void density_finalize(const PassParams &p, const Particles &ps, const double *acc, const int *targets, int n_targets,
                       cudaStream_t s);
 // `rec` is scratch for the packed neighbour records: at least n x

@@ -63,14 +63,12 @@ GZ_DEV DensRec load_dens_rec(const DensRec *__restrict__ rec, int j)
     return r;
 }
 
+// The sums of target t's density row, by the TPT lanes (`lane` of them, on
+// `mask`) that own it; lane 0 stores them.
 template <typename T, int TPT>
-__global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p, Particles ps, DensityWork w)
+GZ_DEV void density_row(const PassParams &p, const Particles &ps, const DensityWork &w, int t, int lane,
+                        unsigned mask)
 {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = gtid / TPT, lane = gtid % TPT;
-    if (slot >= w.n_todo) return;
-    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
-    const int t = w.todo[slot];
     const double xi = ps.x[t], yi = ps.y[t], zi = ps.z[t];
     const double hd = ps.h[t];
     const double h2 = hd * hd;
@@ -145,6 +143,46 @@ __global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p,
         const size_t n = (size_t)ps.n;
 #pragma unroll
         for (int k = 0; k < 17; k++) w.acc[k * n + t] = a[k];
+    }
+}
+
+template <typename T, int TPT>
+__global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums(PassParams p, Particles ps, DensityWork w)
+{
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = gtid / TPT, lane = gtid % TPT;
+    if (slot >= w.n_todo) return;
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
+    density_row<T, TPT>(p, ps, w, w.todo[slot], lane, mask);
+}
+
+// The same rows for a captured pass: the iteration's target count and lane
+// count come from the device state. A fixed number of blocks stand in for the
+// plain launch's grid: each takes the next block-sized chunk of rows (the
+// plain grid's next block) from a counter, so the rows in flight are a
+// contiguous run of the list and the chunks go to whichever block is free, as
+// the hardware hands out the blocks of a plain launch. An instance whose TPT
+// is not the iteration's returns at once. Each row is summed by the same
+// lanes in the same order as k_density_sums sums it.
+template <typename T, int TPT>
+__global__ void __launch_bounds__(kDensityBlock, 6) k_density_sums_graph(PassParams p, Particles ps, DensityWork w,
+                                                                         GraphState *gs,
+                                                                         const int *__restrict__ todo)
+{
+    __shared__ int s_chunk;
+    if (gs->fail || gs->tpt != TPT) return;
+    const int n_todo = gs->n_todo;
+    constexpr int kRows = kDensityBlock / TPT;
+    const unsigned mask = (TPT == 32) ? 0xffffffffu : (((1u << TPT) - 1u) << ((threadIdx.x & 31) & ~(TPT - 1)));
+    const int lane = threadIdx.x % TPT;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(&gs->sums_next, 1);
+        __syncthreads();
+        const int chunk = s_chunk;
+        __syncthreads();  // read by every thread before the next draw
+        if ((long long)chunk * kRows >= n_todo) break;
+        const int slot = chunk * kRows + (int)threadIdx.x / TPT;
+        if (slot < n_todo) density_row<T, TPT>(p, ps, w, todo[slot], lane, mask);
     }
 }
 

@@ -36,6 +36,14 @@ void density_sums_fp64(const PassParams &p, const Particles &ps, const DensityWo
     launch_density_sums<double>(p, ps, w, tpt, s);
 }
 
+void density_sums_graph(const PassParams &p, const Particles &ps, const DensityWork &w, GraphState *gs,
+                        const int *todo, int blocks, cudaStream_t s)
+{
+    k_density_sums_graph<double, 4><<<blocks, kDensityBlock, 0, s>>>(p, ps, w, gs, todo);
+    k_density_sums_graph<double, 8><<<blocks, kDensityBlock, 0, s>>>(p, ps, w, gs, todo);
+    k_density_sums_graph<double, 16><<<blocks, kDensityBlock, 0, s>>>(p, ps, w, gs, todo);
+}
+
 void gradients_fp64(const PassParams &p, const Particles &ps, const int *targets, int n_targets, Csr rows, int tpt,
                     void *rec, const EventPair *ev, cudaStream_t s)
 {
@@ -99,42 +107,90 @@ void force_refine(const PassParams &p, const Particles &ps, const RefineQueue &q
     k_force_refine<<<sms * 4, 128, 0, s>>>(p, ps, q, flux, st);
 }
 
-// DensitySpec::after_iter_body per iterating particle, plus the runner's
-// radius update and compaction flag (neighbor_loop_runner.cc:7340-7372).
+// DensitySpec::after_iter_body for one target of iteration `iter`, plus the
+// runner's radius update (neighbor_loop_runner.cc:7340-7372): returns whether
+// it still iterates, sets `regrow` when its new radius outgrew its row and
+// `moved` to that radius.
+GZ_DEV bool after_iter_target(const PassParams &p, const Particles &ps, const DensityWork &w, int iter, int t,
+                              DevStatus *st, bool &regrow, double &moved)
+{
+    const size_t n = (size_t)ps.n;
+    double acc[14];
+    for (int k = 0; k < 14; k++) acc[k] = w.acc[k * n + t];
+    const double h = ps.h[t];
+    DensityScratch sc = w.scratch[t];
+    double nh = h;
+    int stop = 0;
+    const int conv = after_iter(p, iter, h, acc, ps.cond[t], sc, nh, stop);
+    w.scratch[t] = sc;
+    ps.iters[t] = iter + 1;
+    if (stop) record_status(st, stop, t);
+    regrow = false;
+    if (!conv) {
+        ps.h[t] = nh;
+        moved = nh;
+        regrow = nh > w.h_built[t];
+    }
+    return !conv;
+}
+
+// after_iter per iterating particle, with the compaction flags
+// (neighbor_loop_runner.cc:7340-7372).
 __global__ void k_after_iter(PassParams p, Particles ps, DensityWork w, DevStatus *st)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double moved = 0;  // the radius this particle moves to (0: none), for the iteration's largest
     if (s < w.n_todo) {
-        const int t = w.todo[s];
-        const size_t n = (size_t)ps.n;
-        double acc[14];
-        for (int k = 0; k < 14; k++) acc[k] = w.acc[k * n + t];
-        const double h = ps.h[t];
-        DensityScratch sc = w.scratch[t];
-        double nh = h;
-        int stop = 0;
-        const int conv = after_iter(p, w.iter, h, acc, ps.cond[t], sc, nh, stop);
-        w.scratch[t] = sc;
-        ps.iters[t] = w.iter + 1;
-        if (stop) record_status(st, stop, t);
-        int regrow = 0;
-        if (!conv) {
-            ps.h[t] = nh;
-            moved = nh;
-            regrow = nh > w.h_built[t];
-            if (regrow) atomicExch(w.rebuild, 1);
-        }
-        w.keep[s] = conv ? 0 : 1;
+        bool regrow = false;
+        const bool keep = after_iter_target(p, ps, w, w.iter, w.todo[s], st, regrow, moved);
+        if (regrow) atomicExch(w.rebuild, 1);
+        w.keep[s] = keep ? 1 : 0;
         w.regrow[s] = (unsigned char)regrow;
     }
     if (w.h_iter_max) warp_atomic_max_nonneg(w.h_iter_max, moved);  // every lane of the block
+}
+
+// after_iter for a captured pass: the iteration and its target count come
+// from the device state; the flags (still iterating, radius outgrew its row)
+// are per slot, as k_after_iter writes them, for the compaction that follows.
+// Blocks take block-sized chunks of the list from a counter, in order, as
+// the hardware hands out the blocks of the plain launch.
+__global__ void __launch_bounds__(128) k_after_iter_graph(PassParams p, Particles ps, DensityWork w, DevStatus *st,
+                                                          GraphState *gs, const int *__restrict__ todo)
+{
+    __shared__ int s_chunk;
+    if (gs->fail) return;
+    const int iter = gs->iter, n_todo = gs->n_todo;
+    double moved = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(&gs->after_next, 1);
+        __syncthreads();
+        const int chunk = s_chunk;
+        __syncthreads();
+        if ((long long)chunk * blockDim.x >= n_todo) break;
+        const int s = chunk * blockDim.x + threadIdx.x;
+        if (s < n_todo) {
+            bool regrow = false;
+            double mv = 0;
+            const bool keep = after_iter_target(p, ps, w, iter, todo[s], st, regrow, mv);
+            moved = fmax(moved, mv);
+            w.keep[s] = keep ? 1 : 0;
+            w.regrow[s] = (unsigned char)regrow;
+        }
+    }
+    if (w.h_iter_max) warp_atomic_max_nonneg(w.h_iter_max, moved);
 }
 
 void density_after_iter(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st, cudaStream_t s)
 {
     if (w.n_todo <= 0) return;
     k_after_iter<<<(w.n_todo + 127) / 128, 128, 0, s>>>(p, ps, w, st);
+}
+
+void density_after_iter_graph(const PassParams &p, const Particles &ps, const DensityWork &w, DevStatus *st,
+                              GraphState *gs, const int *todo, int blocks, cudaStream_t s)
+{
+    k_after_iter_graph<<<blocks, 128, 0, s>>>(p, ps, w, st, gs, todo);
 }
 
 // density_finalize_post_runner (density_loop.cc:303-733), gas, non-SPH.

@@ -101,4 +101,28 @@ struct Csr {
     const int *nbr;                 // sorted particle indices
 };
 
+// The density iteration's control state on the device, for a pass captured as
+// one CUDA graph (no host round trip between iterations). Each iteration takes
+// its targets from one list and selects, in list order, the ones still
+// iterating into the next and those whose radius outgrew their row into the
+// regrow list; the rows rebuilt are those of every target in the first
+// iteration and of the regrow list afterwards. `fail` stops the graph's work
+// where a device-sized buffer would overflow (the host then runs the pass
+// without the graph).
+struct GraphState {
+    int n_todo, n_grow, iter, fail;
+    int n_next, n_regrow, n_over, tpt;  // this iteration's selections, padded-row overflows, density lanes
+    int cap, walk_solo, next_group[2];  // padded slots, walk mode, walk work counters
+    long long base, need, extra;        // padded entries in use, after this iteration's block, overflow room
+    long long entries;                  // density row entries built (the pass's pairs_density)
+    long long sym_total;                // symmetric row entries
+    int todo_left;                      // after the loop: targets still iterating (MAXITER reached)
+    int sums_next, after_next;          // the density sums' and after_iter's next chunk of the list
+    int pad;
+};
+
+// Fail reasons (GraphState::fail, bit flags).
+constexpr int kGraphFailRows = 1;   // padded density rows beyond the row buffer
+constexpr int kGraphFailSym = 2;    // symmetric rows beyond their buffers or the pair-flux buffer
+
 }  // namespace gz

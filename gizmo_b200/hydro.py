@@ -197,6 +197,17 @@ class HydroPass:
         self.hydro_gradient_calc(active)
         self.hydro_force(active)
 
+    def hydro_pass(self, graph: bool = True):
+        """density -> gradients -> force over every particle in one call
+        (gz_hydro_pass); with graph=True as one CUDA graph once a plain pass
+        has sized its buffers. Results equal full_pass()'s."""
+        self._check(self.lib.gz_hydro_pass(self._ctx, abi.PASS_GRAPH if graph else 0))
+
+    def graph_stats(self) -> dict:
+        g = abi.GzGraphInfo()
+        self._check(self.lib.gz_graph_stats(self._ctx, C.byref(g)))
+        return {k: int(getattr(g, k)) for k, _ in abi.GzGraphInfo._fields_}
+
     # -- walk tuning ------------------------------------------------------------
     def tuning(self) -> dict:
         t = abi.GzTuning()

@@ -181,6 +181,29 @@ int gz_hydro_density(gz_context *ctx, const int *active, int n_active);
 int gz_hydro_gradients(gz_context *ctx, const int *active, int n_active);
 int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
 
+/* The three passes over every particle in one call (compute_hydro_densities_
+ * and_forces, src/core/accel.cc:80-169, with all gas active). With
+ * GZ_PASS_GRAPH the pass runs as one CUDA graph with no host round trip: the
+ * density iteration as a device-driven loop, then the symmetric rows, gradients
+ * and force. The graph is captured at the first such call after a plain pass
+ * has sized its buffers (the first call runs plain) and replayed while the
+ * context's buffers and settings are unchanged (a gz_restage keeps them); its
+ * results equal the three calls' bit for bit. Where a device-sized buffer
+ * would overflow, the call runs the plain pass from the same inputs
+ * (gz_graph_stats counts those). Kernel timing (gz_kernel_timing) runs plain. */
+#define GZ_PASS_GRAPH 1
+int gz_hydro_pass(gz_context *ctx, int flags);
+
+typedef struct gz_graph_info {
+    int64_t captures;               /* graphs captured (a change of buffers or settings captures again) */
+    int64_t replays;                /* passes run through a graph */
+    int64_t fallbacks;              /* ... of which ran again as plain passes */
+    int64_t kernels_top;            /* kernels of one replay outside the conditional bodies */
+    int64_t kernels_per_iteration;  /* kernels of one density iteration */
+    int64_t kernels_after;          /* kernels of the symmetric rows, gradients and force */
+} gz_graph_info;
+int gz_graph_stats(gz_context *ctx, gz_graph_info *out);
+
 /* Copy outputs device -> host (original order). */
 int gz_download(gz_context *ctx, const gz_outputs *out);
 

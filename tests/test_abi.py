@@ -62,7 +62,7 @@ int main(void) {
                                           ("gz_outputs", abi.GzOutputs), ("gz_status_info", abi.GzStatusInfo),
                                           ("gz_timestep_params", abi.GzTimestepParams),
                                           ("gz_timestep_fields", abi.GzTimestepFields),
-                                          ("gz_tuning", abi.GzTuning)])
+                                          ("gz_tuning", abi.GzTuning), ("gz_graph_info", abi.GzGraphInfo)])
 def test_device_field_structs_match_c_field_by_field(tmp_path, cname, mirror):
     """Every field of the ctypes mirror sits at the C offset of the field of the same name: two
     pointer fields in swapped order would keep the size and hand the kernel the wrong arrays."""
