@@ -112,6 +112,13 @@ struct gz_context {
         bool capturing = false;                     // no timer events while a graph is captured
     } g;
     DevBuf gstate, g_hseed, g_cseed, g_over_list, g_over_off, g_sel;
+    // pipelined transfers (gz_upload_async / gz_download_async): the inputs of
+    // the next step land in p_* while a step runs; the outputs of a step leave
+    // from dstage while the next one runs
+    DevBuf p_stage3, p_vel, p_mass, p_u, p_dt, p_h, p_cond, dstage;
+    cudaStream_t cstream = nullptr;  // the copy stream
+    cudaEvent_t ev_in_free = nullptr, ev_in_done = nullptr, ev_out_ready = nullptr, ev_out_done = nullptr;
+    bool in_pending = false, out_pending = false;
 };
 
 namespace {
@@ -280,7 +287,8 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->d_beg, &c->d_end, &c->flag, &c->counts, &c->d_off, &c->d_nbr, &c->n_sel, &c->s_off, &c->s_nbr,
             &c->s_counts, &c->rec, &c->work, &c->hmax, &c->refined, &c->rq, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl, &c->o_timebin,
             &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out,
-            &c->gstate, &c->g_hseed, &c->g_cseed, &c->g_over_list, &c->g_over_off, &c->g_sel};
+            &c->gstate, &c->g_hseed, &c->g_cseed, &c->g_over_list, &c->g_over_off, &c->g_sel,
+            &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond, &c->dstage};
 }
 
 Tree tree_view(gz_context *c)
@@ -596,6 +604,33 @@ int build_rows_padded(gz_context *c, const double *reach, const int *targets, in
     }
     *used = need + extra;
     *entries = built;
+    return 0;
+}
+
+// the copy stream and events of the pipelined transfers, made on first use
+int copy_stream(gz_context *c)
+{
+    if (c->cstream) return 0;
+    GZ_CUDA(c, cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+    cudaEvent_t *ev[] = {&c->ev_in_free, &c->ev_in_done, &c->ev_out_ready, &c->ev_out_done};
+    for (cudaEvent_t *e : ev) GZ_CUDA(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return 0;
+}
+
+// inputs of a pipelined upload become the resident ones: the context's stream
+// waits for their copies, and the buffers trade places (no copy)
+int take_pending_inputs(gz_context *c)
+{
+    if (!c->in_pending) return 0;
+    GZ_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in_done, 0));
+    std::swap(c->stage3, c->p_stage3);
+    std::swap(c->o_vel, c->p_vel);
+    std::swap(c->o_mass, c->p_mass);
+    std::swap(c->o_u, c->p_u);
+    std::swap(c->o_dt, c->p_dt);
+    std::swap(c->o_h, c->p_h);
+    std::swap(c->o_cond, c->p_cond);
+    c->in_pending = false;
     return 0;
 }
 
@@ -1056,8 +1091,18 @@ int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap)
 // particle count, the pass settings
 std::vector<unsigned long long> graph_signature(gz_context *c)
 {
+    // the resident inputs, their pipelined copies and the download staging are
+    // read by the restage and the downloads only, never by the graph (and the
+    // pipelined upload swaps them every step)
+    const DevBuf *outside[] = {&c->stage3, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond,
+                               &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond,
+                               &c->dstage, &c->dl};
     std::vector<unsigned long long> v;
-    for (DevBuf *b : all_buffers(c)) { v.push_back((unsigned long long)(uintptr_t)b->p); v.push_back(b->bytes); }
+    for (DevBuf *b : all_buffers(c)) {
+        if (std::find(std::begin(outside), std::end(outside), b) != std::end(outside)) continue;
+        v.push_back((unsigned long long)(uintptr_t)b->p);
+        v.push_back(b->bytes);
+    }
     v.push_back((unsigned long long)c->n);
     const unsigned char *pp = (const unsigned char *)&c->pp;
     for (size_t k = 0; k < sizeof(PassParams); k++) v.push_back(pp[k]);
@@ -1419,6 +1464,11 @@ int gz_destroy(gz_context *c)
     graph_release(c);
     for (auto &b : c->g.body)
         if (b) cudaStreamDestroy(b);
+    if (c->cstream) {
+        cudaStreamSynchronize(c->cstream);
+        cudaStreamDestroy(c->cstream);
+        for (cudaEvent_t e : {c->ev_in_free, c->ev_in_done, c->ev_out_ready, c->ev_out_done}) cudaEventDestroy(e);
+    }
     for (DevBuf *b : all_buffers(c)) release(*b);
     for (auto &t : c->timers)
         for (auto &e : t.ev) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
@@ -1536,6 +1586,7 @@ static int upload_from(gz_context *c, const gz_particles *in, cudaMemcpyKind kin
     if (!c || !in || in->n < 0 || in->n > INT32_MAX / 16) return GZ_ERR_ARG;
     if (in->n > 0 && (!in->pos || !in->vel || !in->mass || !in->u || !in->dt || !in->h)) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
+    c->in_pending = false;  // a pipelined upload not yet restaged is superseded
     const int n = (int)in->n;
     c->n = n;
     cudaStream_t s = c->stream;
@@ -1599,7 +1650,55 @@ int gz_restage(gz_context *c)
     if (!c) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     if (!c->grid_valid && c->n > 0) return fail(c, GZ_ERR_ORDER, "restage before upload");
+    if (take_pending_inputs(c)) return c->err;
     if (stage_inputs(c)) return c->err;
+    return GZ_OK;
+}
+
+int gz_upload_async(gz_context *c, const gz_particles *in)
+{
+    if (!c || !in) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    // a new size, timebins, or no set yet: the synchronous upload
+    if (!c->grid_valid || in->n != c->n || in->timebin || c->n == 0) return upload_from(c, in, cudaMemcpyHostToDevice);
+    if (!in->pos || !in->vel || !in->mass || !in->u || !in->dt || !in->h) return GZ_ERR_ARG;
+    if (copy_stream(c)) return c->err;
+    if (take_pending_inputs(c)) return c->err;  // an upload not yet restaged is taken now
+    const size_t N = (size_t)c->n;
+    if (ensure(c, c->p_stage3, sizeof(double) * 3 * N) || ensure(c, c->p_vel, sizeof(double) * 3 * N) ||
+        ensure(c, c->p_mass, sizeof(double) * N) || ensure(c, c->p_u, sizeof(double) * N) ||
+        ensure(c, c->p_dt, sizeof(double) * N) || ensure(c, c->p_h, sizeof(double) * N) ||
+        ensure(c, c->p_cond, sizeof(double) * N))
+        return c->err;
+    // the copies wait for the work queued so far (it may read these buffers'
+    // previous contents), then run beside the next pass
+    GZ_CUDA(c, cudaEventRecord(c->ev_in_free, c->stream));
+    GZ_CUDA(c, cudaStreamWaitEvent(c->cstream, c->ev_in_free, 0));
+    const cudaMemcpyKind k = cudaMemcpyHostToDevice;
+    GZ_CUDA(c, cudaMemcpyAsync(c->p_stage3.p, in->pos, sizeof(double) * 3 * N, k, c->cstream));
+    GZ_CUDA(c, cudaMemcpyAsync(c->p_vel.p, in->vel, sizeof(double) * 3 * N, k, c->cstream));
+    struct { const double *src; DevBuf *dst; } f1[] = {
+        {in->mass, &c->p_mass}, {in->u, &c->p_u}, {in->dt, &c->p_dt}, {in->h, &c->p_h}, {in->cond, &c->p_cond}};
+    for (auto &f : f1) {
+        if (f.src) GZ_CUDA(c, cudaMemcpyAsync(f.dst->p, f.src, sizeof(double) * N, k, c->cstream));
+        else GZ_CUDA(c, cudaMemsetAsync(f.dst->p, 0, sizeof(double) * N, c->cstream));
+    }
+    GZ_CUDA(c, cudaEventRecord(c->ev_in_done, c->cstream));
+    c->in_pending = true;
+    return GZ_OK;
+}
+
+int gz_wait(gz_context *c)
+{
+    if (!c) return GZ_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->out_pending) {
+        // the context's stream is ordered after the copies too (a caller's event
+        // recorded on it then covers them)
+        GZ_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_out_done, 0));
+        GZ_CUDA(c, cudaEventSynchronize(c->ev_out_done));
+        c->out_pending = false;
+    }
     return GZ_OK;
 }
 
@@ -1847,8 +1946,57 @@ int gz_graph_stats(gz_context *c, gz_graph_info *out)
     return GZ_OK;
 }
 
+// The requested output fields, each as (destination, sorted source, values per
+// particle, element size).
+struct OutField {
+    void *dst;
+    const void *src;
+    int k;
+    int bytes;  // 8 (double) or 4 (int)
+};
+
+static int output_fields(gz_context *c, const gz_outputs *o, std::vector<OutField> &f)
+{
+    const size_t n = (size_t)c->n;
+    struct { double *dst; DevBuf *src; int k; } d[] = {
+        {o->h, &c->h, 1}, {o->num_ngb, &c->num_ngb, 1}, {o->drkern, &c->drkern, 1}, {o->divvel, &c->divvel, 1},
+        {o->rho, &c->rho, 1}, {o->pressure, &c->pressure, 1}, {o->nvt, &c->nvt, 6}, {o->cond, &c->cond, 1},
+        {o->fce, &c->fce, 1}, {o->pvel, &c->pv, 3}, {o->accel, &c->accel, 3}, {o->dudt, &c->dudt, 1},
+        {o->vsig, &c->vsig, 1}, {o->dtmass, &c->dtmass, 1}, {o->dmass, &c->dmass, 1}, {o->gravwork, &c->gw, 3},
+        {o->flux_abs, &c->fabs3, 3}};
+    for (auto &e : d)
+        if (e.dst) {
+            if ((size_t)e.k * n * sizeof(double) > e.src->bytes) return fail(c, GZ_ERR_CAPACITY, "output field");
+            f.push_back({e.dst, e.src->p, e.k, 8});
+        }
+    struct { double *dst; int off; int k; } g[] = {{o->grad_rho, 0, 3}, {o->grad_p, 3, 3}, {o->grad_v, 6, 9}};
+    for (auto &e : g)
+        if (e.dst) f.push_back({e.dst, ptr<double>(c->grad) + (size_t)e.off * n, e.k, 8});
+    if (o->iters) f.push_back({o->iters, c->iters.p, 1, 4});
+    if (o->wakeup) {
+        if (!c->have_bins) return fail(c, GZ_ERR_ORDER, "wakeup: no timebins were uploaded");
+        f.push_back({o->wakeup, c->wakeup.p, 1, 4});
+    }
+    return 0;
+}
+
+// one field from sorted to the caller's order, at `to` (device memory)
+static void scatter_field(gz_context *c, const OutField &e, void *to, cudaStream_t s)
+{
+    const int n = c->n;
+    const long long cnt = (long long)n * e.k;
+    if (e.bytes == 8)
+        k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, e.k, ptr<int>(c->perm), (const double *)e.src,
+                                                                      (double *)to);
+    else
+        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), (const int *)e.src, (int *)to);
+    c->launches++;
+}
+
 // gz_download into host arrays through the staging buffer, or (to_device)
-// straight into the caller's device arrays (gz_download_device).
+// straight into the caller's device arrays (gz_download_device). The host
+// form scatters as many fields as the staging holds (up to 16 doubles per
+// particle), copies them out and waits once per such group.
 static int download_to(gz_context *c, const gz_outputs *o, bool to_device)
 {
     if (!c || !o) return GZ_ERR_ARG;
@@ -1858,63 +2006,87 @@ static int download_to(gz_context *c, const gz_outputs *o, bool to_device)
     const int n = c->n;
     if (n == 0) return GZ_OK;
     cudaStream_t s = c->stream;
-    if (ensure(c, c->dl, sizeof(double) * 9 * (size_t)n)) return c->err;
-    struct { double *dst; DevBuf *src; int k; } f[] = {
-        {o->h, &c->h, 1}, {o->num_ngb, &c->num_ngb, 1}, {o->drkern, &c->drkern, 1}, {o->divvel, &c->divvel, 1},
-        {o->rho, &c->rho, 1}, {o->pressure, &c->pressure, 1}, {o->nvt, &c->nvt, 6}, {o->cond, &c->cond, 1},
-        {o->fce, &c->fce, 1}, {o->pvel, &c->pv, 3}, {o->accel, &c->accel, 3}, {o->dudt, &c->dudt, 1},
-        {o->vsig, &c->vsig, 1}, {o->dtmass, &c->dtmass, 1}, {o->dmass, &c->dmass, 1}, {o->gravwork, &c->gw, 3},
-        {o->flux_abs, &c->fabs3, 3}};
-    for (auto &e : f) {
-        if (!e.dst) continue;
-        const long long cnt = (long long)n * e.k;
-        if ((size_t)cnt * sizeof(double) > c->dl.bytes || (size_t)cnt * sizeof(double) > e.src->bytes)
-            return fail(c, GZ_ERR_CAPACITY, "download staging smaller than the field");
-        k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, e.k, ptr<int>(c->perm), ptr<double>(*e.src),
-                                                                      to_device ? e.dst : ptr<double>(c->dl));
-        c->launches++;
-        if (to_device) continue;
-        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+    std::vector<OutField> f;
+    if (output_fields(c, o, f)) return c->err;
+    if (to_device) {
+        for (auto &e : f) scatter_field(c, e, e.dst, s);
+        GZ_CUDA(c, cudaGetLastError());
         GZ_CUDA(c, cudaStreamSynchronize(s));
+        return GZ_OK;
     }
-    struct { double *dst; int off; } g[] = {{o->grad_rho, 0}, {o->grad_p, 3}, {o->grad_v, 6}};
-    for (auto &e : g) {
-        if (!e.dst) continue;
-        const int k = (e.off == 6) ? 9 : 3;
-        const long long cnt = (long long)n * k;
-        if ((size_t)cnt * sizeof(double) > c->dl.bytes) return fail(c, GZ_ERR_CAPACITY, "download staging too small");
-        k_scatter_out<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(n, k, ptr<int>(c->perm),
-                                                                      ptr<double>(c->grad) + (size_t)e.off * n,
-                                                                      to_device ? e.dst : ptr<double>(c->dl));
-        c->launches++;
-        if (to_device) continue;
-        GZ_CUDA(c, cudaMemcpyAsync(e.dst, c->dl.p, sizeof(double) * (size_t)cnt, cudaMemcpyDeviceToHost, s));
-        GZ_CUDA(c, cudaStreamSynchronize(s));
-    }
-    if (o->iters) {
-        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->iters),
-                                                      to_device ? o->iters : ptr<int>(c->dl));
-        c->launches++;
-        if (!to_device) {
-            GZ_CUDA(c, cudaMemcpyAsync(o->iters, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
-            GZ_CUDA(c, cudaStreamSynchronize(s));
+    const size_t cap = sizeof(double) * 16 * (size_t)n;
+    if (ensure(c, c->dl, cap)) return c->err;
+    size_t used = 0;
+    std::vector<const OutField *> group;
+    auto flush = [&]() -> int {
+        size_t at = 0;
+        for (const OutField *e : group) {
+            const size_t nb = (size_t)e->bytes * e->k * n;
+            GZ_CUDA(c, cudaMemcpyAsync(e->dst, (char *)c->dl.p + at, nb, cudaMemcpyDeviceToHost, s));
+            at += nb;
         }
-    }
-    if (o->wakeup) {
-        if (!c->have_bins) return fail(c, GZ_ERR_ORDER, "wakeup: no timebins were uploaded");
-        k_scatter_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->wakeup),
-                                                      to_device ? o->wakeup : ptr<int>(c->dl));
-        c->launches++;
-        if (!to_device)
-            GZ_CUDA(c, cudaMemcpyAsync(o->wakeup, c->dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));
+        group.clear();
+        used = 0;
+        return 0;
+    };
+    for (auto &e : f) {
+        const size_t nb = (size_t)e.bytes * e.k * n;
+        if (used + nb > cap && flush()) return c->err;
+        scatter_field(c, e, (char *)c->dl.p + used, s);
+        group.push_back(&e);
+        used += nb;
     }
     GZ_CUDA(c, cudaGetLastError());
-    GZ_CUDA(c, cudaStreamSynchronize(s));
+    if (!group.empty() && flush()) return c->err;
     return GZ_OK;
 }
 
+// gz_download_async: every requested field is scattered into its own staging
+// slot on the context's stream, then copied out on the copy stream, which the
+// next pass does not wait for. A second call waits (on the device) until the
+// staging is free again; gz_wait waits for the copies.
+static int download_async(gz_context *c, const gz_outputs *o)
+{
+    if (!c || !o) return GZ_ERR_ARG;
+    if (o->flux_abs && !c->fabs_valid)
+        return fail(c, GZ_ERR_ORDER, "flux_abs: the last force pass ran without GZ_DIAG_FLUX_ABS");
+    cudaSetDevice(c->device);
+    const int n = c->n;
+    if (n == 0) return GZ_OK;
+    std::vector<OutField> f;
+    if (output_fields(c, o, f)) return c->err;
+    size_t total = 0;
+    for (auto &e : f) total += (size_t)e.bytes * e.k * n;
+    if (copy_stream(c)) return c->err;
+    if (c->out_pending) GZ_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_out_done, 0));
+    if (!c->dstage.p || c->dstage.bytes < total) {
+        if (c->out_pending) GZ_CUDA(c, cudaEventSynchronize(c->ev_out_done));
+        if (!try_ensure(c->dstage, total)) return download_to(c, o, false);  // no room: the plain download
+    }
+    cudaStream_t s = c->stream;
+    size_t at = 0;
+    for (auto &e : f) {
+        scatter_field(c, e, (char *)c->dstage.p + at, s);
+        at += (size_t)e.bytes * e.k * n;
+    }
+    GZ_CUDA(c, cudaGetLastError());
+    GZ_CUDA(c, cudaEventRecord(c->ev_out_ready, s));
+    GZ_CUDA(c, cudaStreamWaitEvent(c->cstream, c->ev_out_ready, 0));
+    at = 0;
+    for (auto &e : f) {
+        const size_t nb = (size_t)e.bytes * e.k * n;
+        GZ_CUDA(c, cudaMemcpyAsync(e.dst, (char *)c->dstage.p + at, nb, cudaMemcpyDeviceToHost, c->cstream));
+        at += nb;
+    }
+    GZ_CUDA(c, cudaEventRecord(c->ev_out_done, c->cstream));
+    c->out_pending = true;
+    return GZ_OK;
+}
 
 int gz_download(gz_context *c, const gz_outputs *o) { return download_to(c, o, false); }
+
+int gz_download_async(gz_context *c, const gz_outputs *o) { return download_async(c, o); }
 
 int gz_download_device(gz_context *c, const gz_outputs *o) { return download_to(c, o, true); }
 

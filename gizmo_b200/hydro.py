@@ -128,23 +128,48 @@ class HydroPass:
     def upload_raw(self, n: int, ptrs: dict):
         """Upload from caller-owned host buffers (e.g. pinned memory): ptrs maps
         pos/vel/mass/u/dt/h/cond to addresses of row-major FP64 arrays."""
+        p = self._raw_particles(n, ptrs)
+        self._check(self.lib.gz_upload(self._ctx, C.byref(p)))
+        self.n = int(n)
+
+    @staticmethod
+    def _raw_particles(n: int, ptrs: dict):
         p = abi.GzParticles()
         p.n = int(n)
         for k in ("pos", "vel", "mass", "u", "dt", "h", "cond"):
             if ptrs.get(k):
                 setattr(p, k, C.cast(C.c_void_p(int(ptrs[k])), C.POINTER(C.c_double)))
-        self._check(self.lib.gz_upload(self._ctx, C.byref(p)))
-        self.n = int(n)
+        return p
+
+    @staticmethod
+    def _raw_outputs(ptrs: dict):
+        o = abi.GzOutputs()
+        for k, v in ptrs.items():
+            if k in ("iters", "wakeup"):
+                setattr(o, k, C.cast(C.c_void_p(int(v)), C.POINTER(C.c_int)))
+            else:
+                setattr(o, k, C.cast(C.c_void_p(int(v)), C.POINTER(C.c_double)))
+        return o
 
     def download_raw(self, ptrs: dict):
         """Download into caller-owned host buffers (addresses per output field)."""
-        o = abi.GzOutputs()
-        for k, v in ptrs.items():
-            if k == "iters":
-                o.iters = C.cast(C.c_void_p(int(v)), C.POINTER(C.c_int))
-            else:
-                setattr(o, k, C.cast(C.c_void_p(int(v)), C.POINTER(C.c_double)))
-        self._check(self.lib.gz_download(self._ctx, C.byref(o)))
+        self._check(self.lib.gz_download(self._ctx, C.byref(self._raw_outputs(ptrs))))
+
+    def upload_raw_async(self, n: int, ptrs: dict):
+        """gz_upload_async from caller-owned (pinned) host buffers: the copies run
+        beside the current pass; the next restage() takes them. The buffers must
+        stay untouched until that restage returns."""
+        p = self._raw_particles(n, ptrs)
+        self._check(self.lib.gz_upload_async(self._ctx, C.byref(p)))
+        self.n = int(n)
+
+    def download_raw_async(self, ptrs: dict):
+        """gz_download_async into caller-owned (pinned) host buffers; they are
+        filled when wait() returns."""
+        self._check(self.lib.gz_download_async(self._ctx, C.byref(self._raw_outputs(ptrs))))
+
+    def wait(self):
+        self._check(self.lib.gz_wait(self._ctx))
 
     def restage(self):
         """Rebuild grid + sorted mirror from the resident inputs (no host traffic)."""

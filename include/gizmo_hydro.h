@@ -43,8 +43,9 @@ extern "C" {
 
 /* Arithmetic forms of the pass. */
 #define GZ_PRECISION_FP64  0   /* every pair and per-particle operation in FP64 */
-#define GZ_PRECISION_MIXED 1   /* FP32 pair math; FP64 positions, membership,
-                                  h-iteration, 3x3 inversion and flux sums */
+#define GZ_PRECISION_MIXED 1   /* FP32 force-pair arithmetic (pairs whose FP32 decisions are too close
+                                  to call evaluated again in FP64); FP64 positions, membership,
+                                  density and h-iteration, gradients, 3x3 inversion and flux sums */
 
 /* Return codes. */
 #define GZ_OK                   0
@@ -206,6 +207,25 @@ int gz_graph_stats(gz_context *ctx, gz_graph_info *out);
 
 /* Copy outputs device -> host (original order). */
 int gz_download(gz_context *ctx, const gz_outputs *out);
+
+/* Pipelined transfers, for a host that overlaps the copies of one step with
+ * the pass of another (from pinned host memory they run on a copy stream of
+ * the context, beside its kernels):
+ *   gz_upload_async  : the inputs of the next step (same n, no timebins; other
+ *                      uploads fall back to gz_upload) are copied while the
+ *                      current pass runs; the next gz_restage makes them the
+ *                      resident inputs. The host arrays must stay untouched
+ *                      until that gz_restage returns.
+ *   gz_download_async: the outputs of the last pass are scattered to a device
+ *                      staging area on the context's stream and copied to the
+ *                      host arrays on the copy stream; the next pass does not
+ *                      wait for the copies. The host arrays are filled when
+ *                      gz_wait returns.
+ *   gz_wait          : waits for the pending output copies (and orders the
+ *                      context's stream after them). */
+int gz_upload_async(gz_context *ctx, const gz_particles *in);
+int gz_download_async(gz_context *ctx, const gz_outputs *out);
+int gz_wait(gz_context *ctx);
 
 /* gz_upload and gz_download with the caller's arrays in DEVICE memory (the
  * same layouts; device-to-device copies and scatters, no host traffic), for a
