@@ -143,7 +143,7 @@ EXPORTED_SYMBOLS = [
     "gz_neighbors", "gz_density_sums", "gz_density_sums_noalloc", "gz_kick",
     "gz_drift", "gz_set_bin_active", "gz_active_list", "gz_wakeup_bins", "gz_timestep",
     "gz_upload_device", "gz_download_device", "gz_get_tuning", "gz_set_tuning", "gz_autotune",
-    "gz_hydro_pass", "gz_graph_stats", "gz_upload_async", "gz_download_async", "gz_wait",
+    "gz_hydro_pass", "gz_graph_stats", "gz_upload_async", "gz_download_async", "gz_wait", "gz_set_boxes",
 ]
 PASS_GRAPH = 1  # GZ_PASS_GRAPH
 TIMEBINS = 60  # GZ_TIMEBINS

@@ -112,6 +112,11 @@ struct gz_context {
         bool capturing = false;                     // no timer events while a graph is captured
     } g;
     DevBuf gstate, g_hseed, g_cseed, g_over_list, g_over_off, g_sel;
+    // box sets (gz_set_boxes): consecutive runs of the particles, each its own
+    // periodic box; their index above the Morton bits of the keys
+    std::vector<long long> box_counts;
+    int box_bits = 0;                // bits of the box index (a multiple of 3: whole octree levels)
+    DevBuf box_bid, box_of, root_of; // box of each particle (caller's order, sorted), subtree of each box
     // pipelined transfers (gz_upload_async / gz_download_async): the inputs of
     // the next step land in p_* while a step runs; the outputs of a step leave
     // from dstage while the next one runs
@@ -288,7 +293,8 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->s_counts, &c->rec, &c->work, &c->hmax, &c->refined, &c->rq, &c->pad_over, &c->pad_list, &c->pad_sum, &c->pad_counts, &c->s_acnt, &c->s_bcnt, &c->s_tmp, &c->pflux, &c->status, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond, &c->dl, &c->o_timebin,
             &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out,
             &c->gstate, &c->g_hseed, &c->g_cseed, &c->g_over_list, &c->g_over_off, &c->g_sel,
-            &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond, &c->dstage};
+            &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond, &c->dstage,
+            &c->box_bid, &c->box_of, &c->root_of};
 }
 
 Tree tree_view(gz_context *c)
@@ -300,6 +306,10 @@ Tree tree_view(gz_context *c)
     t.node = ptr<int4>(c->t_node);
     t.lo = ptr<double4>(c->t_lo);
     t.hi = ptr<double4>(c->t_hi);
+    if (c->box_bits) {
+        t.box_of = ptr<int>(c->box_of);
+        t.root_of = ptr<int>(c->root_of);
+    }
     return t;
 }
 
@@ -655,7 +665,8 @@ int build_grid(gz_context *c)
     if (ensure(c, c->keys, sizeof(unsigned long long) * N) || ensure(c, c->keys_sorted, sizeof(unsigned long long) * N) ||
         ensure(c, c->idx, sizeof(int) * N))
         return c->err;
-    grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, ptr<unsigned long long>(c->keys), ptr<int>(c->idx), s);
+    grid_keys(n, ptr<double>(c->stage3), c->prm.box_size, c->box_bits ? ptr<int>(c->box_bid) : nullptr,
+              21 - c->box_bits / 3, ptr<unsigned long long>(c->keys), ptr<int>(c->idx), s);
     size_t tmp = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp, ptr<unsigned long long>(c->keys),
                                     ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n, 0,
@@ -665,6 +676,14 @@ int build_grid(gz_context *c)
                                     ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n, 0,
                                     63, s);
     if (n > 0) k_inverse<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->inv));
+    if (c->box_bits && n > 0) {
+        if (ensure(c, c->box_of, sizeof(int) * N) ||
+            ensure(c, c->root_of, sizeof(int) * std::max<size_t>(c->box_counts.size(), 1)))
+            return c->err;
+        k_gather_int<<<(n + 255) / 256, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->box_bid), ptr<int>(c->box_of));
+        GZ_CUDA(c, cudaMemsetAsync(c->root_of.p, 0xff, sizeof(int) * c->box_counts.size(), s));
+        c->launches++;
+    }
     GZ_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -688,9 +707,14 @@ int build_tree(gz_context *c)
     GZ_CUDA(c, cudaMemcpyAsync(c->t_parent.p, &no_parent, sizeof(int), cudaMemcpyHostToDevice, s));
     int beg = 0, cnt = 1, L = 0;
     const unsigned long long *keys = ptr<unsigned long long>(c->keys_sorted);
+    const int split_levels = c->box_bits / 3;
     while (cnt > 0) {
         if (ensure(c, c->t_nch, sizeof(long long) * (size_t)cnt)) return c->err;
-        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<long long>(c->t_nch), c->leaf_max, s);
+        if (c->box_bits && L == split_levels) {  // one node per box
+            box_roots(beg, cnt, ptr<int4>(c->t_node), ptr<int>(c->box_of), ptr<int>(c->root_of), s);
+            c->launches++;
+        }
+        tree_count(keys, L, ptr<int4>(c->t_node), beg, cnt, ptr<long long>(c->t_nch), c->leaf_max, split_levels, s);
         c->launches++;
         long long next = 0;
         if (exclusive_scan_counts(c, cnt, c->t_nch, c->t_cpos, &next)) return c->err;
@@ -1636,6 +1660,18 @@ static int upload_from(gz_context *c, const gz_particles *in, cudaMemcpyKind kin
                 GZ_CUDA(c, cudaMemsetAsync(c->o_vsig.p, 0, sizeof(double) * (size_t)n, s));
         }
     }
+    if (!c->box_counts.empty()) {
+        long long total = 0;
+        for (long long k : c->box_counts) total += k;
+        if (total != n) return fail(c, GZ_ERR_ARG, "box counts do not add up to the particle count");
+        std::vector<int> bid((size_t)std::max(n, 1));
+        size_t at = 0;
+        for (size_t b = 0; b < c->box_counts.size(); b++)
+            for (long long k = 0; k < c->box_counts[b]; k++) bid[at++] = (int)b;
+        if (ensure(c, c->box_bid, sizeof(int) * N)) return c->err;
+        GZ_CUDA(c, cudaMemcpyAsync(c->box_bid.p, bid.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        GZ_CUDA(c, cudaStreamSynchronize(s));  // (bid is freed on return)
+    }
     if (stage_inputs(c)) return c->err;
     GZ_CUDA(c, cudaStreamSynchronize(s));
     return c->err;
@@ -1931,6 +1967,24 @@ int gz_hydro_pass(gz_context *c, int flags)
     if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
     if (!rc) rc = gz_hydro_force(c, nullptr, 0);
     return rc;
+}
+
+int gz_set_boxes(gz_context *c, int n_boxes, const int64_t *counts)
+{
+    if (!c || n_boxes < 0 || n_boxes > (1 << 15) || (n_boxes > 1 && !counts)) return GZ_ERR_ARG;
+    if (n_boxes <= 1) {
+        c->box_counts.clear();
+        c->box_bits = 0;
+    } else {
+        for (int b = 0; b < n_boxes; b++)
+            if (counts[b] < 0) return GZ_ERR_ARG;
+        int bits = 0;
+        while ((1 << bits) < n_boxes) bits++;
+        c->box_counts.assign(counts, counts + n_boxes);
+        c->box_bits = 3 * ((bits + 2) / 3);  // whole octree levels
+    }
+    c->grid_valid = false;  // the next upload builds the grid of the boxes
+    return GZ_OK;
 }
 
 int gz_graph_stats(gz_context *c, gz_graph_info *out)

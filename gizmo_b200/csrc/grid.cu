@@ -45,19 +45,35 @@ GZ_DEV unsigned long long spread21(unsigned long long x)
     return x;
 }
 
-__global__ void k_keys(int n, const double *__restrict__ pos, double box, unsigned long long *keys, int *idx)
+// Morton key of `axis_bits` bits per axis; with box sets (bid non-null) the
+// particle's box index above them, so every box is one run of the sorted keys
+// and one subtree of the octree (its top levels split the box bits).
+__global__ void k_keys(int n, const double *__restrict__ pos, double box, const int *__restrict__ bid, int axis_bits,
+                       unsigned long long *keys, int *idx)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const long long G = 1ll << kBits;
+    const long long G = 1ll << axis_bits;
     unsigned long long c[3];
     for (int k = 0; k < 3; k++) {
         long long v = (long long)(pos[3 * (size_t)i + k] / box * (double)G);
         v = v < 0 ? 0 : (v >= G ? G - 1 : v);
         c[k] = (unsigned long long)v;
     }
-    keys[i] = spread21(c[0]) | (spread21(c[1]) << 1) | (spread21(c[2]) << 2);
+    unsigned long long key = spread21(c[0]) | (spread21(c[1]) << 1) | (spread21(c[2]) << 2);
+    if (bid) key |= (unsigned long long)bid[i] << (3 * axis_bits);
+    keys[i] = key;
     idx[i] = i;
+}
+
+// The subtree of each box: the nodes of the level below the box bits, each one
+// box's particles.
+__global__ void k_box_roots(int beg, int cnt, const int4 *__restrict__ node, const int *__restrict__ box_of,
+                            int *root_of)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    root_of[box_of[node[beg + i].x]] = beg + i;
 }
 
 // first position in [a, b) whose key is >= key
@@ -86,14 +102,15 @@ GZ_DEV void child_bounds(const unsigned long long *__restrict__ keys, int a, int
 }
 
 // number of non-empty children of every node of one level
+// (levels above split_levels split whatever their size: the box bits of box sets)
 __global__ void k_tree_count(const unsigned long long *__restrict__ keys, int L, const int4 *__restrict__ node,
-                             int beg, int cnt, long long *nch, int leaf_max)
+                             int beg, int cnt, long long *nch, int leaf_max, int split_levels)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
     const int4 nd = node[beg + i];
     int c = 0;
-    if (nd.y > leaf_max && L < kBits) {
+    if ((nd.y > leaf_max || L < split_levels) && L < kBits) {
         int bound[9];
         child_bounds(keys, nd.x, nd.x + nd.y, L, bound);
         for (int d = 0; d < 8; d++) c += bound[d + 1] > bound[d];
@@ -287,14 +304,23 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
         fl = make_float4(__double2float_rd(l.x), __double2float_rd(l.y), __double2float_rd(l.z), __double2float_ru(l.w));
         fu = make_float4(__double2float_ru(u.x), __double2float_ru(u.y), __double2float_ru(u.z), 0.0f);
     };
+    // The tree is walked from its root; with box sets from each lane's box
+    // subtree, one box at a time (the lanes of a group of consecutive targets
+    // span one box or a few)
+    const int my_root = (t.root_of && valid) ? t.root_of[t.box_of[tg]] : 0;
+    unsigned roots_left = __ballot_sync(full, valid);
     int sp = 0;
+    while (roots_left) {
+    const int root = __shfl_sync(full, my_root, __ffs(roots_left) - 1);
+    const bool in_root = valid && my_root == root;
+    roots_left &= ~__ballot_sync(full, in_root);
     {
         float4 l, u;
-        outward(t.lo[0], t.hi[0], l, u);
-        const unsigned m = __ballot_sync(full, reaches(l, u));
+        outward(t.lo[root], t.hi[root], l, u);
+        const unsigned m = __ballot_sync(full, in_root && reaches(l, u));
         if (m) {
             if (lane == 0) {
-                const int4 nd = t.node[0];
+                const int4 nd = t.node[root];
                 s_stack[wib][0] = StackNode{nd.x, nd.y, nd.z, nd.w, m};
             }
             sp = 1;
@@ -447,6 +473,8 @@ __device__ __forceinline__ void walk_group(const int group, const Tree &t, const
         sp += npush;
         __syncwarp();
     }
+    if (sp > 0) break;  // the stack overflowed (recorded): no further box
+    }  // the roots
     if (!FILL || cap) {
         if (SOLO) { if (lane == 0) counts[slot] = cnt; }
         else if (valid) counts[slot] = cnt;
@@ -680,15 +708,21 @@ void padded_rows(int na, const int *t, const long long *counts, int cap, long lo
     if (na > 0) k_padded_rows<<<(na + 255) / 256, 256, 0, s>>>(na, t, counts, cap, base, beg, end, over);
 }
 
-void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s)
+void grid_keys(int n, const double *pos, double box, const int *bid, int axis_bits, unsigned long long *keys, int *idx,
+               cudaStream_t s)
 {
-    if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, keys, idx);
+    if (n > 0) k_keys<<<(n + 255) / 256, 256, 0, s>>>(n, pos, box, bid, axis_bits, keys, idx);
 }
 
 void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch,
-                int leaf_max, cudaStream_t s)
+                int leaf_max, int split_levels, cudaStream_t s)
 {
-    if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch, leaf_max);
+    if (cnt > 0) k_tree_count<<<(cnt + 127) / 128, 128, 0, s>>>(keys, L, node, beg, cnt, nch, leaf_max, split_levels);
+}
+
+void box_roots(int beg, int cnt, const int4 *node, const int *box_of, int *root_of, cudaStream_t s)
+{
+    if (cnt > 0) k_box_roots<<<(cnt + 127) / 128, 128, 0, s>>>(beg, cnt, node, box_of, root_of);
 }
 
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,

@@ -9,9 +9,13 @@
 namespace gz {
 
 // grid.cu
-void grid_keys(int n, const double *pos, double box, unsigned long long *keys, int *idx, cudaStream_t s);
+// keys of axis_bits per axis, with the box index above them for box sets (bid non-null)
+void grid_keys(int n, const double *pos, double box, const int *bid, int axis_bits, unsigned long long *keys, int *idx,
+               cudaStream_t s);
 void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg, int cnt, long long *nch,
-                int leaf_max, cudaStream_t s);
+                int leaf_max, int split_levels, cudaStream_t s);
+// the subtree of each box from the nodes of the level below the box bits
+void box_roots(int beg, int cnt, const int4 *node, const int *box_of, int *root_of, cudaStream_t s);
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
                 const long long *cpos, int next, cudaStream_t s);
 void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,

@@ -63,6 +63,10 @@ struct Tree {
     const int4 *node;               // {first, count, child or -1, nchild}
     const double4 *lo;              // tight box minimum xyz; w = maximum h in the node
     const double4 *hi;              // tight box maximum xyz
+    // box sets (null for one box): each particle's box (sorted order) and the
+    // node of each box's subtree, where the walk of its particles starts
+    const int *box_of;
+    const int *root_of;
 };
 
 // What a density row reads of each neighbour, in one 64-byte record (sorted

@@ -228,6 +228,16 @@ class HydroPass:
         has sized its buffers. Results equal full_pass()'s."""
         self._check(self.lib.gz_hydro_pass(self._ctx, abi.PASS_GRAPH if graph else 0))
 
+    def set_boxes(self, counts=None):
+        """Box sets (gz_set_boxes): the next uploads hold len(counts) consecutive
+        runs of counts[b] particles, each its own periodic box; None: one box."""
+        if counts is None or len(counts) <= 1:
+            self._check(self.lib.gz_set_boxes(self._ctx, 0, None))
+            return
+        a = np.ascontiguousarray(counts, dtype=np.int64)
+        self._keep.append(a)
+        self._check(self.lib.gz_set_boxes(self._ctx, int(a.shape[0]), a.ctypes.data_as(C.POINTER(C.c_int64))))
+
     def graph_stats(self) -> dict:
         g = abi.GzGraphInfo()
         self._check(self.lib.gz_graph_stats(self._ctx, C.byref(g)))

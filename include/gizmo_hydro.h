@@ -195,6 +195,17 @@ int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
 #define GZ_PASS_GRAPH 1
 int gz_hydro_pass(gz_context *ctx, int flags);
 
+/* Box sets: the particles of the following uploads are n_boxes consecutive
+ * runs of counts[b] particles, each an independent periodic box of the
+ * context's box_size and parameters (a pair never joins two boxes). The passes
+ * then cover all boxes in one launch per kernel (and gz_hydro_pass in one
+ * graph): the Morton keys carry the box index above 21 - box_bits/3 bits per
+ * axis (box_bits = 3 ceil(log2(n_boxes) / 3)), so each box is one run of the
+ * sorted particles and one subtree of the octree, where the walks of its
+ * particles start. n_boxes <= 1 returns to one box; at most 32768 boxes.
+ * The next gz_upload must hold sum(counts) particles. */
+int gz_set_boxes(gz_context *ctx, int n_boxes, const int64_t *counts);
+
 typedef struct gz_graph_info {
     int64_t captures;               /* graphs captured (a change of buffers or settings captures again) */
     int64_t replays;                /* passes run through a graph */
