@@ -404,7 +404,7 @@ def run_ours(args, world, rank, local):
     for name, d in (ktimes or {}).items():
         if d["launches"] == 0 or d["ms"] <= 0:
             continue
-        e = {"launches_per_step": d["launches"] / K, "ms_per_step": d["ms"] / K,
+        e = {"launches_per_step": d["launches"] / K64, "ms_per_step": d["ms"] / K64,
              "ms_per_launch": d["ms"] / d["launches"], "units_per_launch": d["units"] / d["launches"]}
         flops = None
         if name == "density_sums":  # FP64; a converged row holds ~DesNumNgb accepted pairs

@@ -59,7 +59,7 @@ struct gz_context {
     DevBuf work;                     // work counter of the persistent walks
     long long launches = 0;          // kernels of this library launched by the context
     // octree over the sorted particles
-    DevBuf t_node, t_lo, t_hi, t_parent, t_done, t_nch, t_cpos;
+    DevBuf t_node, t_lo, t_hi, t_parent, t_done, t_nch, t_cpos, t_build;
     int t_nodes = 0, t_levels = 0;
     bool grid_valid = false;
     // density work: rows are [d_beg[t], d_end[t]) in d_nbr; d_used entries are taken
@@ -294,7 +294,7 @@ std::vector<DevBuf *> all_buffers(gz_context *c)
             &c->o_vsig, &c->timebin, &c->vsig_prev, &c->wakeup, &c->binact, &c->sel_flags, &c->sel_out,
             &c->gstate, &c->g_hseed, &c->g_cseed, &c->g_over_list, &c->g_over_off, &c->g_sel,
             &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond, &c->dstage,
-            &c->box_bid, &c->box_of, &c->root_of};
+            &c->box_bid, &c->box_of, &c->root_of, &c->t_build};
 }
 
 Tree tree_view(gz_context *c)
@@ -688,9 +688,9 @@ int build_grid(gz_context *c)
     return 0;
 }
 
-// Octree over the sorted keys, split top-down one level per step (the size of
-// the next level is read back each step), then boxes and h maxima bottom-up.
-int build_tree(gz_context *c)
+// Octree over the sorted keys, split top-down one level per step with the size
+// of the next level read back each step (the fallback of build_tree).
+int build_tree_levels(gz_context *c)
 {
     const int n = c->n;
     cudaStream_t s = c->stream;
@@ -743,6 +743,43 @@ int build_tree(gz_context *c)
     }
     c->t_nodes = beg;
     c->t_levels = L;
+    if (ensure(c, c->t_lo, sizeof(double4) * (size_t)c->t_nodes) || ensure(c, c->t_hi, sizeof(double4) * (size_t)c->t_nodes) ||
+        ensure(c, c->t_done, sizeof(int) * (size_t)c->t_nodes))
+        return c->err;
+    tree_up(c->t_nodes, ptr<int4>(c->t_node), ptr<int>(c->t_parent), ptr<double>(c->x), ptr<double>(c->y),
+            ptr<double>(c->z), ptr<double>(c->h), ptr<double4>(c->t_lo), ptr<double4>(c->t_hi), ptr<int>(c->t_done), 1, s);
+    c->launches++;
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// Octree over the sorted keys, all levels on the device (tree_build_device)
+// with one read-back of the node count at the end, then boxes and h maxima
+// bottom-up. A tree larger than the nodes held for it (a few coincident
+// particles split down to the deepest level) is built level by level instead.
+int build_tree(gz_context *c)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    c->t_nodes = 0;
+    c->t_levels = 0;
+    if (n == 0) return 0;
+    const long long cap = std::max<long long>(4096, n / 4) + 2 * (long long)c->box_counts.size() + 64;
+    if (cap > INT32_MAX) return fail(c, GZ_ERR_CAPACITY, "octree exceeds capacity");
+    if (ensure(c, c->t_node, sizeof(int4) * (size_t)cap) || ensure(c, c->t_parent, sizeof(int) * (size_t)cap) ||
+        ensure(c, c->t_build, sizeof(TreeBuild)))
+        return c->err;
+    tree_build_device(ptr<unsigned long long>(c->keys_sorted), n, ptr<int4>(c->t_node), ptr<int>(c->t_parent),
+                      ptr<TreeBuild>(c->t_build), (int)cap, c->leaf_max, c->box_bits / 3,
+                      c->box_bits ? ptr<int>(c->box_of) : nullptr, c->box_bits ? ptr<int>(c->root_of) : nullptr,
+                      c->sms * 8, s);
+    c->launches += 1 + 2 * 22;
+    TreeBuild tb{};
+    GZ_CUDA(c, cudaMemcpyAsync(&tb, c->t_build.p, sizeof(tb), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(c, cudaStreamSynchronize(s));
+    if (tb.fail) return build_tree_levels(c);
+    c->t_nodes = tb.total;
+    c->t_levels = tb.L;
     if (ensure(c, c->t_lo, sizeof(double4) * (size_t)c->t_nodes) || ensure(c, c->t_hi, sizeof(double4) * (size_t)c->t_nodes) ||
         ensure(c, c->t_done, sizeof(int) * (size_t)c->t_nodes))
         return c->err;

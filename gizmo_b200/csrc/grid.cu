@@ -118,6 +118,70 @@ __global__ void k_tree_count(const unsigned long long *__restrict__ keys, int L,
     nch[i] = c;
 }
 
+// ---------------------------------------------- the octree built on the device
+// All levels in one stream of launches with no host round trip: each level's
+// nodes take their children's places from a counter (a node's children are
+// contiguous and in octant order; the order of the nodes of a level depends on
+// the atomics, and nothing downstream depends on it: the walks follow child
+// ranges, the boxes are reduced bottom-up). A level that would pass the node
+// capacity sets `fail` and the host builds the tree level by level instead.
+__global__ void k_tree_init(TreeBuild *tb, int4 *node, int *parent, int n)
+{
+    node[0] = make_int4(0, n, -1, 0);
+    parent[0] = -1;
+    TreeBuild t{};
+    t.level_cnt = n > 0 ? 1 : 0;
+    t.total = t.level_cnt;
+    *tb = t;
+}
+
+__global__ void k_tree_level(const unsigned long long *__restrict__ keys, int4 *node, int *parent, TreeBuild *tb,
+                             int cap, int leaf_max, int split_levels, const int *__restrict__ box_of, int *root_of)
+{
+    if (tb->fail) return;
+    const int L = tb->L, beg = tb->level_beg, cnt = tb->level_cnt, end = tb->total;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int4 nd = node[beg + i];
+        if (box_of && L == split_levels) root_of[box_of[nd.x]] = beg + i;  // one node per box
+        int bound[9];
+        int c = 0;
+        if ((nd.y > leaf_max || L < split_levels) && L < kBits) {
+            child_bounds(keys, nd.x, nd.x + nd.y, L, bound);
+            for (int d = 0; d < 8; d++) c += bound[d + 1] > bound[d];
+        }
+        nd.z = -1;
+        nd.w = 0;
+        if (c > 0) {
+            const int first = end + atomicAdd(&tb->next_cnt, c);
+            if ((long long)first + c > cap) {
+                atomicOr(&tb->fail, 1);
+            } else {
+                int k = 0;
+                for (int d = 0; d < 8; d++) {
+                    if (bound[d + 1] > bound[d]) {
+                        node[first + k] = make_int4(bound[d], bound[d + 1] - bound[d], -1, 0);
+                        parent[first + k] = beg + i;
+                        k++;
+                    }
+                }
+                nd.z = first;
+                nd.w = c;
+            }
+        }
+        node[beg + i] = nd;
+    }
+}
+
+__global__ void k_tree_next(TreeBuild *tb)
+{
+    TreeBuild &t = *tb;
+    t.level_beg = t.total;
+    t.level_cnt = t.fail ? 0 : t.next_cnt;
+    t.total += t.level_cnt;
+    t.next_cnt = 0;
+    t.L++;
+}
+
 // children of one level written at next + cpos[i] (cpos: inclusive scan of nch)
 __global__ void k_tree_write(const unsigned long long *__restrict__ keys, int L, int4 *node, int *parent, int beg,
                              int cnt, const long long *__restrict__ cpos, int next)
@@ -163,12 +227,13 @@ GZ_DEV void st_cg4(double4 *p, double4 v)
 // particles, and the last child to finish (atomic count per parent) reduces
 // the parent's children, and so on to the root. With boxes == 0 only the h
 // maxima (lo.w) are refreshed.
-__global__ void k_tree_up(int n_nodes, const int4 *__restrict__ node, const int *__restrict__ parent,
-                          const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
-                          const double *__restrict__ h, double4 *lo, double4 *hi, int *done, int boxes)
+__global__ void k_tree_up(int n_nodes, const int *__restrict__ n_nodes_dev, const int4 *__restrict__ node,
+                          const int *__restrict__ parent, const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, const double *__restrict__ h, double4 *lo, double4 *hi,
+                          int *done, int boxes)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_nodes) return;
+    if (i >= (n_nodes_dev ? *n_nodes_dev : n_nodes)) return;
     const int4 nd = node[i];
     if (nd.z >= 0) return;  // internal: reduced by its last child
     double4 l = make_double4(1e300, 1e300, 1e300, 0.0), u = make_double4(-1e300, -1e300, -1e300, 0.0);
@@ -732,11 +797,22 @@ void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, 
 }
 
 void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,
-             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s)
+             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s, const int *n_nodes_dev)
 {
     if (n_nodes <= 0) return;
     cudaMemsetAsync(done, 0, sizeof(int) * (size_t)n_nodes, s);
-    k_tree_up<<<(n_nodes + 127) / 128, 128, 0, s>>>(n_nodes, node, parent, x, y, z, h, lo, hi, done, boxes);
+    k_tree_up<<<(n_nodes + 127) / 128, 128, 0, s>>>(n_nodes, n_nodes_dev, node, parent, x, y, z, h, lo, hi, done,
+                                                     boxes);
+}
+
+void tree_build_device(const unsigned long long *keys, int n, int4 *node, int *parent, TreeBuild *tb, int cap,
+                       int leaf_max, int split_levels, const int *box_of, int *root_of, int blocks, cudaStream_t s)
+{
+    k_tree_init<<<1, 1, 0, s>>>(tb, node, parent, n);
+    for (int L = 0; L <= kBits; L++) {
+        k_tree_level<<<blocks, 128, 0, s>>>(keys, node, parent, tb, cap, leaf_max, split_levels, box_of, root_of);
+        k_tree_next<<<1, 1, 0, s>>>(tb);
+    }
 }
 
 template <bool SYM, bool FILL, bool SOLO>

@@ -18,8 +18,14 @@ void tree_count(const unsigned long long *keys, int L, const int4 *node, int beg
 void box_roots(int beg, int cnt, const int4 *node, const int *box_of, int *root_of, cudaStream_t s);
 void tree_write(const unsigned long long *keys, int L, int4 *node, int *parent, int beg, int cnt,
                 const long long *cpos, int next, cudaStream_t s);
+// boxes and h maxima bottom-up over the first n_nodes nodes (or *n_nodes_dev of them, when given)
 void tree_up(int n_nodes, const int4 *node, const int *parent, const double *x, const double *y, const double *z,
-             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s);
+             const double *h, double4 *lo, double4 *hi, int *done, int boxes, cudaStream_t s,
+             const int *n_nodes_dev = nullptr);
+// the octree of n sorted keys built level by level on the device (TreeBuild on
+// the device: total nodes, fail when cap would be passed)
+void tree_build_device(const unsigned long long *keys, int n, int4 *node, int *parent, TreeBuild *tb, int cap,
+                       int leaf_max, int split_levels, const int *box_of, int *root_of, int blocks, cudaStream_t s);
 void walk_rows(const Tree &t, const double *x, const double *y, const double *z, const double *reach,
                const double *hsym, int symmetric, const int *targets, int n_targets, long long *counts,
                const long long *off, int *nbr, int cap, DevStatus *st, int *next_group, cudaStream_t s);

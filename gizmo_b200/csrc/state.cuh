@@ -69,6 +69,11 @@ struct Tree {
     const int *root_of;
 };
 
+// Device state of the octree build (tree_build_device).
+struct TreeBuild {
+    int level_beg, level_cnt, next_cnt, total, fail, L;
+};
+
 // What a density row reads of each neighbour, in one 64-byte record (sorted
 // order), packed once per pass: the pair loop then issues two 32-byte reads
 // per neighbour instead of seven scattered ones.
