@@ -223,6 +223,36 @@ def cpu_baseline(n1: int, name: str, kind_pref: str = "reference", steps: int = 
 
 
 # ------------------------------------------------------------------ GPU arm
+def vector_peaks(torch, n: int = 8192, reps: int = 5) -> dict:
+    """Measured non-tensor FP64 and FP32 rates on this GPU, for the roofline of
+    the pair kernels (MEASURED_PEAKS.json holds bf16 tensor and HBM figures
+    only): cuBLAS DGEMM and SGEMM (TF32 off) at n^3, best of `reps` timed with
+    CUDA events, 2 n^3 flop each."""
+    out = {}
+    tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for dtype, tag in ((torch.float64, "fp64"), (torch.float32, "fp32")):
+            a = torch.randn(n, n, device="cuda", dtype=dtype)
+            b = torch.randn(n, n, device="cuda", dtype=dtype)
+            torch.matmul(a, b)
+            best = None
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(a, b)
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / 1e3
+                best = t if best is None else min(best, t)
+            out[tag] = 2.0 * n ** 3 / best / 1e12
+            del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -230,6 +260,7 @@ def run_ours(args, world, rank, local):
     from gizmo_b200.hydro import HydroPass
 
     torch.cuda.set_device(local)
+    measured = vector_peaks(torch)
     n1 = args.n1 or default_n1(args.workload)
     t_gen = time.time()
     wl = make_workload(args.workload, n1, abi.PRECISION_FP64)
@@ -258,16 +289,17 @@ def run_ours(args, world, rank, local):
     hpm.upload_workload(wl)
 
     def run_steps(hp, K, W, record_clock=False, graph=True, timing=False):
-        """K timed steps of restage + pass after W untimed ones. graph: the pass
-        as one CUDA graph (gz_hydro_pass), events around the restage and the
-        graph; otherwise the three plain calls with events between them (and,
-        with timing, the library's per-kernel timers)."""
+        """K timed steps of restage + pass after W untimed ones. graph: the
+        restage and the pass as one CUDA graph (gz_hydro_pass with
+        GZ_PASS_GRAPH | GZ_PASS_RESTAGE), events around it; otherwise restage
+        and the three plain calls with events between them (and, with timing,
+        the library's per-kernel timers)."""
         stream = torch.cuda.ExternalStream(hp.stream)
         for _ in range(W):
-            hp.restage()
             if graph:
-                hp.hydro_pass(graph=True)
+                hp.hydro_pass(graph=True, restage=True)
             else:
+                hp.restage()
                 hp.full_pass()
         torch.cuda.synchronize()
         dist_barrier(world)
@@ -276,16 +308,16 @@ def run_ours(args, world, rank, local):
         if timing:
             hp.kernel_timing(True)
         l0 = hp.status()["kernel_launches"]
-        names = ["grid", "pass"] if graph else ["grid", "density", "gradients", "force"]
+        names = ["step"] if graph else ["grid", "density", "gradients", "force"]
         ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)] for _ in range(K)]
         for k in range(K):
             ev[k][0].record(stream)
-            hp.restage()
-            ev[k][1].record(stream)
-            if graph:
-                hp.hydro_pass(graph=True)
-                ev[k][2].record(stream)
+            if graph:  # the restage and the pass in one graph
+                hp.hydro_pass(graph=True, restage=True)
+                ev[k][1].record(stream)
             else:
+                hp.restage()
+                ev[k][1].record(stream)
                 hp.density()
                 ev[k][2].record(stream)
                 hp.hydro_gradient_calc()
@@ -398,8 +430,9 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    fp64_peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+    nominal = {"fp32": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12, "fp64": 148 * 64 * 2 * sm_mhz * 1e6 / 1e12}
+    fp32_peak = measured.get("fp32") or nominal["fp32"]
+    fp64_peak = measured.get("fp64") or nominal["fp64"]
     kernels = {}
     for name, d in (ktimes or {}).items():
         if d["launches"] == 0 or d["ms"] <= 0:
@@ -432,9 +465,12 @@ def run_ours(args, world, rank, local):
         roofline = {"kernel": kernel_names[dom], "bound": d["pipe"], "achieved": d["achieved"], "peak": d["peak"],
                     "unit": "TFLOP/s", "frac": d["frac"], "work": d["work"],
                     "ms_per_launch": d["ms_per_launch"], "launches_per_step": d["launches_per_step"],
-                    "peak_source": f"nominal {d['pipe'].upper()} pipe: 148 SM x {128 if d['pipe'] == 'fp32' else 64} "
-                                   f"lanes x 2 x {sm_mhz:.0f} MHz (no measured FP32/FP64 figure in "
-                                   "MEASURED_PEAKS.json; the kernels use no tensor cores)",
+                    "peak_source": (f"measured: cuBLAS {'DGEMM' if d['pipe'] == 'fp64' else 'SGEMM (TF32 off)'} "
+                                    "8192^3 on this GPU, best of 5 (MEASURED_PEAKS.json holds no FP32/FP64 vector "
+                                    "figure; the pair kernels use no tensor cores)"
+                                    if measured.get(d["pipe"]) else "nominal pipe rate (no measurement)"),
+                    "peak_nominal": nominal[d["pipe"]],
+                    "peaks_measured": measured,
                     "traffic": d.get("traffic_bytes_per_launch"),
                     "traffic_source": "ncu DRAM bytes per unit of the 64^3 capture, scaled to this launch's units"}
     result = {
@@ -461,8 +497,9 @@ def run_ours(args, world, rank, local):
                   "captures": gstats["captures"], "replays": gstats["replays"], "fallbacks": gstats["fallbacks"],
                   "kernels_per_replay": gstats["kernels_top"] + gstats["kernels_after"]
                   + gstats["kernels_per_iteration"] * st_mix["density_iterations"],
-                  "what": "value and fp64_value: restage + gz_hydro_pass(GZ_PASS_GRAPH) per step; pass_ms and the "
-                          "kernel rooflines: plain calls with events between the stages"},
+                  "what": "value and fp64_value: gz_hydro_pass(GZ_PASS_GRAPH | GZ_PASS_RESTAGE) per step (the "
+                          "restage and the pass in one graph); pass_ms and the kernel rooflines: plain calls with "
+                          "events between the stages"},
         "conservation": cons, "density_iterations": st_mix["density_iterations"], "pairs_symmetric": pairs_sym,
     }
     # the long tables go to stderr (the one stdout line stays short)
@@ -483,9 +520,11 @@ def run_ours(args, world, rank, local):
         pout_p = {k: t.data_ptr() for k, t in pout.items()}
 
         def pipelined(steps):
+            # the restage stays a call of its own here: it returns with its work
+            # queued, so the next step's upload is issued before this pass runs
             hpm.upload_raw_async(N, pin_p)
             for k in range(steps):
-                hpm.restage()
+                hpm.restage()  # takes step k's inputs
                 if k + 1 < steps:
                     hpm.upload_raw_async(N, pin_p)
                 hpm.hydro_pass(graph=True)
@@ -506,7 +545,7 @@ def run_ours(args, world, rank, local):
         d2h = sum(t.numel() * 8 for t in pout.values())
         result["e2e"] = {"value": world * N * Ke / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
                          "d2h_bytes_per_step": d2h, "steps": Ke,
-                         "how": "gz_upload_async / restage / gz_hydro_pass(GZ_PASS_GRAPH) / gz_download_async per "
+                         "how": "gz_upload_async / gz_restage / gz_hydro_pass(GZ_PASS_GRAPH) / gz_download_async per "
                                 "step from pinned host buffers, the next step's upload and the last step's download "
                                 "beside the pass; gz_wait after the last"}
     hpm.close()
@@ -752,7 +791,7 @@ def run_boxes(args):
     (seed 5; each a 3-D shock tube or a Sedov blast).
       * set: the boxes as one box set (gz_set_boxes) on one context: every
         kernel of a pass covers all boxes in one launch, and the pass runs as
-        one CUDA graph; K steps of restage + pass, device-resident inputs,
+        one CUDA graph with the restage; K steps, device-resident inputs,
         timed with CUDA events, and the same with the transfers (upload of the
         inputs, download of the rates) every step;
       * per_box: a pass per box on one context (upload, pass, download),
@@ -785,15 +824,13 @@ def run_boxes(args):
             hp.upload(cat["pos"], cat["vel"], cat["mass"], cat["u"], cat["dt"], cat["h"], cat["cond"])
             hp.full_pass()  # sizes the graph
             for _ in range(W):
-                hp.restage()
-                hp.hydro_pass(graph=True)
+                hp.hydro_pass(graph=True, restage=True)
             torch.cuda.synchronize()
             l0 = hp.status()["kernel_launches"]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(K):
-                hp.restage()
-                hp.hydro_pass(graph=True)
+                hp.hydro_pass(graph=True, restage=True)
             e1.record(stream)
             torch.cuda.synchronize()
             sec = e0.elapsed_time(e1) / 1e3 / K

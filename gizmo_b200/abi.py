@@ -146,6 +146,7 @@ EXPORTED_SYMBOLS = [
     "gz_hydro_pass", "gz_graph_stats", "gz_upload_async", "gz_download_async", "gz_wait", "gz_set_boxes",
 ]
 PASS_GRAPH = 1  # GZ_PASS_GRAPH
+PASS_RESTAGE = 2  # GZ_PASS_RESTAGE
 TIMEBINS = 60  # GZ_TIMEBINS
 NOALLOC_MAX_PARTICLES = 65536  # GZ_NOALLOC_MAX_PARTICLES
 DIAG_FLUX_ABS = 1  # GZ_DIAG_FLUX_ABS

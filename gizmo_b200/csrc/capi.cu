@@ -108,6 +108,7 @@ struct gz_context {
         std::vector<unsigned long long> sig;        // what the graph was captured for (buffers, sizes, settings)
         long long kernels_top = 0, kernels_loop = 0, kernels_sym = 0, kernels_tail = 0;
         long long rq_cap = 0;                       // refine-queue room the graph was captured with
+        bool with_restage = false;                  // the graph starts with the restage
         long long replays = 0, captures = 0, fallbacks = 0;
         bool capturing = false;                     // no timer events while a graph is captured
     } g;
@@ -629,10 +630,21 @@ int copy_stream(gz_context *c)
 
 // inputs of a pipelined upload become the resident ones: the context's stream
 // waits for their copies, and the buffers trade places (no copy)
-int take_pending_inputs(gz_context *c)
+int take_pending_inputs(gz_context *c, bool copy = false)
 {
     if (!c->in_pending) return 0;
     GZ_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in_done, 0));
+    if (copy) {  // into the resident buffers, which keep their addresses
+        const size_t N = (size_t)c->n;
+        struct { DevBuf *dst, *src; size_t k; } f[] = {
+            {&c->stage3, &c->p_stage3, 3}, {&c->o_vel, &c->p_vel, 3}, {&c->o_mass, &c->p_mass, 1},
+            {&c->o_u, &c->p_u, 1}, {&c->o_dt, &c->p_dt, 1}, {&c->o_h, &c->p_h, 1}, {&c->o_cond, &c->p_cond, 1}};
+        for (auto &e : f)
+            GZ_CUDA(c, cudaMemcpyAsync(e.dst->p, e.src->p, sizeof(double) * e.k * N, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+        c->in_pending = false;
+        return 0;
+    }
     std::swap(c->stage3, c->p_stage3);
     std::swap(c->o_vel, c->p_vel);
     std::swap(c->o_mass, c->p_mass);
@@ -753,6 +765,12 @@ int build_tree_levels(gz_context *c)
     return 0;
 }
 
+// nodes held for the octree of c->n particles (and its box sets)
+long long tree_cap(const gz_context *c)
+{
+    return std::max<long long>(4096, c->n / 4) + 2 * (long long)c->box_counts.size() + 64;
+}
+
 // Octree over the sorted keys, all levels on the device (tree_build_device)
 // with one read-back of the node count at the end, then boxes and h maxima
 // bottom-up. A tree larger than the nodes held for it (a few coincident
@@ -764,7 +782,7 @@ int build_tree(gz_context *c)
     c->t_nodes = 0;
     c->t_levels = 0;
     if (n == 0) return 0;
-    const long long cap = std::max<long long>(4096, n / 4) + 2 * (long long)c->box_counts.size() + 64;
+    const long long cap = tree_cap(c);
     if (cap > INT32_MAX) return fail(c, GZ_ERR_CAPACITY, "octree exceeds capacity");
     if (ensure(c, c->t_node, sizeof(int4) * (size_t)cap) || ensure(c, c->t_parent, sizeof(int) * (size_t)cap) ||
         ensure(c, c->t_build, sizeof(TreeBuild)))
@@ -852,6 +870,70 @@ int build_sym_rows(gz_context *c, int rows, bool all)
     }
     c->sym_rows = rows;
     c->sym_valid = true;
+    return 0;
+}
+
+// The octree built on the device with nothing read back: the bottom-up pass
+// covers the nodes held and stops at the count the build left on the device.
+int enqueue_tree_device(gz_context *c)
+{
+    const long long cap = tree_cap(c);
+    cudaStream_t s = c->stream;
+    tree_build_device(ptr<unsigned long long>(c->keys_sorted), c->n, ptr<int4>(c->t_node), ptr<int>(c->t_parent),
+                      ptr<TreeBuild>(c->t_build), (int)cap, c->leaf_max, c->box_bits / 3,
+                      c->box_bits ? ptr<int>(c->box_of) : nullptr, c->box_bits ? ptr<int>(c->root_of) : nullptr,
+                      c->sms * 8, s);
+    tree_up((int)cap, ptr<int4>(c->t_node), ptr<int>(c->t_parent), ptr<double>(c->x), ptr<double>(c->y),
+            ptr<double>(c->z), ptr<double>(c->h), ptr<double4>(c->t_lo), ptr<double4>(c->t_hi), ptr<int>(c->t_done), 1, s,
+            &ptr<TreeBuild>(c->t_build)->total);
+    GZ_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+// The restage's device work: status cleared, keys, sort, the sorted mirror
+// gathered from the resident inputs, outputs zeroed, the octree. in_graph (a
+// restage captured into the pass's graph): the tree is built without its
+// read-back (tree_build_device; the node count stays on the device and the
+// bottom-up pass runs over the nodes held).
+int enqueue_restage(gz_context *c, bool in_graph)
+{
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    GZ_CUDA(c, cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
+    if (n > 0) {
+        if (build_grid(c)) return c->err;
+        c->launches += 2;  // keys, inverse permutation
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        k_gather_inputs<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->stage3), ptr<double>(c->o_vel),
+                                               ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z),
+                                               ptr<double>(c->vx), ptr<double>(c->vy), ptr<double>(c->vz),
+                                               c->prm.box_size, ptr<DevStatus>(c->status));
+        c->launches += 1;
+        struct { DevBuf *src; DevBuf *dst; } one_in[] = {
+            {&c->o_mass, &c->m}, {&c->o_u, &c->u}, {&c->o_dt, &c->dt}, {&c->o_h, &c->h}, {&c->o_cond, &c->cond}};
+        for (auto &f : one_in) {
+            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(*f.src), ptr<double>(*f.dst));
+            c->launches += 1;
+        }
+        if (c->have_bins) {
+            k_gather_int<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->o_timebin), ptr<int>(c->timebin));
+            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->o_vsig), ptr<double>(c->vsig_prev));
+            GZ_CUDA(c, cudaMemsetAsync(c->wakeup.p, 0, sizeof(int) * (size_t)n, s));
+            c->launches += 2;
+        }
+        DevBuf *zero[] = {&c->num_ngb, &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig,
+                          &c->dtmass, &c->dmass};
+        for (DevBuf *b : zero) GZ_CUDA(c, cudaMemsetAsync(b->p, 0, sizeof(double) * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->nvt.p, 0, sizeof(double) * 6 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->pv.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->grad.p, 0, sizeof(double) * 15 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->accel.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->gw.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->fabs3.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        GZ_CUDA(c, cudaMemsetAsync(c->iters.p, 0, sizeof(int) * (size_t)n, s));
+        GZ_CUDA(c, cudaGetLastError());
+        if (in_graph ? enqueue_tree_device(c) : build_tree(c)) return c->err;
+    }
     return 0;
 }
 
@@ -1086,6 +1168,12 @@ __global__ void k_g_sym_check(GraphState *gs, const long long *total, long long 
     cudaGraphSetConditional(h, ok ? 1u : 0u);
 }
 
+// a restage captured into the graph: a tree that would overflow its nodes stops the pass
+__global__ void k_g_tree_check(const TreeBuild *tb, GraphState *gs)
+{
+    if (tb->fail) gs->fail |= kGraphFailTree;
+}
+
 int density_caps(const gz_context *c, int *cap0, int *cap1)
 {
     const double fs[2] = {kDensityBufferFirst, kDensityBuffer};
@@ -1103,7 +1191,7 @@ int density_caps(const gz_context *c, int *cap0, int *cap1)
 // (no error recorded) when the device has no room for them: the pass then
 // runs plain.
 constexpr int kNoRoom = -1;
-int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap)
+int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap, bool with_restage)
 {
     const int n = c->n;
     const size_t N = (size_t)std::max(n, 1);
@@ -1138,10 +1226,20 @@ int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap)
     }
     if (!try_ensure(c->pflux, pair_flux_bytes(mixed) * (size_t)sc)) return kNoRoom;
     if (mixed && !try_ensure(c->rq, sizeof(RefineItem) * (size_t)rq)) return kNoRoom;
-    size_t tmp = 0;
+    size_t tmp = 0, tmp_sort = 0;
     cub::DeviceScan::InclusiveSum(nullptr, tmp, ptr<long long>(c->s_counts), ptr<long long>(c->s_off) + 1, n,
                                   c->stream);
-    if (ensure(c, c->cub_tmp, tmp)) return c->err;
+    if (with_restage) {  // the restage's key sort and octree, sized before the capture
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, ptr<unsigned long long>(c->keys),
+                                        ptr<unsigned long long>(c->keys_sorted), ptr<int>(c->idx), ptr<int>(c->perm), n,
+                                        0, 63, c->stream);
+        const size_t cap = (size_t)tree_cap(c);
+        if (ensure(c, c->t_node, sizeof(int4) * cap) || ensure(c, c->t_parent, sizeof(int) * cap) ||
+            ensure(c, c->t_lo, sizeof(double4) * cap) || ensure(c, c->t_hi, sizeof(double4) * cap) ||
+            ensure(c, c->t_done, sizeof(int) * cap) || ensure(c, c->t_build, sizeof(TreeBuild)))
+            return c->err;
+    }
+    if (ensure(c, c->cub_tmp, std::max(tmp, tmp_sort))) return c->err;
     *sym_cap = std::min<long long>({sc, (long long)(c->s_nbr.bytes / sizeof(int)), (long long)(c->s_tmp.bytes / sizeof(int)),
                                     (long long)(c->pflux.bytes / pair_flux_bytes(mixed))});
     *rq_cap = rq;
@@ -1150,17 +1248,19 @@ int graph_buffers(gz_context *c, long long *sym_cap, long long *rq_cap)
 
 // what a captured graph depends on: every buffer's address and size, the
 // particle count, the pass settings
-std::vector<unsigned long long> graph_signature(gz_context *c)
+std::vector<unsigned long long> graph_signature(gz_context *c, bool with_restage)
 {
-    // the resident inputs, their pipelined copies and the download staging are
-    // read by the restage and the downloads only, never by the graph (and the
-    // pipelined upload swaps them every step)
-    const DevBuf *outside[] = {&c->stage3, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond,
-                               &c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond,
+    // the pipelined copies of the inputs and the download staging are never
+    // read by the graph; the resident inputs only by a restage in it (the
+    // pipelined upload swaps them every step when the restage is outside)
+    const DevBuf *outside[] = {&c->p_stage3, &c->p_vel, &c->p_mass, &c->p_u, &c->p_dt, &c->p_h, &c->p_cond,
                                &c->dstage, &c->dl};
+    const DevBuf *inputs[] = {&c->stage3, &c->o_vel, &c->o_mass, &c->o_u, &c->o_dt, &c->o_h, &c->o_cond};
     std::vector<unsigned long long> v;
+    v.push_back(with_restage ? 1 : 0);
     for (DevBuf *b : all_buffers(c)) {
         if (std::find(std::begin(outside), std::end(outside), b) != std::end(outside)) continue;
+        if (!with_restage && std::find(std::begin(inputs), std::end(inputs), b) != std::end(inputs)) continue;
         v.push_back((unsigned long long)(uintptr_t)b->p);
         v.push_back(b->bytes);
     }
@@ -1326,7 +1426,7 @@ int capture_gradients_force(gz_context *c, cudaStream_t s, long long rq_cap)
 }
 
 // Captures the pass into c->g (graph_buffers has sized everything it uses).
-int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
+int graph_capture(gz_context *c, long long sym_cap, long long rq_cap, bool with_restage)
 {
     graph_release(c);
     for (auto &b : c->g.body)
@@ -1356,7 +1456,16 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
         if (e != cudaSuccess) return fail(c, GZ_ERR_CUDA, cudaGetErrorString(e));
         return 0;
     };
+    long long restage_kernels = 0;
     do {
+        k_g_init<<<1, 1, 0, s>>>(ptr<GraphState>(c->gstate), n);
+        if (with_restage) {  // the restage first, its tree with nothing read back
+            const long long l0 = c->launches;
+            if ((rc = enqueue_restage(c, true))) break;
+            k_g_tree_check<<<1, 1, 0, s>>>(ptr<TreeBuild>(c->t_build), ptr<GraphState>(c->gstate));
+            restage_kernels = c->launches - l0 + 1 + 2 * 22 + 1 + 1;  // + tree build, bottom-up pass, check
+            if ((rc = check_last(c, "restage"))) break;
+        }
         // the inputs a plain pass would restart from
         cudaMemcpyAsync(c->g_hseed.p, c->h.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(c->g_cseed.p, c->cond.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
@@ -1368,7 +1477,6 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
                                                        ptr<unsigned long long>(c->hmax));
         cudaMemcpyAsync(c->todo_a.p, c->targets.p, sizeof(int) * N, cudaMemcpyDeviceToDevice, s);
         density_pack(ps, ptr<DensRec>(c->rec), s);
-        k_g_init<<<1, 1, 0, s>>>(ptr<GraphState>(c->gstate), n);
         if ((rc = check_last(c, "density setup"))) break;
         if ((rc = make_handle(c, s, &h_loop, 1))) break;
         if ((rc = add_conditional(c, s, h_loop, cudaGraphCondTypeWhile, &body_loop))) break;
@@ -1407,7 +1515,7 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
     // the selection's three steps, next; the rows' split, counts and check;
     // scatter, sort, the gradient pack and rows, the force preloop, pack,
     // pairs, (refine,) gather, finish
-    c->g.kernels_top = 7;
+    c->g.kernels_top = 7 + restage_kernels;
     c->g.kernels_loop = 15;
     c->g.kernels_sym = 3;
     c->g.kernels_tail = c->prm.precision == GZ_PRECISION_MIXED ? 10 : 9;
@@ -1422,6 +1530,7 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
     }
     if (check_last(c, "instantiation")) { graph_release(c); return c->err; }
     c->g.rq_cap = rq_cap;
+    c->g.with_restage = with_restage;
     c->g.captures++;
     return 0;
 }
@@ -1429,46 +1538,65 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap)
 // One replay of the captured pass; a buffer overflow (or more fragile pairs
 // than the refine queue holds) is answered by the plain pass from the
 // graph's starting kernel lengths and condition numbers.
-int graph_pass(gz_context *c)
+int graph_pass(gz_context *c, bool with_restage)
 {
     cudaStream_t s = c->stream;
     const int n = c->n;
-    long long sym_cap = 0, rq_cap = 0;
-    const int room = graph_buffers(c, &sym_cap, &rq_cap);
-    if (room == kNoRoom) {  // no room for the graph's buffers: the plain pass
-        int rc = gz_hydro_density(c, nullptr, 0);
+    auto plain = [&]() -> int {
+        int rc = with_restage ? gz_restage(c) : 0;
+        if (!rc) rc = gz_hydro_density(c, nullptr, 0);
         if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
         if (!rc) rc = gz_hydro_force(c, nullptr, 0);
         return rc;
-    }
+    };
+    long long sym_cap = 0, rq_cap = 0;
+    const int room = graph_buffers(c, &sym_cap, &rq_cap, with_restage);
+    if (room == kNoRoom) return plain();  // no room for the graph's buffers
     if (room) return room;
-    std::vector<unsigned long long> sig = graph_signature(c);
+    if (with_restage) {
+        // the graph reads the resident inputs at their addresses: inputs of a
+        // pipelined upload are copied into them rather than swapped in
+        if (take_pending_inputs(c, true)) return c->err;
+        c->fabs_valid = false;
+        c->err = 0;
+        c->err_index = -1;
+        c->msg[0] = 0;
+    }
+    std::vector<unsigned long long> sig = graph_signature(c, with_restage);
     if (!c->g.exec || sig != c->g.sig) {
-        if (graph_capture(c, sym_cap, rq_cap)) return c->err;
+        if (graph_capture(c, sym_cap, rq_cap, with_restage)) return c->err;
         c->g.sig = sig;
     }
     if (check_last(c, "before the launch")) return c->err;
     GZ_CUDA(c, cudaGraphLaunch(c->g.exec, s));
     GraphState gs{};
+    TreeBuild tb{};
     unsigned long long refined = 0, hbits = 0;
     const int mixed = c->prm.precision == GZ_PRECISION_MIXED;
     GZ_CUDA(c, cudaMemcpyAsync(&gs, c->gstate.p, sizeof(gs), cudaMemcpyDeviceToHost, s));
     GZ_CUDA(c, cudaMemcpyAsync(&hbits, c->hmax.p, sizeof(hbits), cudaMemcpyDeviceToHost, s));
     if (mixed) GZ_CUDA(c, cudaMemcpyAsync(&refined, c->refined.p, sizeof(refined), cudaMemcpyDeviceToHost, s));
+    if (with_restage) GZ_CUDA(c, cudaMemcpyAsync(&tb, c->t_build.p, sizeof(tb), cudaMemcpyDeviceToHost, s));
     GZ_CUDA(c, cudaStreamSynchronize(s));
     if (check_last(c, "graph launch")) return c->err;
     c->g.replays++;
+    if (with_restage) {
+        c->t_nodes = tb.total;
+        c->t_levels = tb.L;
+        c->grid_valid = true;
+        c->have_density = c->have_gradients = false;
+        c->sym_valid = false;
+        c->dens_all = false;
+    }
     const bool converged = gs.todo_left == 0 && !gs.fail;
     c->launches += c->g.kernels_top + c->g.kernels_loop * gs.iter + (converged ? c->g.kernels_sym : 0) +
                    ((converged && !(gs.fail & kGraphFailSym)) ? c->g.kernels_tail : 0);
     if (gs.fail || (long long)refined > c->g.rq_cap) {
         c->g.fallbacks++;
+        if (with_restage) return plain();  // the restage starts again from the resident inputs
         GZ_CUDA(c, cudaMemcpyAsync(c->h.p, c->g_hseed.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
         GZ_CUDA(c, cudaMemcpyAsync(c->cond.p, c->g_cseed.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-        int rc = gz_hydro_density(c, nullptr, 0);
-        if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
-        if (!rc) rc = gz_hydro_force(c, nullptr, 0);
-        return rc;
+        return plain();
     }
     c->last_iters = gs.iter;
     c->d_used = gs.base;
@@ -1592,47 +1720,11 @@ int gz_kernel_time(gz_context *c, int timer, double *ms, int64_t *launches, int6
 // outputs, tree.
 static int stage_inputs(gz_context *c)
 {
-    const int n = c->n;
-    cudaStream_t s = c->stream;
     c->fabs_valid = false;
-    GZ_CUDA(c, cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
     c->err = 0;
     c->err_index = -1;
     c->msg[0] = 0;
-    if (n > 0) {
-        if (build_grid(c)) return c->err;
-        c->launches += 2;  // keys, inverse permutation
-        const unsigned blocks = (unsigned)((n + 255) / 256);
-        k_gather_inputs<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->stage3), ptr<double>(c->o_vel),
-                                               ptr<double>(c->x), ptr<double>(c->y), ptr<double>(c->z),
-                                               ptr<double>(c->vx), ptr<double>(c->vy), ptr<double>(c->vz),
-                                               c->prm.box_size, ptr<DevStatus>(c->status));
-        c->launches += 1;
-        struct { DevBuf *src; DevBuf *dst; } one_in[] = {
-            {&c->o_mass, &c->m}, {&c->o_u, &c->u}, {&c->o_dt, &c->dt}, {&c->o_h, &c->h}, {&c->o_cond, &c->cond}};
-        for (auto &f : one_in) {
-            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(*f.src), ptr<double>(*f.dst));
-            c->launches += 1;
-        }
-        if (c->have_bins) {
-            k_gather_int<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<int>(c->o_timebin), ptr<int>(c->timebin));
-            k_gather1<<<blocks, 256, 0, s>>>(n, ptr<int>(c->perm), ptr<double>(c->o_vsig), ptr<double>(c->vsig_prev));
-            GZ_CUDA(c, cudaMemsetAsync(c->wakeup.p, 0, sizeof(int) * (size_t)n, s));
-            c->launches += 2;
-        }
-        DevBuf *zero[] = {&c->num_ngb, &c->drkern, &c->divvel, &c->rho, &c->pressure, &c->fce, &c->dudt, &c->vsig,
-                          &c->dtmass, &c->dmass};
-        for (DevBuf *b : zero) GZ_CUDA(c, cudaMemsetAsync(b->p, 0, sizeof(double) * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->nvt.p, 0, sizeof(double) * 6 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->pv.p, 0, sizeof(double) * 3 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->grad.p, 0, sizeof(double) * 15 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->accel.p, 0, sizeof(double) * 3 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->gw.p, 0, sizeof(double) * 3 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->fabs3.p, 0, sizeof(double) * 3 * (size_t)n, s));
-        GZ_CUDA(c, cudaMemsetAsync(c->iters.p, 0, sizeof(int) * (size_t)n, s));
-        GZ_CUDA(c, cudaGetLastError());
-        if (build_tree(c)) return c->err;
-    }
+    if (enqueue_restage(c, false)) return c->err;
     c->grid_valid = true;
     c->have_density = c->have_gradients = false;
     c->sym_valid = false;
@@ -1993,14 +2085,16 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
 
 int gz_hydro_pass(gz_context *c, int flags)
 {
-    if (!c || (flags & ~GZ_PASS_GRAPH)) return GZ_ERR_ARG;
+    if (!c || (flags & ~(GZ_PASS_GRAPH | GZ_PASS_RESTAGE))) return GZ_ERR_ARG;
     cudaSetDevice(c->device);
     if (!c->grid_valid) return fail(c, GZ_ERR_ORDER, "pass before upload");
+    const bool restage = (flags & GZ_PASS_RESTAGE) != 0;
     // the graph needs the counts of a plain pass to size its buffers, and the
     // kernel timers need plain launches
     const bool graph = (flags & GZ_PASS_GRAPH) && c->n > 0 && c->pairs_symmetric > 0 && !c->timing;
-    if (graph) return graph_pass(c);
-    int rc = gz_hydro_density(c, nullptr, 0);
+    if (graph) return graph_pass(c, restage);
+    int rc = restage ? gz_restage(c) : 0;
+    if (!rc) rc = gz_hydro_density(c, nullptr, 0);
     if (!rc) rc = gz_hydro_gradients(c, nullptr, 0);
     if (!rc) rc = gz_hydro_force(c, nullptr, 0);
     return rc;

@@ -133,5 +133,6 @@ struct GraphState {
 // Fail reasons (GraphState::fail, bit flags).
 constexpr int kGraphFailRows = 1;   // padded density rows beyond the row buffer
 constexpr int kGraphFailSym = 2;    // symmetric rows beyond their buffers or the pair-flux buffer
+constexpr int kGraphFailTree = 4;   // a restage in the graph: the octree beyond its nodes
 
 }  // namespace gz

@@ -222,11 +222,13 @@ class HydroPass:
         self.hydro_gradient_calc(active)
         self.hydro_force(active)
 
-    def hydro_pass(self, graph: bool = True):
+    def hydro_pass(self, graph: bool = True, restage: bool = False):
         """density -> gradients -> force over every particle in one call
         (gz_hydro_pass); with graph=True as one CUDA graph once a plain pass
-        has sized its buffers. Results equal full_pass()'s."""
-        self._check(self.lib.gz_hydro_pass(self._ctx, abi.PASS_GRAPH if graph else 0))
+        has sized its buffers; with restage=True the restage first (in the
+        graph). Results equal full_pass()'s (after restage())."""
+        flags = (abi.PASS_GRAPH if graph else 0) | (abi.PASS_RESTAGE if restage else 0)
+        self._check(self.lib.gz_hydro_pass(self._ctx, flags))
 
     def set_boxes(self, counts=None):
         """Box sets (gz_set_boxes): the next uploads hold len(counts) consecutive

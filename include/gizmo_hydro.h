@@ -193,6 +193,10 @@ int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
  * would overflow, the call runs the plain pass from the same inputs
  * (gz_graph_stats counts those). Kernel timing (gz_kernel_timing) runs plain. */
 #define GZ_PASS_GRAPH 1
+/* GZ_PASS_RESTAGE: the pass starts with gz_restage (inside the graph with
+ * GZ_PASS_GRAPH, the octree then built on the device with nothing read back;
+ * a pipelined upload is copied into the resident inputs instead of swapped). */
+#define GZ_PASS_RESTAGE 2
 int gz_hydro_pass(gz_context *ctx, int flags);
 
 /* Box sets: the particles of the following uploads are n_boxes consecutive

@@ -88,3 +88,34 @@ def test_graph_falls_back_to_plain_pass():
         g = hp.graph_stats()
         assert g["captures"] == 2 and g["replays"] == 2 and g["fallbacks"] == 1, g
         _same(hp.download(FIELDS), ref)
+
+
+@pytest.mark.parametrize("case", ["plummer32_mfv", "sedov24_mfm"])
+def test_graph_with_restage_equals_plain(case):
+    """GZ_PASS_RESTAGE: the restage (keys, sort, mirror, octree built on the
+    device with nothing read back) captured at the start of the graph: the
+    step's results equal restage() + the three plain calls, with box sets too."""
+    wl = CASES[case](abi.PRECISION_MIXED)
+    ref = _plain(wl)
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.hydro_pass(graph=True, restage=True)  # plain: sizes
+        _same(hp.download(FIELDS), ref)
+        for k in range(2):
+            hp.hydro_pass(graph=True, restage=True)
+            g = hp.graph_stats()
+            assert g["captures"] == 1 and g["replays"] == k + 1 and g["fallbacks"] == 0, g
+            _same(hp.download(FIELDS), ref)
+    # two copies of the set as a box set of two boxes: each box's outputs equal the set's alone
+    two = {k: np.concatenate([np.asarray(getattr(wl, k))] * 2) for k in ("pos", "vel", "mass", "u", "dt", "h", "cond")}
+    with HydroPass(wl.params) as hp:
+        hp.set_boxes([wl.n, wl.n])
+        hp.upload(two["pos"], two["vel"], two["mass"], two["u"], two["dt"], two["h"], two["cond"])
+        hp.hydro_pass(graph=True, restage=True)
+        plain = hp.download(FIELDS)
+        hp.hydro_pass(graph=True, restage=True)
+        graph = hp.download(FIELDS)
+        assert hp.graph_stats()["replays"] == 1
+    for f in FIELDS:
+        assert np.array_equal(graph[f], plain[f]), f
+        assert np.array_equal(plain[f][:wl.n], plain[f][wl.n:]), f
