@@ -1519,7 +1519,6 @@ int graph_capture(gz_context *c, long long sym_cap, long long rq_cap, bool with_
     c->g.kernels_loop = 15;
     c->g.kernels_sym = 3;
     c->g.kernels_tail = c->prm.precision == GZ_PRECISION_MIXED ? 10 : 9;
-    (void)body_loop;
     const cudaError_t ie = cudaGraphInstantiate(&c->g.exec, g, 0);
     if (ie != cudaSuccess) {
         char b[200];

@@ -76,7 +76,10 @@ def _rank(rank, world, port, h, q, engine_kind="oracle"):
         owner = halo.domain_owner(inputs["pos"], wl.params.box_size, world)
         gid = np.nonzero(owner == rank)[0]
         mine = {k: np.asarray(v)[gid] for k, v in inputs.items()}
-        engine = _oracle_engine if engine_kind == "oracle" else _FirstIterationTooLong()
+        if engine_kind == "gpu":
+            engine = halo.hydro_pass_engine(0)
+        else:
+            engine = _oracle_engine if engine_kind == "oracle" else _FirstIterationTooLong()
         hp = halo.HaloPass(wl.params, halo.Exchange(rank, world), engine)
         out = hp(gid, mine)
         q.put((rank, gid, out, hp.last_radius, hp.last_imported, hp.last_h_iter_max))
@@ -154,3 +157,44 @@ def test_long_intermediate_kernel_length_redoes_the_pass():
                 np.testing.assert_allclose(a, b, rtol=0, atol=1e-14 * np.abs(ref[f]).max())
             else:
                 assert np.array_equal(a, b), (rank, f)
+
+
+@pytest.mark.gpu
+def test_domains_on_the_gpu_engine_equal_one_domain():
+    """The GPU engine (hydro_pass_engine: a HydroPass per rank over the C ABI,
+    density / gradients / force on the rank's active lists) in two gloo ranks
+    that share one GPU: the ranks exchange on the host, so no kernel of one
+    waits on the other's. Against one GPU pass over the whole set, FP64 form:
+    the parity tolerances of tests/test_gpu_parity.py (the active lists change
+    the lanes per row, so the sums run in another order)."""
+    from gizmo_b200.hydro import HydroPass
+    from tests._util import DENSITY_FIELDS, FORCE_FIELDS, GRADIENT_FIELDS, field_err
+    wl = _workload()
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.density()
+        wl.h = hp.download(["h"])["h"].copy()  # converged lengths, as a step after the first starts from
+    with HydroPass(wl.params) as hp:
+        hp.upload_workload(wl)
+        hp.full_pass()
+        ref = hp.download()
+    got = _run_ranks(wl.h, 2, engine_kind="gpu")
+    covered = np.zeros(wl.n, dtype=int)
+    for rank, gid, out, radius, imported, h_iter_max in got:
+        covered[gid] += 1
+        assert imported < wl.n - len(gid)
+        assert h_iter_max <= radius / 2
+        h_rel = np.abs(np.asarray(out["h"]) - ref["h"][gid]) / ref["h"][gid]
+        same = (np.asarray(out["iters"]) == ref["iters"][gid]) & (h_rel <= 1e-10)
+        assert same.mean() >= 0.999 and h_rel.max() <= 3e-3, (same.mean(), h_rel.max())
+        keep = np.flatnonzero(same)
+        for f in DENSITY_FIELDS + GRADIENT_FIELDS:
+            assert field_err(f, np.asarray(out[f])[keep], ref[f][gid][keep], 1e-6) < 1e-10, (rank, f)
+        if same.all():
+            for f in FORCE_FIELDS:
+                if f == "dmass":
+                    continue
+                assert field_err(f, np.asarray(out[f]), ref[f][gid], 1e-3) < 1e-10, (rank, f)
+            np.testing.assert_allclose(np.asarray(out["dmass"]), ref["dmass"][gid], rtol=0,
+                                       atol=1e-12 * np.abs(ref["dmass"]).max())
+    assert (covered == 1).all()
