@@ -19,6 +19,15 @@
 //  * pow: exp(y log x) in double-double; y = 3, 2 and -1 are exact products
 //    or a quotient rounded once.
 //
+// Each function first takes a shorter evaluation (Ziv's strategy: Ziv,
+// "Fast evaluation of elementary mathematical functions with correctly
+// rounded last bit", ACM TOMS 17(3), 1991): the same reduction with the
+// series from its cubic term on in double, accurate to 2^-70 of the result,
+// rounded once when that error bound proves the rounding (the value lies
+// farther than the bound from the midpoint between two doubles); otherwise
+// the ~2^-100 evaluation above decides. Both give the correctly rounded
+// result, so the shorter one changes no output, only the time.
+//
 // Every operation is an explicitly rounded add/mul/fma, so no contraction can
 // change a result, and the host build of this header (CPU tests) computes
 // the same bits as the device.
@@ -196,10 +205,8 @@ static const double kExp2TableHost[64][2] = GZ_CR_EXP2_TABLE;
 // |r| <= ln2 / 128, e^a = 2^m 2^(j/64) e^r. expm1(r) is a Taylor series whose
 // first five terms are summed in double-double and whose terms from r^6 on
 // (below 1e-15 relative) in double, Horner form throughout; accuracy ~2^-100.
-CR_HD dd dd_exp(dd a)
+CR_HD dd dd_exp_core(dd a, int &m)  // e^a = (result) 2^m, result in [0.98, 2.03]
 {
-    if (a.hi > 709.7) return {INFINITY, 0.0};
-    if (a.hi < -745.2) return {0.0, 0.0};
     const double N = ::rint(mul(a.hi, kInv64Ln2));
     dd nl = two_prod(N, kLn2Hi64);
     nl.lo = add(nl.lo, mul(N, kLn2Lo64));
@@ -221,39 +228,146 @@ CR_HD dd dd_exp(dd a)
     s = dd_add(dd_mul(s, r), {1.0, 0.0});
     const dd p = dd_mul(s, r);  // expm1(r)
     const int Ni = (int)N;
-    const int j = Ni & 63, m = (Ni - j) >> 6;
+    const int j = Ni & 63;
+    m = (Ni - j) >> 6;
 #ifdef __CUDA_ARCH__
     const dd t = {kExp2TableDev[j][0], kExp2TableDev[j][1]};
 #else
     const dd t = {kExp2TableHost[j][0], kExp2TableHost[j][1]};
 #endif
-    dd e = dd_add(t, dd_mul(t, p));
+    return dd_add(t, dd_mul(t, p));
+}
+
+CR_HD dd dd_exp(dd a)
+{
+    if (a.hi > 709.7) return {INFINITY, 0.0};
+    if (a.hi < -745.2) return {0.0, 0.0};
+    int m = 0;
+    dd e = dd_exp_core(a, m);
     e.hi = ::ldexp(e.hi, m);
     e.lo = ::ldexp(e.lo, m);
     return e;
+}
+
+// e^a rounded once: the sum is rounded before the scaling by 2^m, which is
+// exact for a normal result (scaling the low part first would drop its bits
+// once it falls below the normal range, from results of ~2^-969 down)
+CR_HD double exp_rounded(dd a)
+{
+    if (a.hi > 709.7) return INFINITY;
+    if (a.hi < -745.2) return 0.0;
+    int m = 0;
+    const dd e = dd_exp_core(a, m);
+    return ::ldexp(add(e.hi, e.lo), m);
 }
 
 // log(x) for finite x > 0, as a double-double
 CR_HD dd dd_log(double x)
 {
     const double y0 = ::log(x);
-    const dd e = dd_exp({-y0, 0.0});
-    const dd t = dd_mul_d(e, x);
+    int m = 0;
+    const dd e = dd_exp_core({-y0, 0.0}, m);      // e^-y0 = e 2^m
+    const dd t = dd_mul_d(e, ::ldexp(x, m));      // x 2^m ~ 1/e: exact
     const dd u = dd_add(t, {-1.0, 0.0});
     return dd_add({y0, 0.0}, u);
 }
 
 CR_HD double round_dd(dd a) { return add(a.hi, a.lo); }
 
+// ------------------------------------------------------- the shorter evaluation
+// Spacing of the doubles just below v (normal, v > 0): half the ulp of v when
+// v is a power of two, its ulp otherwise. A value within half of it of v, on
+// either side, rounds to v.
+CR_HD double gap_below(double v)
+{
+    int e = 0;
+    const double f = ::frexp(v, &e);  // v = f 2^e, f in [0.5, 1)
+    return ::ldexp(f == 0.5 ? 0.5 : 1.0, e - 53);
+}
+
+// Whether hi + lo (|lo| <= half the spacing at hi, hi > 0 normal), known to
+// within err of the exact value, rounds to hi.
+CR_HD bool rounds_to_hi(double hi, double lo, double err) { return add(::fabs(lo), err) < mul(0.5, gap_below(hi)); }
+
+// e^(a.hi + a.lo) = (hi + lo) 2^m for |a.hi| <= 708, |a.lo| <= 2^-40 |a.hi| + 2^-60,
+// with |hi + lo - e^a 2^-m| <= 2^-72 hi and hi in [0.98, 2.03]:
+//  * the reduction of dd_exp (r = a - N ln2/64 as rh + rl, |rh| <= 0.0055);
+//  * expm1(r) = rh + rh^2/2 (rh^2 exact) + rh^3 P(rh) + rl (1 + rh + rh^2/2),
+//    P the Taylor series of (e^r - 1 - r - r^2/2) / r^3 to r^5 / 8! (the
+//    truncation is below 2^-85), in double: its rounding, below
+//    5 x 2^-53 x rh^3/6 <= 2^-75.8, dominates;
+//  * 2^(j/64) (1 + p) from the double-double table with one exact product and
+//    sum, the small terms in double (their rounding below 2^-75).
+CR_HD dd exp_short(dd a, int &m)
+{
+    const double N = ::rint(mul(a.hi, kInv64Ln2));
+    dd nl = two_prod(N, kLn2Hi64);
+    nl.lo = add(nl.lo, mul(N, kLn2Lo64));
+    dd r = two_sum(a.hi, -nl.hi);
+    r.lo = add(sub(r.lo, nl.lo), a.lo);
+    r = two_sum(r.hi, r.lo);  // r.hi may be the smaller part when a lies near N ln2/64
+    const double rh = r.hi, rl = r.lo;
+    double q = 2.48015873015873015873e-05;           // 1/8!
+    q = add(mul(q, rh), 1.98412698412698412698e-04);  // 1/7!
+    q = add(mul(q, rh), 1.38888888888888888889e-03);  // 1/6!
+    q = add(mul(q, rh), 8.33333333333333333333e-03);  // 1/5!
+    q = add(mul(q, rh), 4.16666666666666666667e-02);  // 1/4!
+    q = add(mul(q, rh), 1.66666666666666666667e-01);  // 1/3!
+    const dd s2 = two_prod(rh, rh);
+    const double cub = mul(mul(s2.hi, rh), q);
+    const double tail = mul(rl, add(1.0, mul(rh, add(1.0, mul(0.5, rh)))));
+    const dd p0 = two_sum(rh, mul(0.5, s2.hi));
+    const double ph = p0.hi, pl = add(p0.lo, add(mul(0.5, s2.lo), add(cub, tail)));
+    const int Ni = (int)N;
+    const int j = Ni & 63;
+    m = (Ni - j) >> 6;
+#ifdef __CUDA_ARCH__
+    const double th = kExp2TableDev[j][0], tl = kExp2TableDev[j][1];
+#else
+    const double th = kExp2TableHost[j][0], tl = kExp2TableHost[j][1];
+#endif
+    const dd tp = two_prod(th, ph);
+    const dd sum = two_sum(th, tp.hi);
+    const double lo = add(sum.lo, add(tp.lo, add(tl, add(mul(th, pl), mul(tl, ph)))));
+    return quick_two_sum(sum.hi, lo);
+}
+
+constexpr double kShortErr = 0x1p-70;  // relative error bound of exp_short, with margin
+
+// log(x) as Lh + Ll within 2^-71 absolute, for normal x with |log x| <= 708:
+// one Newton step from the library log y0 (within a few ulp), L = y0 + u -
+// u^2/2 with u = x e^-y0 - 1 (|u| < 2^-40), e^-y0 from exp_short.
+CR_HD dd log_short(double x)
+{
+    const double y0 = ::log(x);
+    int m = 0;
+    const dd E = exp_short({-y0, 0.0}, m);
+    const double xs = ::ldexp(x, m);  // x 2^m ~ 1 / E: exact (normal)
+    const dd t = two_prod(xs, E.hi);
+    const double u0 = sub(t.hi, 1.0);  // exact: t.hi lies within 2^-39 of 1
+    const double u = add(u0, add(t.lo, mul(xs, E.lo)));
+    return two_sum(y0, sub(u, mul(0.5, mul(u, u))));
+}
+
 CR_HD double exp(double x)
 {
     if (!(x == x)) return x;
-    return round_dd(dd_exp({x, 0.0}));
+    if (::fabs(x) <= 708.0) {
+        int m = 0;
+        const dd e = exp_short({x, 0.0}, m);
+        if (rounds_to_hi(e.hi, e.lo, mul(kShortErr, e.hi))) return ::ldexp(e.hi, m);
+    }
+    return exp_rounded({x, 0.0});
 }
 
 CR_HD double log(double x)
 {
     if (!(x > 0.0) || x == INFINITY) return ::log(x);
+    if (x >= 0x1p-1020 && x <= 0x1p1020 && x != 1.0) {
+        const dd L = log_short(x);
+        if (L.hi != 0.0 && rounds_to_hi(::fabs(L.hi), ::fabs(L.hi) == L.hi ? L.lo : -L.lo, 0x1p-71))
+            return L.hi;
+    }
     return round_dd(dd_log(x));
 }
 
@@ -264,7 +378,20 @@ CR_HD double pow(double x, double y)
     if (y == -1.0) return div_(1.0, x);
     if (y == 1.0) return x;
     if (!(x > 0.0) || x == INFINITY || !(y == y) || y == INFINITY || y == -INFINITY) return ::pow(x, y);
-    return round_dd(dd_exp(dd_mul_d(dd_log(x), y)));
+    if (x >= 0x1p-1020 && x <= 0x1p1020 && ::fabs(y) <= 16.0) {
+        // z = y log x within |y| 2^-71 + 2^-100 |z|; e^z within 2^-72 of itself
+        const dd L = log_short(x);
+        dd z = two_prod(y, L.hi);
+        z.lo = add(z.lo, mul(y, L.lo));
+        z = quick_two_sum(z.hi, z.lo);
+        if (::fabs(z.hi) <= 708.0) {
+            int m = 0;
+            const dd e = exp_short(z, m);
+            const double err = mul(e.hi, add(kShortErr, mul(add(::fabs(y), 1.0), 0x1p-70)));
+            if (rounds_to_hi(e.hi, e.lo, err)) return ::ldexp(e.hi, m);
+        }
+    }
+    return exp_rounded(dd_mul_d(dd_log(x), y));
 }
 
 }  // namespace cr
