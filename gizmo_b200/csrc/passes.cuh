@@ -480,23 +480,41 @@ __global__ void __launch_bounds__(128) k_force(PassParams p, Particles ps, const
         const long long b0 = rows.off[slot], b1 = rows.off[slot + 1];
         long long e = b0 + lane;
         int jn = e < b1 ? rows.nbr[e] : 0;
+        // kGather: the next entry's flux and neighbour record are in flight
+        // while this entry is accumulated, its index one entry further ahead
+        PairFlux<T> Fn{};
+        GatherRec gn{};
+        int jnn = 0;
+        if (MODE == kGather) {
+            if (e < b1) {
+                Fn = flux[e];
+                if (mfv) gn = grec[jn];
+            }
+            jnn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;
+        }
         for (; e < b1; e += TPT) {
             const int j = jn;
-            jn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;  // the next index is in flight during this entry
             PairFlux<T> F;
             double mj, dtj, dx, dy, dz;
             int j_active;
             if (MODE == kGather) {
-                F = flux[e];  // valid only if both particles have mass and density
+                F = Fn;  // valid only if both particles have mass and density
+                const GatherRec g = gn;
+                jn = jnn;
+                if (e + TPT < b1) {
+                    Fn = flux[e + TPT];
+                    if (mfv) gn = grec[jn];
+                }
+                jnn = e + 2 * TPT < b1 ? rows.nbr[e + 2 * TPT] : 0;
                 if (!F.valid) continue;
                 if (mfv) {  // only the MFV bookkeeping reads the neighbour
-                    const GatherRec g = grec[j];
                     mj = g.m;
                     dtj = g.dt;
                     j_active = g.active;
                     sep2(xi, yi, zi, g.x, g.y, g.z, p.box, p.half, dx, dy, dz);
                 }
             } else {
+                jn = e + TPT < b1 ? rows.nbr[e + TPT] : 0;  // the next index is in flight during this entry
                 const ForceRec<T> *rjp = rec + j;
                 mj = rjp->m;
                 const double rhoj = rjp->rho;
