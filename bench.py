@@ -385,6 +385,14 @@ def run_ours(args, world, rank, local):
         cons[tag] = {"momentum": float(np.abs(mom.sum(0)).max() / np.abs(mom).sum()),
                      "mass": float(abs(dtm.sum()) / (np.abs(dtm).sum() + 1e-300))}
 
+    # Accepted pairs per density row: the one-way rows (r < h at the converged
+    # h, the target itself included, as the density sums count it) of a random
+    # sample of targets. The density sums' algorithmic work is this count x 72
+    # flop per row summed; the candidates the row radius adds are not work.
+    sample = np.sort(np.random.default_rng(17).choice(N, min(N, 1 << 16), replace=False)).astype(np.int32)
+    off_s, _ = hpm.neighbors(0, sample)
+    accepted_per_row = float(off_s[-1]) / len(sample)
+
     # Cold seed: one mixed-form pass from the generator's h seed (octree density
     # estimate, h0 = (3 DesNumNgb / (4 pi n_local))^(1/3)), timed once after the
     # steady-state runs. Its density runs in slices of 2,097,152 particles (a
@@ -419,10 +427,10 @@ def run_ours(args, world, rank, local):
 
     # Roofline of each timed kernel family (CUDA events around its launches on
     # the context's stream, over the timed steps of the mixed form): algorithmic
-    # FLOPs / kernel time against the nominal rate of the pipe its arithmetic
-    # runs on. None of these kernels is a contraction (no tensor cores) or
-    # DRAM-bound (the gathers hit L1/L2: see `traffic`); MEASURED_PEAKS.json
-    # holds no FP32/FP64 vector figure, so the peaks are nominal.
+    # FLOPs / kernel time against the rate of the pipe its arithmetic runs on,
+    # measured here as cuBLAS DGEMM / SGEMM (MEASURED_PEAKS.json holds no
+    # FP32/FP64 vector figure). None of these kernels is a contraction (no
+    # tensor cores) or DRAM-bound (the gathers hit L1/L2: see `traffic`).
     pairs_sym = st_mix["pairs_symmetric"]
     peaks = {}
     try:
@@ -440,9 +448,10 @@ def run_ours(args, world, rank, local):
         e = {"launches_per_step": d["launches"] / K64, "ms_per_step": d["ms"] / K64,
              "ms_per_launch": d["ms"] / d["launches"], "units_per_launch": d["units"] / d["launches"]}
         flops = None
-        if name == "density_sums":  # FP64; a converged row holds ~DesNumNgb accepted pairs
-            flops, peak, pipe = FLOPS_PER_PAIR["density"] * p.des_num_ngb * d["units"], fp64_peak, "fp64"
-            e["work"] = f"{FLOPS_PER_PAIR['density']:.0f} flop x DesNumNgb ({p.des_num_ngb:.0f}) pairs per row"
+        if name == "density_sums":  # FP64, accepted pairs only
+            flops, peak, pipe = FLOPS_PER_PAIR["density"] * accepted_per_row * d["units"], fp64_peak, "fp64"
+            e["work"] = (f"{FLOPS_PER_PAIR['density']:.0f} flop x {accepted_per_row:.2f} accepted pairs per row "
+                         f"(one-way rows at the converged h of {len(sample)} random targets, self included)")
         elif name == "force":  # FP32 pair arithmetic, each pair evaluated once
             flops, peak, pipe = FLOPS_PER_PAIR["force"] * d["units"], fp32_peak, "fp32"
             e["work"] = f"{FLOPS_PER_PAIR['force']:.0f} flop per pair evaluation"
