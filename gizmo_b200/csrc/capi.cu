@@ -1875,6 +1875,14 @@ int gz_hydro_density(gz_context *c, const int *active, int n_active)
     cudaStream_t s = c->stream;
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (na == 0) {  // no target (an empty set or active list): nothing runs, no output changes
+        c->last_iters = 0;
+        c->h_iter_max = 0;
+        c->have_density = true;
+        c->sym_valid = false;
+        c->dens_all = (active == nullptr);
+        return GZ_OK;
+    }
     Particles ps = view(c);
     const int n = c->n;
     if (ensure(c, c->todo_a, sizeof(int) * (size_t)std::max(na, 1)) ||
@@ -1990,6 +1998,11 @@ int gz_hydro_gradients(gz_context *c, const int *active, int n_active)
     if (!c->have_density) return fail(c, GZ_ERR_ORDER, "gradients before density");
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (na == 0) {  // no target: nothing runs, no output changes
+        c->sym_valid = false;
+        c->have_gradients = true;
+        return GZ_OK;
+    }
     if (build_sym_rows(c, na, active == nullptr)) return c->err;
     c->sym_all = (active == nullptr);
     c->sym_active.assign(active ? active : (const int *)nullptr, active ? active + n_active : (const int *)nullptr);
@@ -2015,6 +2028,10 @@ int gz_hydro_force(gz_context *c, const int *active, int n_active)
     if (!c->have_gradients) return fail(c, GZ_ERR_ORDER, "force before gradients");
     int na = 0;
     if (sort_targets(c, active, n_active, &na)) return c->err;
+    if (na == 0) {  // no target: nothing runs, no output changes
+        c->pairs_refined = 0;
+        return GZ_OK;
+    }
     // the gradient pass's symmetric rows are reused when the active set is
     // the same (the corridor list shared by both loops, hydro_corridor.cc:195-255)
     const bool same = c->sym_valid && c->sym_rows == na &&

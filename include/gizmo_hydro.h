@@ -177,7 +177,10 @@ int gz_restage(gz_context *ctx);
  * like ActiveParticleList filtered by density_isactive / GasGrad_isactive.
  *   gz_hydro_density   : DensitySpec loop + density_finalize_post_runner
  *   gz_hydro_gradients : GradientsSpec loop + gradient finalize/limiter
- *   gz_hydro_force     : preloop + HydroForceSpec loop + hydro_final_operations */
+ *   gz_hydro_force     : preloop + HydroForceSpec loop + hydro_final_operations
+ * With no target (no particles, or n_active == 0) a call returns GZ_OK,
+ * launches nothing and changes no output, as the reference's loops do not
+ * run on an empty active list. */
 int gz_hydro_density(gz_context *ctx, const int *active, int n_active);
 int gz_hydro_gradients(gz_context *ctx, const int *active, int n_active);
 int gz_hydro_force(gz_context *ctx, const int *active, int n_active);
