@@ -37,8 +37,13 @@
 
 #ifdef __CUDACC__
 #define CR_HD __host__ __device__ __forceinline__
+// the ~2^-100 evaluations, taken about once in 10^4-10^5 calls: one copy each,
+// called, so the callers' code (and the instruction cache) holds only the
+// shorter evaluation
+#define CR_COLD inline __host__ __device__ __noinline__
 #else
 #define CR_HD inline
+#define CR_COLD inline
 #endif
 
 namespace gz {
@@ -274,6 +279,10 @@ CR_HD dd dd_log(double x)
 
 CR_HD double round_dd(dd a) { return add(a.hi, a.lo); }
 
+CR_COLD double exp_long(double x) { return exp_rounded({x, 0.0}); }
+CR_COLD double log_long(double x) { return round_dd(dd_log(x)); }
+CR_COLD double pow_long(double x, double y) { return exp_rounded(dd_mul_d(dd_log(x), y)); }
+
 // ------------------------------------------------------- the shorter evaluation
 // Spacing of the doubles just below v (normal, v > 0): half the ulp of v when
 // v is a power of two, its ulp otherwise. A value within half of it of v, on
@@ -357,7 +366,7 @@ CR_HD double exp(double x)
         const dd e = exp_short({x, 0.0}, m);
         if (rounds_to_hi(e.hi, e.lo, mul(kShortErr, e.hi))) return ::ldexp(e.hi, m);
     }
-    return exp_rounded({x, 0.0});
+    return exp_long(x);
 }
 
 CR_HD double log(double x)
@@ -368,7 +377,7 @@ CR_HD double log(double x)
         if (L.hi != 0.0 && rounds_to_hi(::fabs(L.hi), ::fabs(L.hi) == L.hi ? L.lo : -L.lo, 0x1p-71))
             return L.hi;
     }
-    return round_dd(dd_log(x));
+    return log_long(x);
 }
 
 CR_HD double pow(double x, double y)
@@ -391,7 +400,7 @@ CR_HD double pow(double x, double y)
             if (rounds_to_hi(e.hi, e.lo, err)) return ::ldexp(e.hi, m);
         }
     }
-    return exp_rounded(dd_mul_d(dd_log(x), y));
+    return pow_long(x, y);
 }
 
 }  // namespace cr
