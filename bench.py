@@ -47,9 +47,9 @@ FLOPS_PER_PAIR = {"density": 72.0, "gradients": 60.0, "force": 430.0}
 # (dram__bytes_read.sum + dram__bytes_write.sum over the units of the captured
 # launch), scaled to the units of a launch here: density sums per row
 # (profiles/density_sums_plummer64.md: 140.1 MB over 262,144 rows), the force
-# pair kernel per pair (profiles/force_pairs_plummer64.md: 1670.1 MB over
+# pair kernel per pair (profiles/force_pairs_plummer64.md: 1313.8 MB over
 # 7,841,073 pairs).
-DRAM_BYTES_PER_UNIT = {"density_sums": 140.1e6 / 262144, "force": 1670.1e6 / 7841073}
+DRAM_BYTES_PER_UNIT = {"density_sums": 140.1e6 / 262144, "force": 1313.8e6 / 7841073}
 
 
 def parse_args():
