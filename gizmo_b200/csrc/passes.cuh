@@ -228,7 +228,7 @@ template <typename T> __global__ void __launch_bounds__(kPackBlock) k_pack_gradi
 // finalize: construct_gradient (gradients_loop.cc:129-136) and
 // local_slopelimiter (gradients_loop.cc:1077-1130).
 template <typename T, int TPT>
-__global__ void __launch_bounds__(128, 5) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
+__global__ void __launch_bounds__(128, 4) k_gradients(PassParams p, Particles ps, const int *__restrict__ targets,
                                                    int n_targets, Csr rows, const GradRec<T> *__restrict__ rec)
 {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
