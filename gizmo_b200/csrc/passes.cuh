@@ -673,11 +673,10 @@ GZ_DEV void push_refine(const RefineQueue &q, bool fragile, long long e, long lo
 }
 
 // Resident 128-thread blocks per multiprocessor the pair kernel asks of the
-// register allocator. FP32: five (at most 96 registers a thread), measured
-// against four and six. FP64: three (168 registers), the allocation it gets
-// with no bound; at one (196 registers, two blocks) it ran 12% slower, at
-// five or six 6-10% slower.
-template <typename T> constexpr int kForcePairsMinBlocks = sizeof(T) == 4 ? 5 : 3;
+// register allocator, each measured at 256^3 against its neighbours. FP32:
+// five (at most 96 registers a thread). FP64: four (at most 128): 96.8 ms
+// against 99.0 at three, 102.8 at two, 101.3 at five.
+template <typename T> constexpr int kForcePairsMinBlocks = sizeof(T) == 4 ? 5 : 4;
 
 template <typename T>
 __global__ void __launch_bounds__(128, kForcePairsMinBlocks<T>) k_force_pairs(PassParams p, Particles ps, int n_rows,
